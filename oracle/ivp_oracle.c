@@ -1,0 +1,715 @@
+/*
+ * ivp_oracle.c -- CPU restatement of the reference's implicit velocity
+ * projection (IP) pressure step.  TEST INFRASTRUCTURE ONLY: it is the checker
+ * for the CUDA engine and the timed CPU baseline, never part of the product.
+ *
+ * Parity status: the reference (medialab-ku/ImplicitVelocityProjection) is
+ * Python + NVIDIA Warp kernels and ships no tests, fixtures or golden vectors.
+ * Warp (`warp-lang>=1.11.1,<2`, requirements.txt:7) is not installable here,
+ * so this restatement is pinned against golden vectors that were produced by
+ * executing the reference's own kernel source (ip.py, pressure_base.py,
+ * neighbour_search.py, sph_kernel.py, math_utils.py, framework.py,
+ * boundary.py) on a NumPy FP32 stand-in for the Warp runtime
+ * (tests/golden/make_golden.py), plus analytic known answers (rest-lattice
+ * density, neighbour counts, gradient antisymmetry, CG vs dense solve).
+ * Parity against real Warp execution is therefore unpinned.
+ *
+ * Layout follows the reference exactly: particle arrays in the caller's order,
+ * neighbour cache rows of `cache_size` entries (`neighbor_ids[i*cache+k]`,
+ * `neighbor_gradW[(i*cache+k)*3+c]`), FP32 arithmetic in the reference's
+ * operation order.  Every function cites the reference lines it restates.
+ *
+ * Two reduction modes:
+ *   REF  : FP32 dot products / averages accumulated in index order (what the
+ *          reference computes with float atomics on a serial device) and the
+ *          scatter form of J^T (ip.py:83-121), serial;
+ *   FAST : FP64 reductions and the gather form of J^T (pressure_base.py:130-166,
+ *          identical in exact arithmetic for symmetric lists), OpenMP over
+ *          particles.  This is the policy of the CUDA engine and the mode the
+ *          CPU baseline is timed in.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define ORC_OK 0
+#define ORC_NOT_SPD 1
+#define ORC_NOT_CONVERGED 2
+#define ORC_BAD_ARG 4
+
+typedef struct {
+    float h;              /* support radius (config_builder.py:51-52) */
+    int cache_size;       /* neighborCacheSize (simulation_data.py:157) */
+    float omega;          /* ip.py / pressure_base.py:317 */
+    double tol_pcg;       /* ip.py:228 */
+    double tol_opt;       /* densityErrorTol, pressure_base.py:316 */
+    int max_outer;        /* maxOuterIters, pressure_base.py:314 */
+    int max_pcg;          /* ip.py:229 */
+    int fixed_iters;      /* fixedOuterIters, pressure_base.py:315 */
+    int fast;             /* 0 = REF mode, 1 = FAST mode */
+} orc_params;
+
+typedef struct {
+    int outer_iters;          /* stats_outer_iters */
+    int n_err;                /* entries written to err_hist */
+    double final_err;         /* stats_final_density_error */
+    int status;
+} orc_stats;
+
+static inline float dot3(const float* a, const float* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+static inline float len3(const float* a) { return sqrtf(dot3(a, a)); }
+
+/* ---------------------------------------------------------------- kernels */
+
+/* sph_kernel.py:8-25 */
+float orc_cubic_kernel(float r, float h) {
+    float res = 0.0f;
+    float k = 8.0f / 3.14159265359f;
+    k = k / (h * h * h);
+    float q = r / h;
+    if (q <= 1.0f) {
+        if (q <= 0.5f) {
+            float q2 = q * q;
+            float q3 = q2 * q;
+            res = k * (6.0f * q3 - 6.0f * q2 + 1.0f);
+        } else {
+            float f = 1.0f - q;
+            res = k * 2.0f * f * f * f;
+        }
+    }
+    return res;
+}
+
+/* sph_kernel.py:52-61 */
+void orc_spiky_grad(const float* r, float h, float* out) {
+    float k = 45.0f / (3.14159265359f * h * h * h * h * h * h);
+    float rn = len3(r);
+    if (rn < 1e-6f) rn = 1e-6f;
+    float t = h - rn;
+    float s = -k * (t * t);
+    for (int c = 0; c < 3; ++c) out[c] = s * (r[c] / rn);
+}
+
+/* ------------------------------------------------------- neighbour cache */
+
+static int cell_of(float v, float lo, float inv, int dim) {
+    int c = (int)floorf((v - lo) * inv);
+    return c < 0 ? 0 : (c >= dim ? dim - 1 : c);
+}
+
+/*
+ * neighbour_search.py:10-51 (build_neighbor_cache) over a uniform grid of cell
+ * size h.  Candidate order is cell (z, y, x ascending) then particle index;
+ * the reference's order is Warp's hash-grid order, which only matters when a
+ * particle has more than cache_size neighbours.  Lists are built for every
+ * particle when only_dynamic == 0 (as the reference does) or for dynamic ones
+ * only.  Returns the number of particles whose true count exceeded the cap.
+ */
+long orc_build_neighbor_cache(int n, const float* x, const int* is_dynamic, int only_dynamic,
+                              float h, int cache, int* count, int* ids, float* gradW) {
+    if (n <= 0) return 0;
+    float lo[3] = {x[0], x[1], x[2]}, hi[3] = {x[0], x[1], x[2]};
+    for (int i = 1; i < n; ++i)
+        for (int c = 0; c < 3; ++c) {
+            if (x[3 * i + c] < lo[c]) lo[c] = x[3 * i + c];
+            if (x[3 * i + c] > hi[c]) hi[c] = x[3 * i + c];
+        }
+    int dim[3];
+    float inv = 1.0f / h;
+    for (int c = 0; c < 3; ++c) {
+        dim[c] = (int)floorf((hi[c] - lo[c]) * inv) + 1;
+        if (dim[c] < 1) dim[c] = 1;
+    }
+    long ncell = (long)dim[0] * dim[1] * dim[2];
+    int* cstart = (int*)calloc(ncell + 1, sizeof(int));
+    int* cell = (int*)malloc(sizeof(int) * n);
+    int* sorted = (int*)malloc(sizeof(int) * n);
+    for (int i = 0; i < n; ++i) {
+        int cx = cell_of(x[3 * i], lo[0], inv, dim[0]);
+        int cy = cell_of(x[3 * i + 1], lo[1], inv, dim[1]);
+        int cz = cell_of(x[3 * i + 2], lo[2], inv, dim[2]);
+        cell[i] = (int)(((long)cz * dim[1] + cy) * dim[0] + cx);
+        cstart[cell[i] + 1]++;
+    }
+    for (long c = 0; c < ncell; ++c) cstart[c + 1] += cstart[c];
+    int* fill = (int*)malloc(sizeof(int) * ncell);
+    memcpy(fill, cstart, sizeof(int) * ncell);
+    for (int i = 0; i < n; ++i) sorted[fill[cell[i]]++] = i;
+    free(fill);
+
+    long overflow = 0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : overflow)
+    for (int i = 0; i < n; ++i) {
+        if (only_dynamic && !is_dynamic[i]) { count[i] = 0; continue; }
+        const float* xi = x + 3 * i;
+        int ci = cell[i];
+        int cx = ci % dim[0], cy = (ci / dim[0]) % dim[1], cz = ci / (dim[0] * dim[1]);
+        int cnt = 0, found = 0;
+        for (int dz = -1; dz <= 1; ++dz) {
+            int z = cz + dz;
+            if (z < 0 || z >= dim[2]) continue;
+            for (int dy = -1; dy <= 1; ++dy) {
+                int y = cy + dy;
+                if (y < 0 || y >= dim[1]) continue;
+                for (int dx = -1; dx <= 1; ++dx) {
+                    int xx = cx + dx;
+                    if (xx < 0 || xx >= dim[0]) continue;
+                    long c = ((long)z * dim[1] + y) * dim[0] + xx;
+                    for (int s = cstart[c]; s < cstart[c + 1]; ++s) {
+                        int j = sorted[s];
+                        if (j == i) continue;
+                        float r[3] = {xi[0] - x[3 * j], xi[1] - x[3 * j + 1], xi[2] - x[3 * j + 2]};
+                        float rn = len3(r);
+                        if (rn < h) {
+                            ++found;
+                            if (cnt < cache) {
+                                long b = (long)i * cache + cnt;
+                                ids[b] = j;
+                                orc_spiky_grad(r, h, gradW + 3 * b);
+                                ++cnt;
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        count[i] = cnt;
+        if (found > cache) ++overflow;
+    }
+    free(cstart);
+    free(cell);
+    free(sorted);
+    return overflow;
+}
+
+static inline int clamp_cnt(int c, int cache) { return c > cache ? cache : c; }
+
+/* pressure_base.py:12-46 */
+void orc_compute_density(int n, const float* x, const float* m, const int* dyn, float h, int cache,
+                         const int* count, const int* ids, float* density) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) {
+        if (!dyn[i]) continue;
+        float rho = 0.0f;
+        rho = rho + m[i] * orc_cubic_kernel(0.0f, h);
+        int cnt = clamp_cnt(count[i], cache);
+        for (int k = 0; k < cnt; ++k) {
+            int j = ids[(long)i * cache + k];
+            float r[3] = {x[3 * i] - x[3 * j], x[3 * i + 1] - x[3 * j + 1], x[3 * i + 2] - x[3 * j + 2]};
+            rho += m[j] * orc_cubic_kernel(len3(r), h);
+        }
+        density[i] = rho;
+    }
+}
+
+/* pressure_base.py:49-87 */
+void orc_compute_aii(int n, const float* m, const float* m_inv, const int* dyn, int cache,
+                     const int* count, const int* ids, const float* gradW, float* kdiag) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) {
+        if (!dyn[i]) { kdiag[i] = 0.0f; continue; }
+        float aii = 0.0f;
+        float jii[3] = {0.0f, 0.0f, 0.0f};
+        int cnt = clamp_cnt(count[i], cache);
+        for (int k = 0; k < cnt; ++k) {
+            long b = (long)i * cache + k;
+            int j = ids[b];
+            float jij[3] = {m[j] * gradW[3 * b], m[j] * gradW[3 * b + 1], m[j] * gradW[3 * b + 2]};
+            if (dyn[j]) aii += dot3(jij, jij) * m_inv[j];
+            for (int c = 0; c < 3; ++c) jii[c] -= jij[c];
+        }
+        aii += dot3(jii, jii) * m_inv[i];
+        kdiag[i] = 1.0f / (aii + 1e-3f);
+    }
+}
+
+/* ip_pack_fused (ip.py:124-171) and compute_J_x_kernel (pressure_base.py:91-127):
+ * out_i = sum_j m_j (val_i - [dyn j] val_j) . gradW_ij */
+static void jx_plain(int n, const float* val, const float* m, const int* dyn, int cache, const int* count,
+                     const int* ids, const float* gradW, float* out) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) {
+        if (!dyn[i]) { out[i] = 0.0f; continue; }
+        const float* vi = val + 3 * i;
+        float acc = 0.0f;
+        int cnt = clamp_cnt(count[i], cache);
+        for (int k = 0; k < cnt; ++k) {
+            long b = (long)i * cache + k;
+            int j = ids[b];
+            const float* g = gradW + 3 * b;
+            if (dyn[j]) {
+                float dv[3] = {vi[0] - val[3 * j], vi[1] - val[3 * j + 1], vi[2] - val[3 * j + 2]};
+                acc += m[j] * dot3(dv, g);
+            } else {
+                acc += m[j] * dot3(vi, g);
+            }
+        }
+        out[i] = acc;
+    }
+}
+
+/* compute_Jx_pcg (ip.py:19-60): y_i = (sum_j (p_i - [dyn j] p_j) . (m_j gradW)) dfdt_i k_i */
+static void jx_pcg(int n, const float* p, const float* m, const float* dfdt, const float* kd, const int* dyn,
+                   int cache, const int* count, const int* ids, const float* gradW, float* y) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) {
+        y[i] = 0.0f;
+        if (!dyn[i]) continue;
+        if (dfdt[i] > 0.0f) {
+            const float* pi = p + 3 * i;
+            float acc = 0.0f;
+            int cnt = clamp_cnt(count[i], cache);
+            for (int k = 0; k < cnt; ++k) {
+                long b = (long)i * cache + k;
+                int j = ids[b];
+                const float* g = gradW + 3 * b;
+                float vij[3] = {m[j] * g[0], m[j] * g[1], m[j] * g[2]};
+                if (dyn[j]) {
+                    float dv[3] = {pi[0] - p[3 * j], pi[1] - p[3 * j + 1], pi[2] - p[3 * j + 2]};
+                    acc += dot3(dv, vij);
+                } else {
+                    acc += dot3(pi, vij);
+                }
+            }
+            y[i] = acc * dfdt[i] * kd[i];
+        }
+    }
+}
+
+/* compute_Ax_part1 + compute_Ax_part2 (ip.py:63-121), scatter form, serial */
+static void ax_scatter(int n, const float* p, const float* y, const float* m, const float* dfdt, float omega,
+                       const int* dyn, int cache, const int* count, const int* ids, const float* gradW,
+                       float* ap) {
+    for (int i = 0; i < n; ++i)
+        for (int c = 0; c < 3; ++c) ap[3 * i + c] = dyn[i] ? m[i] * p[3 * i + c] : 0.0f;
+    for (int i = 0; i < n; ++i) {
+        if (!dyn[i] || dfdt[i] <= 0.0f) continue;
+        float yi = y[i];
+        int cnt = clamp_cnt(count[i], cache);
+        for (int k = 0; k < cnt; ++k) {
+            long b = (long)i * cache + k;
+            int j = ids[b];
+            const float* g = gradW + 3 * b;
+            float s = omega * yi;
+            for (int c = 0; c < 3; ++c) {
+                float contrib = s * (m[j] * g[c]);
+                ap[3 * i + c] += contrib;
+                if (dyn[j]) ap[3 * j + c] -= contrib;
+            }
+        }
+    }
+}
+
+/* Ap = m p + omega J^T y, gather form (pressure_base.py:130-166 algebra) */
+static void ax_gather(int n, const float* p, const float* y, const float* m, float omega, const int* dyn,
+                      int cache, const int* count, const int* ids, const float* gradW, float* ap) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) {
+        if (!dyn[i]) { ap[3 * i] = ap[3 * i + 1] = ap[3 * i + 2] = 0.0f; continue; }
+        float acc[3] = {0.0f, 0.0f, 0.0f};
+        float yi = y[i], mi = m[i];
+        int cnt = clamp_cnt(count[i], cache);
+        for (int k = 0; k < cnt; ++k) {
+            long b = (long)i * cache + k;
+            int j = ids[b];
+            const float* g = gradW + 3 * b;
+            float w = dyn[j] ? (m[j] * yi + mi * y[j]) : (m[j] * yi);
+            for (int c = 0; c < 3; ++c) acc[c] += w * g[c];
+        }
+        for (int c = 0; c < 3; ++c) ap[3 * i + c] = mi * p[3 * i + c] + omega * acc[c];
+    }
+}
+
+/* ip_rhs_fused (ip.py:174-215) */
+static void rhs_fused(int n, const float* f, const float* kd, const float* m, float omega, const int* dyn,
+                      int cache, const int* count, const int* ids, const float* gradW, float* rhs) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) {
+        if (!dyn[i]) { rhs[3 * i] = rhs[3 * i + 1] = rhs[3 * i + 2] = 0.0f; continue; }
+        float fki = f[i] * kd[i], mi = m[i];
+        float acc[3] = {0.0f, 0.0f, 0.0f};
+        int cnt = clamp_cnt(count[i], cache);
+        for (int k = 0; k < cnt; ++k) {
+            long b = (long)i * cache + k;
+            int j = ids[b];
+            const float* g = gradW + 3 * b;
+            float w = dyn[j] ? (m[j] * fki + mi * (f[j] * kd[j])) : (m[j] * fki);
+            for (int c = 0; c < 3; ++c) acc[c] += w * g[c];
+        }
+        for (int c = 0; c < 3; ++c) rhs[3 * i + c] = omega * acc[c];
+    }
+}
+
+/* dot_vec3_tiled (math_utils.py:159-173) as summed by PressureBase.dot (pressure_base.py:425-436) */
+static double dot_dyn(int n, const float* a, const float* b, const int* dyn, int fast) {
+    if (fast) {
+        double s = 0.0;
+        for (int i = 0; i < n; ++i)
+            if (dyn[i]) s += (double)dot3(a + 3 * i, b + 3 * i);
+        return s;
+    }
+    float s = 0.0f;
+    for (int i = 0; i < n; ++i)
+        if (dyn[i]) s += dot3(a + 3 * i, b + 3 * i);
+    return (double)s;
+}
+
+/* coef_wise_div + compute_avg_density_error (math_utils.py:77-91, pressure_base.py:187-203, 405-423):
+ * avg over dynamic particles of max(t_i / max(rho0_i, 1e-6), 0) */
+static double avg_density_error(int n, const float* t, const float* rho0, const int* dyn, int fast) {
+    if (fast) {
+        double s = 0.0;
+        long cnt = 0;
+        for (int i = 0; i < n; ++i) {
+            if (!dyn[i]) continue;
+            float den = rho0[i] < 1e-6f ? 1e-6f : rho0[i];
+            float q = t[i] / den;
+            s += (double)(q > 0.0f ? q : 0.0f);
+            ++cnt;
+        }
+        return cnt > 0 ? s / (double)cnt : 0.0;
+    }
+    float s = 0.0f, cnt = 0.0f;
+    for (int i = 0; i < n; ++i) {
+        if (!dyn[i]) continue;
+        float den = rho0[i] < 1e-6f ? 1e-6f : rho0[i];
+        float q = t[i] / den;
+        s += (q > 0.0f ? q : 0.0f);
+        cnt += 1.0f;
+    }
+    return cnt > 0.0f ? (double)s / (double)cnt : 0.0;
+}
+
+/*
+ * IP.PCG (ip.py:283-329): CG from x = 0 on A = M + omega J^T diag(dfdt k) J.
+ * Returns the iteration count, or -1 on pAp < 0 (the reference raises).
+ */
+static int orc_pcg(int n, const orc_params* P, const float* m, const float* dfdt, const float* kd,
+                   const int* dyn, const int* count, const int* ids, const float* gradW, float* x,
+                   const float* b, float* r, float* p, float* ap, float* y) {
+    int cache = P->cache_size;
+    memcpy(r, b, sizeof(float) * 3 * (size_t)n);
+    double rr_old = dot_dyn(n, r, r, dyn, P->fast);
+    int it = 0;
+    if (rr_old > 1e-30) {
+        memcpy(p, r, sizeof(float) * 3 * (size_t)n);
+        for (;;) {
+            jx_pcg(n, p, m, dfdt, kd, dyn, cache, count, ids, gradW, y);
+            if (P->fast)
+                ax_gather(n, p, y, m, P->omega, dyn, cache, count, ids, gradW, ap);
+            else
+                ax_scatter(n, p, y, m, dfdt, P->omega, dyn, cache, count, ids, gradW, ap);
+            double pap = dot_dyn(n, p, ap, dyn, P->fast);
+            if (pap < 0.0) return -1;
+            double alpha = rr_old / (pap > 1e-30 ? pap : 1e-30);
+            float af = (float)alpha;
+#pragma omp parallel for schedule(static)
+            for (int i = 0; i < n; ++i) {
+                if (!dyn[i]) continue;
+                for (int c = 0; c < 3; ++c) {
+                    x[3 * i + c] = x[3 * i + c] + af * p[3 * i + c];
+                    r[3 * i + c] = r[3 * i + c] - af * ap[3 * i + c];
+                }
+            }
+            double rr_new = dot_dyn(n, r, r, dyn, P->fast);
+            ++it;
+            if ((rr_new < P->tol_pcg && it >= 2) || it >= P->max_pcg) break;
+            double beta = rr_new / (rr_old > 1e-30 ? rr_old : 1e-30);
+            float bf = (float)beta;
+#pragma omp parallel for schedule(static)
+            for (int i = 0; i < n; ++i) {
+                if (!dyn[i]) continue;
+                for (int c = 0; c < 3; ++c) p[3 * i + c] = r[3 * i + c] + bf * p[3 * i + c];
+            }
+            rr_old = rr_new;
+        }
+    }
+    return it;
+}
+
+/*
+ * IP.solve(dt) (ip.py:331-404) with compute_constraint (pressure_base.py:169-184,
+ * 394-403), check_converged (487-495) and final_density_error (438-447).
+ * In: x-independent state (density, rho0, m, dyn, lists, kdiag), v.  Out: v
+ * (overwritten with d/dt), err_hist[max_outer+1], pcg_hist[max_outer],
+ * optional divergence (pressure_base.py:449-457; may be NULL) and stats.
+ * Work buffers are allocated here (the oracle is not a hot path).
+ */
+int orc_ip_solve(int n, const orc_params* P, float dt, const float* density, const float* rho0,
+                 const float* m, const int* dyn, const int* count, const int* ids, const float* gradW,
+                 const float* kd, float* v, double* err_hist, int* pcg_hist, float* divergence,
+                 float* d_out, orc_stats* st) {
+    int cache = P->cache_size;
+    size_t n3 = 3 * (size_t)n;
+    float* c = (float*)calloc(n, sizeof(float));
+    float* t = (float*)calloc(n, sizeof(float));
+    float* f = (float*)calloc(n, sizeof(float));
+    float* dfdt = (float*)calloc(n, sizeof(float));
+    float* y = (float*)calloc(n, sizeof(float));
+    float* d = (float*)calloc(n3, sizeof(float));
+    float* rhs = (float*)calloc(n3, sizeof(float));
+    float* sol = (float*)calloc(n3, sizeof(float));
+    float* r = (float*)calloc(n3, sizeof(float));
+    float* p = (float*)calloc(n3, sizeof(float));
+    float* ap = (float*)calloc(n3, sizeof(float));
+
+    for (int i = 0; i < n; ++i) c[i] = dyn[i] ? density[i] - rho0[i] : 0.0f;
+    for (int i = 0; i < n; ++i)
+        if (dyn[i])
+            for (int q = 0; q < 3; ++q) d[3 * i + q] = dt * v[3 * i + q];
+
+    int status = ORC_OK;
+    int opt_iter = 0, n_err = 0;
+    double err = 0.0;
+    for (;;) {
+        /* ip_pack_fused */
+        jx_plain(n, d, m, dyn, cache, count, ids, gradW, t);
+        for (int i = 0; i < n; ++i) {
+            if (!dyn[i]) { t[i] = f[i] = dfdt[i] = 0.0f; continue; }
+            float ti = t[i] + c[i];
+            t[i] = ti;
+            f[i] = ti > 0.0f ? ti : 0.0f;
+            dfdt[i] = ti >= 1e-6f ? 1.0f : 0.0f;
+        }
+        err = avg_density_error(n, f, rho0, dyn, P->fast);
+        if (err_hist && n_err < P->max_outer + 1) err_hist[n_err] = err;
+        ++n_err;
+        int converged = err < P->tol_opt && !P->fixed_iters;
+        if ((converged && opt_iter >= 1) || opt_iter >= P->max_outer) break;
+        rhs_fused(n, f, kd, m, P->omega, dyn, cache, count, ids, gradW, rhs);
+        for (size_t q = 0; q < n3; ++q) sol[q] = 0.0f;
+        int it = orc_pcg(n, P, m, dfdt, kd, dyn, count, ids, gradW, sol, rhs, r, p, ap, y);
+        if (it < 0) { status = ORC_NOT_SPD; break; }
+        if (pcg_hist && opt_iter < P->max_outer) pcg_hist[opt_iter] = it;
+        for (int i = 0; i < n; ++i)
+            if (dyn[i])
+                for (int q = 0; q < 3; ++q) d[3 * i + q] = d[3 * i + q] + (-1.0f) * sol[3 * i + q];
+        ++opt_iter;
+    }
+    if (status == ORC_OK && !P->fixed_iters && err >= P->tol_opt && opt_iter >= P->max_outer)
+        status = ORC_NOT_CONVERGED;
+
+    float inv_dt = (float)(1.0 / (double)dt);
+    for (int i = 0; i < n; ++i)
+        if (dyn[i])
+            for (int q = 0; q < 3; ++q) v[3 * i + q] = inv_dt * d[3 * i + q];
+
+    /* final_density_error: avg(max((c + J d) / rho0, 0)) */
+    jx_plain(n, d, m, dyn, cache, count, ids, gradW, t);
+    for (int i = 0; i < n; ++i)
+        if (dyn[i]) t[i] = t[i] + 1.0f * c[i];
+    double final_err = avg_density_error(n, t, rho0, dyn, P->fast);
+    if (divergence) {
+        jx_plain(n, v, m, dyn, cache, count, ids, gradW, t);
+        for (int i = 0; i < n; ++i) divergence[i] = dyn[i] ? (t[i] > 0.0f ? t[i] : 0.0f) : 0.0f;
+    }
+    if (d_out) memcpy(d_out, d, sizeof(float) * n3);
+    if (st) {
+        st->outer_iters = opt_iter;
+        st->n_err = n_err;
+        st->final_err = final_err;
+        st->status = status;
+    }
+    free(c); free(t); free(f); free(dfdt); free(y); free(d); free(rhs); free(sol); free(r); free(p); free(ap);
+    return status;
+}
+
+/* apply_gravity (framework.py:26-41) */
+void orc_apply_gravity(int n, float* v, const int* dyn, const float* g, float dt) {
+    float gd[3] = {g[0] * dt, g[1] * dt, g[2] * dt};
+    for (int i = 0; i < n; ++i)
+        if (dyn[i])
+            for (int c = 0; c < 3; ++c) v[3 * i + c] = v[3 * i + c] + gd[c];
+}
+
+/* advect_position (framework.py:117-136) then enforce_boundary (boundary.py:10-91) */
+void orc_advect_and_clamp(int n, float* x, float* v, const int* dyn, float dt, const float* domain,
+                          float padding) {
+    for (int i = 0; i < n; ++i) {
+        float* xi = x + 3 * i;
+        float* vi = v + 3 * i;
+        if (!dyn[i]) vi[0] = vi[1] = vi[2] = 0.0f;
+        for (int c = 0; c < 3; ++c) xi[c] = xi[c] + dt * vi[c];
+        if (!dyn[i]) continue;
+        float nrm[3] = {0.0f, 0.0f, 0.0f};
+        for (int c = 0; c < 3; ++c) {
+            if (xi[c] > domain[c] - padding) { nrm[c] += 1.0f; xi[c] = domain[c] - padding; }
+            if (xi[c] <= padding) { nrm[c] += -1.0f; xi[c] = padding; }
+        }
+        float nl = len3(nrm);
+        if (nl > 1e-6f) {
+            float u[3] = {nrm[0] / nl, nrm[1] / nl, nrm[2] / nl};
+            float vn = dot3(vi, u);
+            for (int c = 0; c < 3; ++c) vi[c] = vi[c] - (1.0f + 0.5f) * vn * u[c];
+        }
+    }
+}
+
+/*
+ * One Framework.forward() step with IP and no viscosity / surface tension
+ * (framework.py:423-544): gravity, IP.solve, advect + clamp, neighbour
+ * rebuild, density, Aii.  `count/ids/gradW/density/kd` must hold the state of
+ * the previous rebuild (Framework.initialize, framework.py:282-290).
+ */
+int orc_step(int n, const orc_params* P, float dt, const float* g, const float* domain, float* x, float* v,
+             const float* rho0, const float* m, const float* m_inv, const int* dyn, int* count, int* ids,
+             float* gradW, float* density, float* kd, double* err_hist, int* pcg_hist, orc_stats* st,
+             long* overflow) {
+    orc_apply_gravity(n, v, dyn, g, dt);
+    int status = orc_ip_solve(n, P, dt, density, rho0, m, dyn, count, ids, gradW, kd, v, err_hist, pcg_hist,
+                              NULL, NULL, st);
+    orc_advect_and_clamp(n, x, v, dyn, dt, domain, P->h);
+    long ov = orc_build_neighbor_cache(n, x, dyn, 1, P->h, P->cache_size, count, ids, gradW);
+    if (overflow) *overflow = ov;
+    orc_compute_density(n, x, m, dyn, P->h, P->cache_size, count, ids, density);
+    orc_compute_aii(n, m, m_inv, dyn, P->cache_size, count, ids, gradW, kd);
+    return status;
+}
+
+/*
+ * FP64 CG on the same linear system as one IP outer iteration: given the
+ * lists, mass, dfdt, k and rhs (all FP32 inputs), solve
+ * (M + omega J^T diag(dfdt k) J) x = rhs in double precision until
+ * ||r||^2 <= rel_tol^2 ||b||^2.  Returns iterations.  Used to state every
+ * result's error against an FP64 solve.
+ */
+int orc_cg_f64(int n, float omega, int cache, const float* m, const float* dfdt, const float* kd,
+               const int* dyn, const int* count, const int* ids, const float* gradW, const float* rhs,
+               double rel_tol, int max_iter, double* x_out) {
+    size_t n3 = 3 * (size_t)n;
+    double* r = (double*)calloc(n3, sizeof(double));
+    double* p = (double*)calloc(n3, sizeof(double));
+    double* ap = (double*)calloc(n3, sizeof(double));
+    double* y = (double*)calloc(n, sizeof(double));
+    double bb = 0.0;
+    for (int i = 0; i < n; ++i) {
+        for (int c = 0; c < 3; ++c) {
+            x_out[3 * i + c] = 0.0;
+            r[3 * i + c] = dyn[i] ? (double)rhs[3 * i + c] : 0.0;
+            p[3 * i + c] = r[3 * i + c];
+            bb += r[3 * i + c] * r[3 * i + c];
+        }
+    }
+    double rr = bb;
+    int it = 0;
+    while (it < max_iter && rr > rel_tol * rel_tol * bb && rr > 0.0) {
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < n; ++i) {
+            y[i] = 0.0;
+            if (!dyn[i] || dfdt[i] <= 0.0f) continue;
+            double acc = 0.0;
+            int cnt = clamp_cnt(count[i], cache);
+            for (int k = 0; k < cnt; ++k) {
+                long b = (long)i * cache + k;
+                int j = ids[b];
+                for (int c = 0; c < 3; ++c) {
+                    double dv = p[3 * i + c] - (dyn[j] ? p[3 * j + c] : 0.0);
+                    acc += (double)m[j] * dv * (double)gradW[3 * b + c];
+                }
+            }
+            y[i] = acc * (double)dfdt[i] * (double)kd[i];
+        }
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < n; ++i) {
+            for (int c = 0; c < 3; ++c) ap[3 * i + c] = 0.0;
+            if (!dyn[i]) continue;
+            double acc[3] = {0.0, 0.0, 0.0};
+            int cnt = clamp_cnt(count[i], cache);
+            for (int k = 0; k < cnt; ++k) {
+                long b = (long)i * cache + k;
+                int j = ids[b];
+                double w = (double)m[j] * y[i] + (dyn[j] ? (double)m[i] * y[j] : 0.0);
+                for (int c = 0; c < 3; ++c) acc[c] += w * (double)gradW[3 * b + c];
+            }
+            for (int c = 0; c < 3; ++c) ap[3 * i + c] = (double)m[i] * p[3 * i + c] + (double)omega * acc[c];
+        }
+        double pap = 0.0;
+        for (size_t q = 0; q < n3; ++q) pap += p[q] * ap[q];
+        if (pap <= 0.0) break;
+        double alpha = rr / pap;
+        double rr_new = 0.0;
+        for (size_t q = 0; q < n3; ++q) {
+            x_out[q] += alpha * p[q];
+            r[q] -= alpha * ap[q];
+            rr_new += r[q] * r[q];
+        }
+        double beta = rr_new / rr;
+        for (size_t q = 0; q < n3; ++q) p[q] = r[q] + beta * p[q];
+        rr = rr_new;
+        ++it;
+    }
+    free(r); free(p); free(ap); free(y);
+    return it;
+}
+
+/* One outer-iteration system at displacement d: returns t, f, dfdt and rhs as
+ * ip_pack_fused + ip_rhs_fused compute them (ip.py:124-215). */
+void orc_ip_system(int n, float omega, int cache, const float* d, const float* c, const float* m,
+                   const int* dyn, const int* count, const int* ids, const float* gradW, const float* kd,
+                   float* t, float* f, float* dfdt, float* rhs) {
+    jx_plain(n, d, m, dyn, cache, count, ids, gradW, t);
+    for (int i = 0; i < n; ++i) {
+        if (!dyn[i]) { t[i] = f[i] = dfdt[i] = 0.0f; continue; }
+        float ti = t[i] + c[i];
+        t[i] = ti;
+        f[i] = ti > 0.0f ? ti : 0.0f;
+        dfdt[i] = ti >= 1e-6f ? 1.0f : 0.0f;
+    }
+    rhs_fused(n, f, kd, m, omega, dyn, cache, count, ids, gradW, rhs);
+}
+
+/* A p applied in FP64 (gather form) for symmetry / SPD checks on small cases. */
+void orc_apply_A_f64(int n, float omega, int cache, const float* m, const float* dfdt, const float* kd,
+                     const int* dyn, const int* count, const int* ids, const float* gradW, const double* p,
+                     double* ap) {
+    double* y = (double*)calloc(n, sizeof(double));
+    for (int i = 0; i < n; ++i) {
+        if (!dyn[i] || dfdt[i] <= 0.0f) continue;
+        double acc = 0.0;
+        int cnt = clamp_cnt(count[i], cache);
+        for (int k = 0; k < cnt; ++k) {
+            long b = (long)i * cache + k;
+            int j = ids[b];
+            for (int c = 0; c < 3; ++c)
+                acc += (double)m[j] * (p[3 * i + c] - (dyn[j] ? p[3 * j + c] : 0.0)) * (double)gradW[3 * b + c];
+        }
+        y[i] = acc * (double)dfdt[i] * (double)kd[i];
+    }
+    /* scatter form of J^T, exact transpose of J even for asymmetric lists */
+    for (int i = 0; i < n; ++i)
+        for (int c = 0; c < 3; ++c) ap[3 * i + c] = dyn[i] ? (double)m[i] * p[3 * i + c] : 0.0;
+    for (int i = 0; i < n; ++i) {
+        if (!dyn[i] || y[i] == 0.0) continue;
+        int cnt = clamp_cnt(count[i], cache);
+        for (int k = 0; k < cnt; ++k) {
+            long b = (long)i * cache + k;
+            int j = ids[b];
+            for (int c = 0; c < 3; ++c) {
+                double contrib = (double)omega * y[i] * (double)m[j] * (double)gradW[3 * b + c];
+                ap[3 * i + c] += contrib;
+                if (dyn[j]) ap[3 * j + c] -= contrib;
+            }
+        }
+    }
+    free(y);
+}
+
+int orc_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+void orc_set_num_threads(int t) {
+#ifdef _OPENMP
+    if (t > 0) omp_set_num_threads(t);
+#else
+    (void)t;
+#endif
+}
