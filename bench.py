@@ -1,0 +1,363 @@
+#!/usr/bin/env python
+"""Benchmark of the IP pressure step: particle-steps/s at <= 0.1 % average
+density error, on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload tall_column|small_column|dam_break]
+
+One step = one full Framework.forward() of every replica's scene (gravity,
+implicit viscosity where the workload enables it, the IP solve with its CG,
+advect + boundary clamp, neighbour rebuild, density, Aii, divergence).  The
+value counts fluid particles x steps / device time; each timed step must end
+with status OK and its final average density error below densityErrorTol.
+
+Multi-GPU (torchrun): the plain form does not shard a scene, so every rank
+runs an independent replica (weak scaling, no data-path collective); time is
+the max over ranks.
+
+`--impl reference` times the CPU restatement of the reference's algorithm
+(oracle/, OpenMP over all host cores) on the same workload, on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "particle-steps/s at <=0.1% avg density error"
+UNIT = "particle-steps/s"
+
+
+def make_scene(name: str):
+    from implicitvelocityprojection_b200 import scenes as S
+    if name == "tall_column":
+        return S.tall_column(viscosity=False)
+    if name == "tall_column_visc":
+        return S.tall_column(viscosity=True)
+    if name == "small_column":
+        return S.small_column()
+    if name == "dam_break":
+        return S.dam_break(viscosity_method=0, viscosity_coeff=0.0, surface_tension_method=0,
+                           surface_tension_coeff=0.0)
+    raise SystemExit(f"unknown workload {name}")
+
+
+def workload_config(sc, name: str) -> dict:
+    return {"workload": sc.name if name != "tall_column" else "tall_column_102k_ip",
+            "fluid_particles": sc.n_dynamic, "boundary_particles": sc.n - sc.n_dynamic,
+            "spacing_m": sc.particle_diameter, "dt_s": sc.dt, "densityErrorTol": sc.density_error_tol,
+            "viscosity": ("weiler18 nu=%g" % sc.viscosity_coeff) if sc.viscosity_method == 1 else "off",
+            "surface_tension": "off", "reductions": "f64 (CG inner products, error averages)",
+            "l2": "flushed between timed steps (256 MiB device write, outside the timed events)"}
+
+
+# ----------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (200 ms period)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------- roofline
+
+def algorithmic_bytes(kernel: str, n_dyn: int, n_all: int, pairs: int) -> float:
+    """Algorithmic bytes of one launch, per the byte model of the path: 16 B
+    per stored neighbour pair (4 B id + 12 B gradient, the reference's cache
+    entry) and each per-particle stream counted once per pass."""
+    P = float(pairs)
+    if kernel == "cg_a":
+        return 16 * P + 48 * n_dyn
+    if kernel == "cg_b":
+        return 16 * P + 64 * n_dyn
+    if kernel == "pack":
+        return 16 * P + 36 * n_dyn
+    if kernel == "rhs":
+        return 16 * P + 32 * n_dyn
+    if kernel == "nbr_build":  # lists written + density + Aii pass
+        return 16 * P + 16 * P + 64 * n_all + 28 * n_all
+    if kernel == "divergence":
+        return 16 * P + 28 * n_dyn
+    return 0.0
+
+
+def load_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic(kernel: str, workload: str):
+    p = os.path.join(REPO, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    return d.get(workload, {}).get(kernel)
+
+
+# ----------------------------------------------------------------- arms
+
+def cpu_baseline(sc, budget_s: float, max_steps: int):
+    """The oracle (C restatement, OpenMP) stepping the same workload."""
+    from oracle import oracle as O
+    st = O.State.from_scene(sc)
+    st.rebuild()
+    t0 = time.perf_counter()
+    steps = 0
+    while steps < max_steps and (time.perf_counter() - t0) < budget_s:
+        st.step(fast=True)
+        steps += 1
+    dt = time.perf_counter() - t0
+    return {"value": sc.n_dynamic * steps / dt, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
+            "sample": f"{steps} full steps of {sc.name} ({sc.n_dynamic} fluid particles), {dt:.1f} s"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    sc = make_scene(args.workload)
+    from oracle import oracle as O
+    st = O.State.from_scene(sc)
+    st.rebuild()
+    for _ in range(args.warmup):
+        st.step(fast=True)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        st.step(fast=True)
+        times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    value = sc.n_dynamic * len(times) / tot
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * tot / len(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "impl": "reference", "config": workload_config(sc, args.workload),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
+                             "sample": f"{len(times)} full steps of {sc.name} on the CPU restatement"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "p50_ms": 1000 * statistics.median(times), "p99_ms": 1000 * float(np.percentile(times, 99))}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from implicitvelocityprojection_b200.engine import Engine, EngineOptions
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    sc = make_scene(args.workload)
+    opts = EngineOptions(lanes_per_particle=args.lanes, particles_per_block=128 // args.lanes)
+    eng = Engine([sc], device=str(dev), options=opts, divergence=True)
+    eng.build()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        flush.zero_()
+        eng.step(1)
+    torch.cuda.synchronize()
+    eng.reset_counters()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    clocks = ClockSampler(local_rank)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    wall0 = time.perf_counter()
+    for k in range(args.steps):
+        flush.zero_()
+        starts[k].record(stream)
+        eng.step(1)
+        ends[k].record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    wall = time.perf_counter() - wall0
+    clk = clocks.stop()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = float(sum(step_ms))
+    raw = eng.raw_stats(0)
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    valid = raw.failed_solves == 0 and raw.solves == args.steps and \
+        raw.max_final_density_error < sc.density_error_tol
+    value = world * sc.n_dynamic * args.steps / (total_ms / 1000.0)
+    n_launch = 12 * args.steps + (raw.sum_outer_iters + args.steps) + raw.sum_outer_iters + 2 * raw.sum_pcg_iters
+
+    # per-kernel device time of the same workload (host-driven launches with
+    # CUDA events around each kernel, after the timed region)
+    prof = eng.profile_step(3)
+    pairs = int(eng.raw_stats(0).neighbour_pairs)
+    dom = max(prof.items(), key=lambda kv: kv[1][0])
+    dom_name, (dom_ms, dom_n) = dom
+    avg_s = dom_ms / dom_n / 1000.0
+    alg = algorithmic_bytes(dom_name, sc.n_dynamic, sc.n, pairs)
+    peak, peak_kind = load_peaks()
+    achieved = alg / avg_s / 1e9 if avg_s > 0 else 0.0
+    roof = {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_kind": peak_kind, "traffic": load_traffic(dom_name, args.workload),
+            "algorithmic_bytes_per_launch": alg, "avg_launch_us": avg_s * 1e6,
+            "share_of_step": dom_ms / sum(v[0] for v in prof.values()),
+            "kernels_ms_per_step": {k: round(v[0] / 3, 4) for k, v in prof.items()}}
+
+    e2e = run_e2e(args, sc, dev) if (rank == 0 and not args.no_e2e) else None
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(sc, args.cpu_budget_s, 200)
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {**workload_config(sc, args.workload), "parallelism": f"replicas x{world}",
+                           "lanes_per_particle": args.lanes},
+                "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
+                "valid": bool(valid), "max_final_density_error": raw.max_final_density_error,
+                "outer_iters_per_step": raw.sum_outer_iters / args.steps,
+                "cg_iters_per_step": raw.sum_pcg_iters / args.steps,
+                "mean_neighbours": pairs / max(sc.n_dynamic, 1),
+                "wall_s": wall, "gpu_launches": int(n_launch), "clocks": clk, "roofline": roof,
+                "cpu_baseline": cpu, "e2e": e2e}
+        print(json.dumps(line), flush=True)
+
+
+def run_e2e(args, sc, dev):
+    """Same metric through the public API (SimulationData + Framework.forward)
+    with the step's state coming from and going back to pinned host memory."""
+    import torch
+    from implicitvelocityprojection_b200.config import SimConfig
+    from implicitvelocityprojection_b200.framework import Framework
+    from implicitvelocityprojection_b200.neighbour_search import NeighbourSearch
+    from implicitvelocityprojection_b200.simulation_data import SimulationData
+    cfg = SimConfig.from_scene(sc)
+    ps = SimulationData.from_scene(sc, cfg, device=str(dev))
+    ns = NeighbourSearch(cfg.domain_size, cfg.support_radius, ps)
+    fw = Framework(ps, ns, cfg)
+    fw.initialize()
+    n = ps.particle_num
+    x_h = torch.empty((n, 3), dtype=torch.float32).pin_memory()
+    v_h = torch.empty((n, 3), dtype=torch.float32).pin_memory()
+    x_h.copy_(ps.x[:n])
+    v_h.copy_(ps.v[:n])
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    steps = max(1, min(args.steps, args.e2e_steps))
+    for _ in range(min(args.warmup, 3)):
+        ps.x[:n].copy_(x_h, non_blocking=True)
+        ps.v[:n].copy_(v_h, non_blocking=True)
+        fw.forward()
+        x_h.copy_(ps.x[:n])
+        v_h.copy_(ps.v[:n])
+    tot = 0.0
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ps.x[:n].copy_(x_h, non_blocking=True)
+        ps.v[:n].copy_(v_h, non_blocking=True)
+        fw.forward()  # raises on a failed solve; reads the stats (one sync)
+        x_h.copy_(ps.x[:n], non_blocking=True)
+        v_h.copy_(ps.v[:n], non_blocking=True)
+        torch.cuda.synchronize()
+        tot += time.perf_counter() - t0
+    return {"value": sc.n_dynamic * steps / tot, "unit": UNIT, "h2d_bytes_per_step": 2 * n * 12,
+            "d2h_bytes_per_step": 2 * n * 12 + 256, "steps": steps,
+            "api": "Framework.forward() with x, v copied from/to pinned host memory every step"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="tall_column")
+    ap.add_argument("--lanes", type=int, default=4)
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--cpu-budget-s", type=float, default=12.0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(local_rank)
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device("cuda", local_rank))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

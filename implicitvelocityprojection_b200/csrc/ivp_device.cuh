@@ -1,0 +1,227 @@
+// ivp_device.cuh -- device data layout and helpers of the IP pressure step.
+//
+// Layout in HBM (one engine = one or more independent scenes):
+//   * bound particle arrays, caller order (SimulationData layout): x, v, m,
+//     density0, is_dynamic, material; outputs density, k;
+//   * slots: every particle gets one slot per rebuild; slots are ordered by
+//     (scene, dynamic-before-static, cell, particle id).  Scene s owns slots
+//     [s_begin, s_end), its dynamic particles [s_begin, s_dyn_end).  Because
+//     of that order "j is dynamic" is `j < s_dyn_end` (no load), and the
+//     vector arrays of the solver hold exact zeros at static slots, which
+//     makes the reference's `[dyn j]` branches (ip.py:55-58, 160-163,
+//     209-213) branch-free with identical rounding;
+//   * per-slot arrays: xm (float4 x,y,z,m), rest density, density, k, c, and
+//     the solver vectors as float4 (16-byte gathers);
+//   * neighbour rows, one per dynamic particle, `stride` entries of int2
+//     {neighbour slot, kernel-gradient weight w} with
+//     grad W_ij = w_ij (x_i - x_j), i.e. the spiky gradient of
+//     sph_kernel.py:52-61 factored as a scalar times the separation;
+//   * tiles: (scene, first slot, end slot, first row) -- a CTA never spans
+//     two scenes, so per-scene reductions are per-CTA partials summed in a
+//     fixed order by the scene's last CTA (deterministic FP64).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ivp {
+
+constexpr int kMaxHistDefault = 128;
+
+struct SceneParams {
+    int p_begin, p_end;        // particle range in the bound arrays
+    int s_begin, s_dyn_end, s_end;
+    int n_dyn;
+    int row_base;              // first neighbour row of this scene
+    int key_base;              // keys [key_base, key_base + 2*ncell): dynamic cells, then static cells
+    int dims[3];
+    int ncell;
+    float cell_inv;            // 1/h (cell size = support radius, neighbour_search.py:105-107)
+    float h;
+    float dt, inv_dt, omega, padding;
+    float domain[3];
+    float gravity[3];
+    float W0;                  // cubic_kernel(0, h)
+    float cubic_k;             // 8/pi / h^3 (sph_kernel.py:14-15)
+    float spiky_k;             // 45 / (pi h^6) (sph_kernel.py:55)
+    float visc_coeff;
+    int visc_method;
+    int max_outer, max_pcg, fixed_iters, cache;
+    int tile_begin, tile_end;
+    int hist_base;
+    double tol_opt, tol_pcg;
+};
+
+// Per-scene solver control block, written only by the scene's last CTA of a
+// launch and read by every CTA of the next launch.
+struct SceneCtl {
+    double err;          // last average density error
+    double rr_old;
+    double pap;
+    double alpha;
+    double beta;
+    double final_err;
+    double rr0;
+    int outer_it;        // updates applied (stats_outer_iters)
+    int cg_it;
+    int outer_active;
+    int solve_pending;
+    int cg_active;
+    int status;
+    int n_err;
+    int total_cg;
+    // sticky counters since the last reset (ivp_reset_counters)
+    double acc_max_final_err;
+    int acc_solves;
+    int acc_outer;
+    int acc_cg;
+    int acc_failed;
+    int acc_last_failure;
+    int acc_pad;
+};
+
+struct Flags {
+    int any_outer, any_solve, any_cg, bad;
+    int bad_index, bad_where;
+    // loop guard: decision launches of the current solve and their budget;
+    // past the budget every active scene stops with IVP_ERR_TIMEOUT, so a
+    // control-flow fault cannot keep a conditional graph loop running
+    int launches, limit;
+    int timeout, pad0, pad1, pad2;
+};
+
+struct Dev {
+    // bound arrays (caller order)
+    float* x;
+    float* v;
+    const float* m;
+    const float* rho0;
+    const int* dyn;
+    const int* material;
+    float* density_out;
+    float* k_out;
+    float* div_out;
+    int n_total;
+    // tables
+    const SceneParams* scenes;
+    int n_scenes;
+    SceneCtl* ctl;
+    const int4* tiles;       // (scene, slot begin, slot end, row begin)
+    int n_tiles;
+    const int* pscene;       // scene of each particle
+    // sort
+    int* key;
+    int* rank;
+    int* cell_count;
+    int* cell_start;         // n_keys + 1
+    int* block_sums;
+    int n_keys;
+    int* placed;             // slot -> particle (unstable within a cell)
+    int* pid;                // slot -> particle (stable)
+    int* inv;                // particle -> slot
+    int* overflow;           // per scene
+    unsigned long long* pairs;  // per scene: neighbour pairs of the last build
+    // per slot
+    float4* xm;
+    float* rho0s;
+    float* dens;
+    float* kd;
+    float* c;
+    float4* d0;
+    float4* d1;
+    float4* sol;
+    float4* r;
+    float4* p0;
+    float4* p1;
+    float* y;
+    float* s;
+    float* fk;
+    // neighbour rows
+    int2* nbr;
+    int* nbr_cnt;
+    int stride;
+    // reductions
+    double* partial;
+    int* scene_counter;
+    int* launch_counter;
+    Flags* flags;
+    double* err_hist;
+    int* pcg_hist;
+    int hist_len;
+    // graph conditionals (0 = not inside a conditional graph)
+    unsigned long long h_outer, h_solve, h_cg;
+    // advect leaves scenes whose last solve raised where they are (the
+    // reference raises before advecting, framework.py:483-513)
+    int advect_skip_failed;
+};
+
+// ------------------------------------------------------------------ math
+
+__device__ __forceinline__ float3 f3(float4 a) { return make_float3(a.x, a.y, a.z); }
+__device__ __forceinline__ float3 sub3(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 scale3(float s, float3 a) { return make_float3(s * a.x, s * a.y, s * a.z); }
+
+// sph_kernel.py:8-25 (cubic spline, FP32 operation order of the reference)
+__device__ __forceinline__ float cubic_W(float r, float h, float k) {
+    float res = 0.0f;
+    float q = r / h;
+    if (q <= 1.0f) {
+        if (q <= 0.5f) {
+            float q2 = q * q;
+            float q3 = q2 * q;
+            res = k * (6.0f * q3 - 6.0f * q2 + 1.0f);
+        } else {
+            float f = 1.0f - q;
+            res = k * 2.0f * f * f * f;
+        }
+    }
+    return res;
+}
+
+// sph_kernel.py:52-61 as a weight: grad W(r) = w * r with
+// w = -k (h - |r|)^2 / max(|r|, 1e-6)
+__device__ __forceinline__ float spiky_w(float rn, float h, float k) {
+    float rc = rn < 1e-6f ? 1e-6f : rn;
+    float t = h - rc;
+    return (-k * (t * t)) / rc;
+}
+
+__device__ __forceinline__ int cell_coord(float v, float inv, int dim) {
+    float c = floorf(v * inv);
+    c = fmaxf(c, 0.0f);                       // NaN -> 0
+    c = fminf(c, (float)(dim - 1));
+    return (int)c;
+}
+
+template <int G>
+__device__ __forceinline__ float group_sum(float v) {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Deterministic block sum (fixed tree), result valid in every thread.
+template <int BLOCK>
+__device__ __forceinline__ double block_sum_d(double v, double* sh) {
+    v = warp_sum_d(v);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) sh[w] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x < 32) {
+        t = (l < BLOCK / 32) ? sh[l] : 0.0;
+        t = warp_sum_d(t);
+        if (l == 0) sh[0] = t;
+    }
+    __syncthreads();
+    return sh[0];
+}
+
+}  // namespace ivp

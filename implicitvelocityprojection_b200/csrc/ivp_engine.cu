@@ -1,0 +1,837 @@
+// ivp_engine.cu -- host side of the IP pressure-step engine and its C ABI
+// (include/ivp.h).  No device allocation after ivp_engine_create: every
+// buffer is carved from the caller's workspace.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/ivp.h"
+#include "ivp_kernels.cuh"
+
+using namespace ivp;
+
+namespace {
+
+thread_local std::string g_err;
+
+#define CK(x)                                                                 \
+    do {                                                                      \
+        cudaError_t e_ = (x);                                                 \
+        if (e_ != cudaSuccess) {                                              \
+            g_err = std::string(#x) + ": " + cudaGetErrorString(e_);          \
+            return IVP_ERR_CUDA;                                              \
+        }                                                                     \
+    } while (0)
+
+#define CKS(x)                          \
+    do {                                \
+        int s_ = (x);                   \
+        if (s_ != IVP_OK) return s_;    \
+    } while (0)
+
+inline size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+struct Layout {
+    size_t total = 0;
+    size_t add(size_t bytes) {
+        size_t off = total;
+        total = align256(total + bytes);
+        return off;
+    }
+};
+
+constexpr int ELEM_BLOCK = 256;
+
+inline int blocks_for(int n, int b) { return (n + b - 1) / b; }
+
+}  // namespace
+
+struct ivp_engine {
+    std::vector<ivp_scene_desc> desc;
+    std::vector<SceneParams> hp;
+    std::vector<int4> tiles;
+    ivp_options opt{};
+    Dev D{};
+    int G = 4, BLOCK = 128, T = 32;
+    int n_total = 0, n_dyn_total = 0, n_keys = 0, n_tiles = 0, scan_blocks = 0;
+    int n_scenes = 0;
+    bool bound = false;
+    bool want_divergence = false;
+    // graphs
+    cudaGraph_t graph_step = nullptr, graph_solve = nullptr, graph_build = nullptr;
+    cudaGraphExec_t exec_step = nullptr, exec_solve = nullptr, exec_build = nullptr;
+    // host mirrors
+    SceneCtl* h_ctl = nullptr;   // pinned
+    Flags* h_flags = nullptr;    // pinned
+    int* h_overflow = nullptr;   // pinned
+    unsigned long long* h_pairs = nullptr;  // pinned
+};
+
+// ------------------------------------------------------------ launching
+
+namespace {
+
+typedef void (*DevKernel)(const Dev);
+
+// Per-launch CUDA events of a profiled host-driven run.
+struct Prof {
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> ids;
+    ~Prof() {
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    }
+};
+
+struct Launcher {
+    // Either launches on a stream or appends a kernel node to a graph chain.
+    cudaStream_t stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphNode_t last = nullptr;
+    bool has_last = false;
+    Prof* prof = nullptr;
+
+    int kernel(int id, const void* fn, dim3 grid, dim3 block, void** args) {
+        if (grid.x == 0) return IVP_OK;
+        if (!graph) {
+            if (prof) {
+                const size_t k = prof->ids.size();
+                while (prof->ev.size() < 2 * (k + 1)) {
+                    cudaEvent_t ev;
+                    CK(cudaEventCreate(&ev));
+                    prof->ev.push_back(ev);
+                }
+                CK(cudaEventRecord(prof->ev[2 * k], stream));
+                CK(cudaLaunchKernel(fn, grid, block, args, 0, stream));
+                CK(cudaEventRecord(prof->ev[2 * k + 1], stream));
+                prof->ids.push_back(id);
+                return IVP_OK;
+            }
+            CK(cudaLaunchKernel(fn, grid, block, args, 0, stream));
+            return IVP_OK;
+        }
+        cudaKernelNodeParams p;
+        memset(&p, 0, sizeof(p));
+        p.func = const_cast<void*>(fn);
+        p.gridDim = grid;
+        p.blockDim = block;
+        p.sharedMemBytes = 0;
+        p.kernelParams = args;
+        p.extra = nullptr;
+        cudaGraphNode_t n;
+        CK(cudaGraphAddKernelNode(&n, graph, has_last ? &last : nullptr, has_last ? 1 : 0, &p));
+        last = n;
+        has_last = true;
+        return IVP_OK;
+    }
+    int dev(int id, DevKernel fn, int grid, int block, const Dev& D) {
+        Dev copy = D;
+        void* args[] = {&copy};
+        return kernel(id, (const void*)fn, dim3(grid), dim3(block), args);
+    }
+    int memset0(void* ptr, size_t bytes) {
+        if (bytes == 0) return IVP_OK;
+        if (!graph) {
+            CK(cudaMemsetAsync(ptr, 0, bytes, stream));
+            return IVP_OK;
+        }
+        cudaMemsetParams mp;
+        memset(&mp, 0, sizeof(mp));
+        mp.dst = ptr;
+        mp.value = 0;
+        mp.elementSize = 1;
+        mp.width = bytes;
+        mp.height = 1;
+        mp.pitch = 0;
+        cudaGraphNode_t n;
+        CK(cudaGraphAddMemsetNode(&n, graph, has_last ? &last : nullptr, has_last ? 1 : 0, &mp));
+        last = n;
+        has_last = true;
+        return IVP_OK;
+    }
+};
+
+template <int G, int BLOCK>
+struct Kern {
+    static DevKernel pack() { return k_pack<G, BLOCK>; }
+    static DevKernel rhs() { return k_rhs<G, BLOCK>; }
+    static DevKernel cg_a() { return k_cg_a<G, BLOCK>; }
+    static DevKernel cg_b() { return k_cg_b<G, BLOCK>; }
+    static DevKernel dens() { return k_density<G, BLOCK>; }
+    static DevKernel aii() { return k_aii<G, BLOCK>; }
+    static DevKernel div() { return k_divergence<G, BLOCK>; }
+};
+
+struct KernelSet {
+    DevKernel pack, rhs, cg_a, cg_b, dens, aii, div;
+};
+
+template <int G>
+KernelSet make_set() {
+    constexpr int B = 128;
+    return {Kern<G, B>::pack(), Kern<G, B>::rhs(), Kern<G, B>::cg_a(), Kern<G, B>::cg_b(),
+            Kern<G, B>::dens(), Kern<G, B>::aii(), Kern<G, B>::div()};
+}
+
+bool kernel_set(int G, KernelSet* out) {
+    switch (G) {
+        case 1: *out = make_set<1>(); return true;
+        case 2: *out = make_set<2>(); return true;
+        case 4: *out = make_set<4>(); return true;
+        case 8: *out = make_set<8>(); return true;
+        default: return false;
+    }
+}
+
+int emit_build(ivp_engine* e, Launcher& L) {
+    const Dev& D = e->D;
+    CKS(L.memset0(D.cell_count, sizeof(int) * (size_t)e->n_keys));
+    CKS(L.memset0(D.overflow, sizeof(int) * (size_t)e->n_scenes));
+    CKS(L.memset0(D.pairs, sizeof(unsigned long long) * (size_t)e->n_scenes));
+    CKS(L.dev(IVP_K_KEYS, k_keys, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D));
+    {
+        int* in = D.cell_count;
+        int* out = D.cell_start;
+        int* bs = D.block_sums;
+        int n = e->n_keys;
+        void* a1[] = {&in, &out, &bs, &n};
+        CKS(L.kernel(IVP_K_SCAN_LOCAL, (const void*)k_scan_local, dim3(e->scan_blocks), dim3(SCAN_BLOCK), a1));
+        int nb = e->scan_blocks;
+        void* a2[] = {&out, &bs, &n, &nb};
+        CKS(L.kernel(IVP_K_SCAN_ADD, (const void*)k_scan_add, dim3(e->scan_blocks), dim3(SCAN_BLOCK), a2));
+    }
+    CKS(L.dev(IVP_K_PLACE, k_place, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D));
+    CKS(L.dev(IVP_K_ORDER, k_order, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D));
+    CKS(L.dev(IVP_K_NBR_BUILD, k_nbr_build, e->n_tiles, e->T, D));
+    CKS(L.dev(IVP_K_STATIC_OUT, k_static_outputs, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D));
+    return IVP_OK;
+}
+
+int add_conditional(cudaGraph_t g, Launcher& L, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type,
+                    cudaGraph_t* body) {
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+    cp.conditional.handle = h;
+    cp.conditional.type = type;
+    cp.conditional.size = 1;
+    cudaGraphNode_t n;
+    CK(cudaGraphAddNode(&n, g, L.has_last ? &L.last : nullptr, L.has_last ? 1 : 0, &cp));
+    *body = cp.conditional.phGraph_out[0];
+    L.last = n;
+    L.has_last = true;
+    return IVP_OK;
+}
+
+// The IP outer loop and its CG, either as nested conditional graph nodes
+// (device-side control) or driven from the host with flag read-backs.
+int emit_solve_loop(ivp_engine* e, Launcher& L) {
+    KernelSet K;
+    if (!kernel_set(e->G, &K)) return IVP_ERR_BAD_ARG;
+    const int nt = e->n_tiles, B = e->BLOCK;
+    if (nt == 0) return IVP_OK;
+    if (!L.graph) {
+        // host-driven: one flag read-back after each decision launch
+        for (int guard = 0; guard < 1000000; ++guard) {
+            CKS(L.dev(IVP_K_PACK, K.pack, nt, B, e->D));
+            CK(cudaMemcpyAsync(e->h_flags, e->D.flags, sizeof(Flags), cudaMemcpyDeviceToHost, L.stream));
+            CK(cudaStreamSynchronize(L.stream));
+            if (!e->h_flags->any_outer) break;
+            if (!e->h_flags->any_solve) continue;
+            CKS(L.dev(IVP_K_RHS, K.rhs, nt, B, e->D));
+            CK(cudaMemcpyAsync(e->h_flags, e->D.flags, sizeof(Flags), cudaMemcpyDeviceToHost, L.stream));
+            CK(cudaStreamSynchronize(L.stream));
+            for (int cg_guard = 0; e->h_flags->any_cg && cg_guard < 1000000; ++cg_guard) {
+                CKS(L.dev(IVP_K_CG_A, K.cg_a, nt, B, e->D));
+                CKS(L.dev(IVP_K_CG_B, K.cg_b, nt, B, e->D));
+                CK(cudaMemcpyAsync(e->h_flags, e->D.flags, sizeof(Flags), cudaMemcpyDeviceToHost, L.stream));
+                CK(cudaStreamSynchronize(L.stream));
+            }
+        }
+        return IVP_OK;
+    }
+    cudaGraphConditionalHandle h_outer, h_solve, h_cg;
+    CK(cudaGraphConditionalHandleCreate(&h_outer, L.graph, 1, cudaGraphCondAssignDefault));
+    cudaGraph_t body_outer, body_solve, body_cg;
+    CKS(add_conditional(L.graph, L, h_outer, cudaGraphCondTypeWhile, &body_outer));
+    CK(cudaGraphConditionalHandleCreate(&h_solve, body_outer, 0, 0));
+    Launcher Lo;
+    Lo.graph = body_outer;
+    {
+        Dev d = e->D;
+        d.h_outer = (unsigned long long)h_outer;
+        d.h_solve = (unsigned long long)h_solve;
+        CKS(Lo.dev(IVP_K_PACK, K.pack, nt, B, d));
+    }
+    CKS(add_conditional(body_outer, Lo, h_solve, cudaGraphCondTypeIf, &body_solve));
+    CK(cudaGraphConditionalHandleCreate(&h_cg, body_solve, 0, 0));
+    Launcher Ls;
+    Ls.graph = body_solve;
+    {
+        Dev d = e->D;
+        d.h_cg = (unsigned long long)h_cg;
+        CKS(Ls.dev(IVP_K_RHS, K.rhs, nt, B, d));
+    }
+    CKS(add_conditional(body_solve, Ls, h_cg, cudaGraphCondTypeWhile, &body_cg));
+    Launcher Lc;
+    Lc.graph = body_cg;
+    {
+        Dev d = e->D;
+        d.h_cg = (unsigned long long)h_cg;
+        CKS(Lc.dev(IVP_K_CG_A, K.cg_a, nt, B, d));
+        CKS(Lc.dev(IVP_K_CG_B, K.cg_b, nt, B, d));
+    }
+    return IVP_OK;
+}
+
+int emit_solve(ivp_engine* e, Launcher& L) {
+    if (e->n_tiles == 0) return IVP_OK;
+    CKS(L.dev(IVP_K_SOLVE_BEGIN, k_solve_begin, e->n_tiles, e->T, e->D));
+    CKS(emit_solve_loop(e, L));
+    CKS(L.dev(IVP_K_SOLVE_END, k_solve_end, e->n_tiles, e->T, e->D));
+    if (e->want_divergence && e->D.div_out) {
+        KernelSet K;
+        kernel_set(e->G, &K);
+        CKS(L.dev(IVP_K_DIVERGENCE, K.div, e->n_tiles, e->BLOCK, e->D));
+    }
+    return IVP_OK;
+}
+
+int emit_advect(ivp_engine* e, Launcher& L) {
+    return L.dev(IVP_K_ADVECT, k_advect, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, e->D);
+}
+
+int emit_step(ivp_engine* e, Launcher& L) {
+    CKS(L.dev(IVP_K_GRAVITY, k_gravity, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, e->D));
+    CKS(emit_solve(e, L));
+    {
+        Dev d = e->D;
+        d.advect_skip_failed = 1;
+        CKS(L.dev(IVP_K_ADVECT, k_advect, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, d));
+    }
+    CKS(emit_build(e, L));
+    return IVP_OK;
+}
+
+void destroy_graphs(ivp_engine* e) {
+    if (e->exec_step) cudaGraphExecDestroy(e->exec_step);
+    if (e->exec_solve) cudaGraphExecDestroy(e->exec_solve);
+    if (e->exec_build) cudaGraphExecDestroy(e->exec_build);
+    if (e->graph_step) cudaGraphDestroy(e->graph_step);
+    if (e->graph_solve) cudaGraphDestroy(e->graph_solve);
+    if (e->graph_build) cudaGraphDestroy(e->graph_build);
+    e->exec_step = e->exec_solve = e->exec_build = nullptr;
+    e->graph_step = e->graph_solve = e->graph_build = nullptr;
+}
+
+typedef int (*Emitter)(ivp_engine*, Launcher&);
+
+int make_graph(ivp_engine* e, Emitter emit, cudaGraph_t* g, cudaGraphExec_t* x) {
+    CK(cudaGraphCreate(g, 0));
+    Launcher L;
+    L.graph = *g;
+    int st = emit(e, L);
+    if (st != IVP_OK) return st;
+    CK(cudaGraphInstantiate(x, *g, 0));
+    return IVP_OK;
+}
+
+int run(ivp_engine* e, Emitter emit, cudaGraph_t* g, cudaGraphExec_t* x, cudaStream_t s) {
+    if (!e->bound) return IVP_ERR_NOT_BOUND;
+    if (e->opt.use_graphs) {
+        if (!*x) CKS(make_graph(e, emit, g, x));
+        CK(cudaGraphLaunch(*x, s));
+        return IVP_OK;
+    }
+    Launcher L;
+    L.stream = s;
+    return emit(e, L);
+}
+
+int validate(const ivp_scene_desc* sc, int n, const ivp_options* o) {
+    if (n <= 0 || !sc || !o) return IVP_ERR_BAD_ARG;
+    if (o->lanes_per_particle != 1 && o->lanes_per_particle != 2 && o->lanes_per_particle != 4 &&
+        o->lanes_per_particle != 8)
+        return IVP_ERR_BAD_ARG;
+    if (o->particles_per_block <= 0 || o->particles_per_block * o->lanes_per_particle != 128) return IVP_ERR_BAD_ARG;
+    if (o->list_stride <= 0 || o->max_hist <= 0) return IVP_ERR_BAD_ARG;
+    long expect = 0;
+    for (int s = 0; s < n; ++s) {
+        const ivp_scene_desc& d = sc[s];
+        // scenes tile the particle arrays in order, without gaps
+        if (d.particle_offset != expect) return IVP_ERR_BAD_ARG;
+        expect += d.n_particles;
+        if (expect > 0x7fffffffL) return IVP_ERR_BAD_ARG;
+        if (d.n_particles < 0 || d.n_dynamic < 0 || d.n_dynamic > d.n_particles) return IVP_ERR_BAD_ARG;
+        if (!(d.particle_radius > 0.0f) || !(d.dt > 0.0f)) return IVP_ERR_BAD_ARG;
+        if (d.cache_size <= 0 || d.cache_size > o->list_stride) return IVP_ERR_BAD_ARG;
+        for (int a = 0; a < 3; ++a)
+            if (!(d.domain_size[a] > 0.0f)) return IVP_ERR_BAD_ARG;
+        if (d.max_outer_iters < 0 || d.max_iteration_pcg < 0) return IVP_ERR_BAD_ARG;
+    }
+    return IVP_OK;
+}
+
+struct Plan {
+    std::vector<SceneParams> hp;
+    std::vector<int4> tiles;
+    int n_total = 0, n_dyn = 0, n_keys = 0, scan_blocks = 0;
+    size_t off[40];
+    Layout lay;
+};
+
+void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
+    const int T = o->particles_per_block;
+    int s_begin = 0, row_base = 0, key_base = 0;
+    P.hp.resize(n);
+    for (int s = 0; s < n; ++s) {
+        const ivp_scene_desc& d = sc[s];
+        SceneParams& q = P.hp[s];
+        memset(&q, 0, sizeof(q));
+        q.p_begin = d.particle_offset;
+        q.p_end = d.particle_offset + d.n_particles;
+        q.s_begin = s_begin;
+        q.s_dyn_end = s_begin + d.n_dynamic;
+        q.s_end = s_begin + d.n_particles;
+        q.n_dyn = d.n_dynamic;
+        q.row_base = row_base;
+        const float h = 4.0f * d.particle_radius;  // config_builder.py:51-52
+        q.h = h;
+        q.cell_inv = 1.0f / h;
+        long ncell = 1;
+        for (int a = 0; a < 3; ++a) {
+            // neighbour_search.py:105-107
+            int dim = (int)std::ceil((double)d.domain_size[a] / (double)h);
+            q.dims[a] = dim < 1 ? 1 : dim;
+            ncell *= q.dims[a];
+            q.domain[a] = d.domain_size[a];
+            q.gravity[a] = d.gravity[a];
+        }
+        q.ncell = (int)ncell;
+        q.key_base = key_base;
+        q.dt = d.dt;
+        q.inv_dt = (float)(1.0 / (double)d.dt);
+        q.omega = d.omega;
+        q.padding = h;
+        float k = 8.0f / 3.14159265359f;
+        k = k / (h * h * h);
+        q.cubic_k = k;
+        q.W0 = k * (6.0f * 0.0f - 6.0f * 0.0f + 1.0f);
+        q.spiky_k = 45.0f / (3.14159265359f * h * h * h * h * h * h);
+        q.visc_coeff = d.viscosity_coeff;
+        q.visc_method = d.viscosity_method;
+        q.max_outer = d.max_outer_iters;
+        q.max_pcg = d.max_iteration_pcg;
+        q.fixed_iters = d.fixed_outer_iters;
+        q.cache = d.cache_size;
+        q.tol_opt = d.density_error_tol;
+        q.tol_pcg = d.tol_pcg;
+        q.hist_base = s * o->max_hist;
+        q.tile_begin = (int)P.tiles.size();
+        for (int b = 0; b < d.n_dynamic; b += T) {
+            int e = std::min(b + T, d.n_dynamic);
+            P.tiles.push_back(make_int4(s, s_begin + b, s_begin + e, row_base + b));
+        }
+        q.tile_end = (int)P.tiles.size();
+        s_begin += d.n_particles;
+        row_base += d.n_dynamic;
+        key_base += 2 * (int)ncell;
+    }
+    P.n_total = s_begin;
+    P.n_dyn = row_base;
+    P.n_keys = key_base;
+    P.scan_blocks = std::max(1, (P.n_keys + SCAN_TILE - 1) / SCAN_TILE);
+    const size_t N = (size_t)P.n_total, S = (size_t)n, NT = std::max<size_t>(P.tiles.size(), 1);
+    Layout& L = P.lay;
+    int i = 0;
+    P.off[i++] = L.add(sizeof(SceneParams) * S);            // 0 scenes
+    P.off[i++] = L.add(sizeof(SceneCtl) * S);               // 1 ctl
+    P.off[i++] = L.add(sizeof(int4) * NT);                  // 2 tiles
+    P.off[i++] = L.add(sizeof(int) * N);                    // 3 pscene
+    P.off[i++] = L.add(sizeof(int) * N);                    // 4 key
+    P.off[i++] = L.add(sizeof(int) * N);                    // 5 rank
+    P.off[i++] = L.add(sizeof(int) * (size_t)P.n_keys);     // 6 cell_count
+    P.off[i++] = L.add(sizeof(int) * ((size_t)P.n_keys + 1));  // 7 cell_start
+    P.off[i++] = L.add(sizeof(int) * (size_t)P.scan_blocks);   // 8 block_sums
+    P.off[i++] = L.add(sizeof(int) * N);                    // 9 placed
+    P.off[i++] = L.add(sizeof(int) * N);                    // 10 pid
+    P.off[i++] = L.add(sizeof(int) * N);                    // 11 inv
+    P.off[i++] = L.add(sizeof(int) * S);                    // 12 overflow
+    P.off[i++] = L.add(sizeof(float4) * N);                 // 13 xm
+    P.off[i++] = L.add(sizeof(float) * N);                  // 14 rho0s
+    P.off[i++] = L.add(sizeof(float) * N);                  // 15 dens
+    P.off[i++] = L.add(sizeof(float) * N);                  // 16 kd
+    P.off[i++] = L.add(sizeof(float) * N);                  // 17 c
+    P.off[i++] = L.add(sizeof(float4) * N);                 // 18 d0
+    P.off[i++] = L.add(sizeof(float4) * N);                 // 19 d1
+    P.off[i++] = L.add(sizeof(float4) * N);                 // 20 sol
+    P.off[i++] = L.add(sizeof(float4) * N);                 // 21 r
+    P.off[i++] = L.add(sizeof(float4) * N);                 // 22 p0
+    P.off[i++] = L.add(sizeof(float4) * N);                 // 23 p1
+    P.off[i++] = L.add(sizeof(float) * N);                  // 24 y
+    P.off[i++] = L.add(sizeof(float) * N);                  // 25 s
+    P.off[i++] = L.add(sizeof(float) * N);                  // 26 fk
+    P.off[i++] = L.add(sizeof(int2) * (size_t)P.n_dyn * (size_t)o->list_stride);  // 27 nbr
+    P.off[i++] = L.add(sizeof(int) * std::max<size_t>((size_t)P.n_dyn, 1));       // 28 nbr_cnt
+    P.off[i++] = L.add(sizeof(double) * NT);                // 29 partial
+    P.off[i++] = L.add(sizeof(int) * S);                    // 30 scene_counter
+    P.off[i++] = L.add(sizeof(int));                        // 31 launch_counter
+    P.off[i++] = L.add(sizeof(Flags));                      // 32 flags
+    P.off[i++] = L.add(sizeof(double) * S * (size_t)o->max_hist);  // 33 err_hist
+    P.off[i++] = L.add(sizeof(int) * S * (size_t)o->max_hist);     // 34 pcg_hist
+    P.off[i++] = L.add(sizeof(unsigned long long) * S);            // 35 pairs
+}
+
+cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+}  // namespace
+
+// ================================================================ C ABI
+
+extern "C" {
+
+void ivp_default_options(ivp_options* o) {
+    memset(o, 0, sizeof(*o));
+    o->lanes_per_particle = 4;
+    o->particles_per_block = 32;
+    o->list_stride = 64;
+    o->max_hist = kMaxHistDefault;
+    o->use_graphs = 1;
+}
+
+int ivp_workspace_bytes(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_options* opt, size_t* bytes) {
+    CKS(validate(scenes, n_scenes, opt));
+    if (!bytes) return IVP_ERR_BAD_ARG;
+    Plan P;
+    plan(scenes, n_scenes, opt, P);
+    *bytes = P.lay.total;
+    return IVP_OK;
+}
+
+int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_options* opt, void* workspace,
+                      size_t workspace_bytes, void* stream, ivp_engine** out) {
+    if (!out || !workspace) return IVP_ERR_BAD_ARG;
+    *out = nullptr;
+    CKS(validate(scenes, n_scenes, opt));
+    if (reinterpret_cast<uintptr_t>(workspace) & 255) return IVP_ERR_BAD_ARG;
+    Plan P;
+    plan(scenes, n_scenes, opt, P);
+    if (workspace_bytes < P.lay.total) return IVP_ERR_BAD_ARG;
+    cudaStream_t s = as_stream(stream);
+    ivp_engine* e = new ivp_engine();
+    e->desc.assign(scenes, scenes + n_scenes);
+    e->hp = P.hp;
+    e->tiles = P.tiles;
+    e->opt = *opt;
+    e->G = opt->lanes_per_particle;
+    e->T = opt->particles_per_block;
+    e->BLOCK = e->G * e->T;
+    e->n_total = P.n_total;
+    e->n_dyn_total = P.n_dyn;
+    e->n_keys = P.n_keys;
+    e->n_tiles = (int)P.tiles.size();
+    e->scan_blocks = P.scan_blocks;
+    e->n_scenes = n_scenes;
+    char* w = static_cast<char*>(workspace);
+    Dev& D = e->D;
+    int i = 0;
+    D.scenes = reinterpret_cast<SceneParams*>(w + P.off[i++]);
+    D.ctl = reinterpret_cast<SceneCtl*>(w + P.off[i++]);
+    D.tiles = reinterpret_cast<int4*>(w + P.off[i++]);
+    D.pscene = reinterpret_cast<int*>(w + P.off[i++]);
+    D.key = reinterpret_cast<int*>(w + P.off[i++]);
+    D.rank = reinterpret_cast<int*>(w + P.off[i++]);
+    D.cell_count = reinterpret_cast<int*>(w + P.off[i++]);
+    D.cell_start = reinterpret_cast<int*>(w + P.off[i++]);
+    D.block_sums = reinterpret_cast<int*>(w + P.off[i++]);
+    D.placed = reinterpret_cast<int*>(w + P.off[i++]);
+    D.pid = reinterpret_cast<int*>(w + P.off[i++]);
+    D.inv = reinterpret_cast<int*>(w + P.off[i++]);
+    D.overflow = reinterpret_cast<int*>(w + P.off[i++]);
+    D.xm = reinterpret_cast<float4*>(w + P.off[i++]);
+    D.rho0s = reinterpret_cast<float*>(w + P.off[i++]);
+    D.dens = reinterpret_cast<float*>(w + P.off[i++]);
+    D.kd = reinterpret_cast<float*>(w + P.off[i++]);
+    D.c = reinterpret_cast<float*>(w + P.off[i++]);
+    D.d0 = reinterpret_cast<float4*>(w + P.off[i++]);
+    D.d1 = reinterpret_cast<float4*>(w + P.off[i++]);
+    D.sol = reinterpret_cast<float4*>(w + P.off[i++]);
+    D.r = reinterpret_cast<float4*>(w + P.off[i++]);
+    D.p0 = reinterpret_cast<float4*>(w + P.off[i++]);
+    D.p1 = reinterpret_cast<float4*>(w + P.off[i++]);
+    D.y = reinterpret_cast<float*>(w + P.off[i++]);
+    D.s = reinterpret_cast<float*>(w + P.off[i++]);
+    D.fk = reinterpret_cast<float*>(w + P.off[i++]);
+    D.nbr = reinterpret_cast<int2*>(w + P.off[i++]);
+    D.nbr_cnt = reinterpret_cast<int*>(w + P.off[i++]);
+    D.partial = reinterpret_cast<double*>(w + P.off[i++]);
+    D.scene_counter = reinterpret_cast<int*>(w + P.off[i++]);
+    D.launch_counter = reinterpret_cast<int*>(w + P.off[i++]);
+    D.flags = reinterpret_cast<Flags*>(w + P.off[i++]);
+    D.err_hist = reinterpret_cast<double*>(w + P.off[i++]);
+    D.pcg_hist = reinterpret_cast<int*>(w + P.off[i++]);
+    D.pairs = reinterpret_cast<unsigned long long*>(w + P.off[i++]);
+    D.n_scenes = n_scenes;
+    D.n_tiles = e->n_tiles;
+    D.n_keys = e->n_keys;
+    D.stride = opt->list_stride;
+    D.hist_len = opt->max_hist;
+    D.n_total = e->n_total;
+
+    auto fail = [&](int code) {
+        ivp_engine_destroy(e);
+        return code;
+    };
+    if (cudaMemsetAsync(workspace, 0, P.lay.total, s) != cudaSuccess) return fail(IVP_ERR_CUDA);
+    std::vector<int> pscene(e->n_total);
+    for (int sc = 0; sc < n_scenes; ++sc)
+        for (int p = P.hp[sc].p_begin; p < P.hp[sc].p_end; ++p) {
+            if (p < 0 || p >= e->n_total) return fail(IVP_ERR_BAD_ARG);
+            pscene[p] = sc;
+        }
+    if (cudaHostAlloc((void**)&e->h_ctl, sizeof(SceneCtl) * n_scenes, cudaHostAllocDefault) != cudaSuccess ||
+        cudaHostAlloc((void**)&e->h_flags, sizeof(Flags), cudaHostAllocDefault) != cudaSuccess ||
+        cudaHostAlloc((void**)&e->h_overflow, sizeof(int) * n_scenes, cudaHostAllocDefault) != cudaSuccess ||
+        cudaHostAlloc((void**)&e->h_pairs, sizeof(unsigned long long) * n_scenes, cudaHostAllocDefault) != cudaSuccess)
+        return fail(IVP_ERR_CUDA);
+    if (cudaMemcpyAsync((void*)D.scenes, P.hp.data(), sizeof(SceneParams) * n_scenes, cudaMemcpyHostToDevice, s) !=
+            cudaSuccess ||
+        (e->n_tiles && cudaMemcpyAsync((void*)D.tiles, P.tiles.data(), sizeof(int4) * e->n_tiles,
+                                       cudaMemcpyHostToDevice, s) != cudaSuccess) ||
+        (e->n_total && cudaMemcpyAsync((void*)D.pscene, pscene.data(), sizeof(int) * e->n_total,
+                                       cudaMemcpyHostToDevice, s) != cudaSuccess))
+        return fail(IVP_ERR_CUDA);
+    // the host vectors go out of scope: make the copies complete first
+    if (cudaStreamSynchronize(s) != cudaSuccess) return fail(IVP_ERR_CUDA);
+    *out = e;
+    return IVP_OK;
+}
+
+int ivp_engine_destroy(ivp_engine* e) {
+    if (!e) return IVP_OK;
+    destroy_graphs(e);
+    if (e->h_ctl) cudaFreeHost(e->h_ctl);
+    if (e->h_flags) cudaFreeHost(e->h_flags);
+    if (e->h_overflow) cudaFreeHost(e->h_overflow);
+    if (e->h_pairs) cudaFreeHost(e->h_pairs);
+    delete e;
+    return IVP_OK;
+}
+
+int ivp_engine_bind(ivp_engine* e, const ivp_particles* p) {
+    if (!e || !p) return IVP_ERR_BAD_ARG;
+    if (p->n_total != e->n_total) return IVP_ERR_BAD_ARG;
+    if (!p->x || !p->v || !p->m || !p->density0 || !p->is_dynamic || !p->density || !p->kdiag)
+        return IVP_ERR_BAD_ARG;
+    destroy_graphs(e);
+    e->D.x = p->x;
+    e->D.v = p->v;
+    e->D.m = p->m;
+    e->D.rho0 = p->density0;
+    e->D.dyn = p->is_dynamic;
+    e->D.material = p->material;
+    e->D.density_out = p->density;
+    e->D.k_out = p->kdiag;
+    e->D.div_out = p->divergence;
+    e->want_divergence = p->divergence != nullptr;
+    e->bound = true;
+    return IVP_OK;
+}
+
+int ivp_update_scene(ivp_engine* e, int32_t scene, const ivp_scene_desc* d, void* stream) {
+    if (!e || !d || scene < 0 || scene >= e->n_scenes) return IVP_ERR_BAD_ARG;
+    const ivp_scene_desc& o = e->desc[scene];
+    if (d->particle_offset != o.particle_offset || d->n_particles != o.n_particles || d->n_dynamic != o.n_dynamic ||
+        d->particle_radius != o.particle_radius || d->cache_size != o.cache_size ||
+        d->domain_size[0] != o.domain_size[0] || d->domain_size[1] != o.domain_size[1] ||
+        d->domain_size[2] != o.domain_size[2])
+        return IVP_ERR_BAD_ARG;
+    if (!(d->dt > 0.0f) || d->max_outer_iters < 0 || d->max_iteration_pcg < 0) return IVP_ERR_BAD_ARG;
+    e->desc[scene] = *d;
+    SceneParams& q = e->hp[scene];
+    q.dt = d->dt;
+    q.inv_dt = (float)(1.0 / (double)d->dt);
+    q.omega = d->omega;
+    for (int a = 0; a < 3; ++a) q.gravity[a] = d->gravity[a];
+    q.max_outer = d->max_outer_iters;
+    q.max_pcg = d->max_iteration_pcg;
+    q.fixed_iters = d->fixed_outer_iters;
+    q.tol_opt = d->density_error_tol;
+    q.tol_pcg = d->tol_pcg;
+    q.visc_coeff = d->viscosity_coeff;
+    q.visc_method = d->viscosity_method;
+    cudaStream_t s = as_stream(stream);
+    CK(cudaMemcpyAsync((void*)(e->D.scenes + scene), &q, sizeof(SceneParams), cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    return IVP_OK;
+}
+
+int ivp_neighbour_build(ivp_engine* e, void* stream) {
+    if (!e) return IVP_ERR_BAD_ARG;
+    return run(e, emit_build, &e->graph_build, &e->exec_build, as_stream(stream));
+}
+
+int ivp_compute_density(ivp_engine* e, void* stream) {
+    if (!e) return IVP_ERR_BAD_ARG;
+    if (!e->bound) return IVP_ERR_NOT_BOUND;
+    KernelSet K;
+    kernel_set(e->G, &K);
+    Launcher L;
+    L.stream = as_stream(stream);
+    return L.dev(IVP_K_PACK, K.dens, e->n_tiles, e->BLOCK, e->D);
+}
+
+int ivp_compute_aii(ivp_engine* e, void* stream) {
+    if (!e) return IVP_ERR_BAD_ARG;
+    if (!e->bound) return IVP_ERR_NOT_BOUND;
+    KernelSet K;
+    kernel_set(e->G, &K);
+    Launcher L;
+    L.stream = as_stream(stream);
+    CKS(L.dev(IVP_K_PACK, K.aii, e->n_tiles, e->BLOCK, e->D));
+    return L.dev(IVP_K_STATIC_OUT, k_static_outputs, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, e->D);
+}
+
+int ivp_ip_solve(ivp_engine* e, void* stream) {
+    if (!e) return IVP_ERR_BAD_ARG;
+    return run(e, emit_solve, &e->graph_solve, &e->exec_solve, as_stream(stream));
+}
+
+int ivp_apply_gravity(ivp_engine* e, void* stream) {
+    if (!e) return IVP_ERR_BAD_ARG;
+    if (!e->bound) return IVP_ERR_NOT_BOUND;
+    Launcher L;
+    L.stream = as_stream(stream);
+    return L.dev(IVP_K_GRAVITY, k_gravity, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, e->D);
+}
+
+int ivp_advect(ivp_engine* e, void* stream) {
+    if (!e) return IVP_ERR_BAD_ARG;
+    if (!e->bound) return IVP_ERR_NOT_BOUND;
+    Launcher L;
+    L.stream = as_stream(stream);
+    return emit_advect(e, L);
+}
+
+int ivp_step(ivp_engine* e, int32_t n_steps, void* stream) {
+    if (!e || n_steps < 0) return IVP_ERR_BAD_ARG;
+    for (int k = 0; k < n_steps; ++k) CKS(run(e, emit_step, &e->graph_step, &e->exec_step, as_stream(stream)));
+    return IVP_OK;
+}
+
+int ivp_read_stats(ivp_engine* e, int32_t scene, void* stream, ivp_solve_stats* out) {
+    if (!e || !out || scene < 0 || scene >= e->n_scenes) return IVP_ERR_BAD_ARG;
+    cudaStream_t s = as_stream(stream);
+    CK(cudaMemcpyAsync(e->h_ctl + scene, e->D.ctl + scene, sizeof(SceneCtl), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(e->h_overflow + scene, e->D.overflow + scene, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(e->h_flags, e->D.flags, sizeof(Flags), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(e->h_pairs + scene, e->D.pairs + scene, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const SceneCtl& C = e->h_ctl[scene];
+    memset(out, 0, sizeof(*out));
+    out->status = C.status;
+    out->outer_iters = C.outer_it;
+    out->n_density_errors = C.n_err;
+    out->overflow_particles = e->h_overflow[scene];
+    out->final_density_error = C.final_err;
+    out->last_density_error = C.err;
+    out->total_pcg_iters = C.total_cg;
+    out->solves = C.acc_solves;
+    out->failed_solves = C.acc_failed;
+    out->last_failure = C.acc_last_failure;
+    out->sum_outer_iters = C.acc_outer;
+    out->sum_pcg_iters = C.acc_cg;
+    out->max_final_density_error = C.acc_max_final_err;
+    out->neighbour_pairs = (int64_t)e->h_pairs[scene];
+    if (e->h_flags->bad) {
+        char buf[128];
+        snprintf(buf, sizeof(buf), "device bounds check failed: index %d at site %d", e->h_flags->bad_index,
+                 e->h_flags->bad_where);
+        g_err = buf;
+        return IVP_ERR_DEVICE_CHECK;
+    }
+    return IVP_OK;
+}
+
+int ivp_read_history(ivp_engine* e, int32_t scene, void* stream, double* errors, int32_t* pcg_iters, int32_t cap,
+                     int32_t* n_errors, int32_t* n_pcg) {
+    if (!e || scene < 0 || scene >= e->n_scenes || cap < 0) return IVP_ERR_BAD_ARG;
+    cudaStream_t s = as_stream(stream);
+    SceneCtl C;
+    CK(cudaMemcpyAsync(&C, e->D.ctl + scene, sizeof(SceneCtl), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const int H = e->opt.max_hist;
+    const int ne = std::min(std::min(C.n_err, H), cap);
+    const int np = std::min(std::min(C.outer_it, H), cap);
+    const size_t base = (size_t)scene * H;
+    if (errors && ne > 0) CK(cudaMemcpy(errors, e->D.err_hist + base, sizeof(double) * ne, cudaMemcpyDeviceToHost));
+    if (pcg_iters && np > 0) CK(cudaMemcpy(pcg_iters, e->D.pcg_hist + base, sizeof(int) * np, cudaMemcpyDeviceToHost));
+    if (n_errors) *n_errors = ne;
+    if (n_pcg) *n_pcg = np;
+    return IVP_OK;
+}
+
+int ivp_export_neighbours(ivp_engine* e, int32_t scene, int32_t* count, int32_t* ids, int32_t cache, void* stream) {
+    if (!e || scene < 0 || scene >= e->n_scenes || !count || !ids || cache <= 0) return IVP_ERR_BAD_ARG;
+    cudaStream_t s = as_stream(stream);
+    const int nd = e->hp[scene].n_dyn;
+    if (nd == 0) return IVP_OK;
+    k_export<<<blocks_for(nd, 128), 128, 0, s>>>(e->D, scene, count, ids, cache);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s));
+    return IVP_OK;
+}
+
+int ivp_reset_counters(ivp_engine* e, void* stream) {
+    if (!e) return IVP_ERR_BAD_ARG;
+    k_reset_counters<<<blocks_for(e->n_scenes, 128), 128, 0, as_stream(stream)>>>(e->D);
+    CK(cudaGetLastError());
+    return IVP_OK;
+}
+
+int ivp_profile_step(ivp_engine* e, int32_t n_steps, void* stream, double* ms, int32_t* launches) {
+    if (!e || n_steps < 0 || !ms || !launches) return IVP_ERR_BAD_ARG;
+    if (!e->bound) return IVP_ERR_NOT_BOUND;
+    cudaStream_t s = as_stream(stream);
+    Prof prof;
+    Launcher L;
+    L.stream = s;
+    L.prof = &prof;
+    for (int k = 0; k < n_steps; ++k) CKS(emit_step(e, L));
+    CK(cudaStreamSynchronize(s));
+    for (int k = 0; k < IVP_K_COUNT; ++k) {
+        ms[k] = 0.0;
+        launches[k] = 0;
+    }
+    for (size_t k = 0; k < prof.ids.size(); ++k) {
+        float t = 0.0f;
+        CK(cudaEventElapsedTime(&t, prof.ev[2 * k], prof.ev[2 * k + 1]));
+        const int id = prof.ids[k];
+        if (id >= 0 && id < IVP_K_COUNT) {
+            ms[id] += t;
+            launches[id] += 1;
+        }
+    }
+    return IVP_OK;
+}
+
+const char* ivp_status_string(int32_t status) {
+    switch (status) {
+        case IVP_OK: return "ok";
+        case IVP_ERR_NOT_SPD: return "non-positive definite matrix (pAp < 0)";
+        case IVP_ERR_NOT_CONVERGED: return "outer iteration did not converge";
+        case IVP_ERR_NBR_OVERFLOW: return "neighbour cache overflow";
+        case IVP_ERR_BAD_ARG: return "bad argument";
+        case IVP_ERR_CUDA: return "CUDA error";
+        case IVP_ERR_TIMEOUT: return "timeout";
+        case IVP_ERR_NOT_BOUND: return "particle arrays not bound";
+        case IVP_ERR_DEVICE_CHECK: return "device-side bounds check failed";
+        default: return "unknown status";
+    }
+}
+
+const char* ivp_last_error(void) { return g_err.c_str(); }
+
+}  // extern "C"

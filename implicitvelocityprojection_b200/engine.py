@@ -1,0 +1,259 @@
+"""Engine: the CUDA IP pressure step over one or more independent scenes.
+
+PyTorch owns every device buffer (particle arrays and one workspace tensor);
+`libivp.so` receives their pointers through the C ABI.  Scenes are
+concatenated in the particle arrays (scene s owns a contiguous range), which
+is how the batched and served forms run many scenes in one set of launches.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+from typing import List, Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check
+
+
+def _stream_ptr(stream: Optional[torch.cuda.Stream] = None) -> int:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return int(s.cuda_stream)
+
+
+@dataclasses.dataclass
+class EngineOptions:
+    lanes_per_particle: int = 4
+    particles_per_block: int = 32
+    list_stride: int = 64
+    max_hist: int = 128
+    use_graphs: bool = True
+
+    def to_c(self) -> _lib.Options:
+        o = _lib.Options()
+        o.lanes_per_particle = self.lanes_per_particle
+        o.particles_per_block = self.particles_per_block
+        o.list_stride = self.list_stride
+        o.max_hist = self.max_hist
+        o.use_graphs = int(self.use_graphs)
+        return o
+
+
+def scene_desc(sc, offset: int) -> _lib.SceneDesc:
+    """C descriptor of a `scenes.Scene` occupying particles [offset, offset+n)."""
+    d = _lib.SceneDesc()
+    d.particle_offset = offset
+    d.n_particles = sc.n
+    d.n_dynamic = sc.n_dynamic
+    d.particle_radius = sc.particle_radius
+    for a in range(3):
+        d.domain_size[a] = float(sc.domain_size[a])
+        d.gravity[a] = float(sc.gravity[a])
+    d.dt = sc.dt
+    d.omega = sc.omega
+    d.tol_pcg = sc.tol_pcg
+    d.density_error_tol = sc.density_error_tol
+    d.max_outer_iters = sc.max_outer_iters
+    d.max_iteration_pcg = sc.max_iteration_pcg
+    d.fixed_outer_iters = int(sc.fixed_outer_iters)
+    d.cache_size = sc.cache_size
+    d.viscosity_coeff = sc.viscosity_coeff
+    d.viscosity_method = sc.viscosity_method
+    return d
+
+
+@dataclasses.dataclass
+class Stats:
+    """Per-scene result of the last IP solve (names of pressure_base.py:331-339)."""
+
+    status: int
+    stats_outer_iters: int
+    stats_final_density_error: float
+    stats_density_errors: list
+    stats_pcg_iters: list
+    overflow_particles: int
+    total_pcg_iters: int
+
+
+class Engine:
+    """IP pressure-step engine over `scenes` (list of `scenes.Scene`).
+
+    Particle arrays are allocated here in the reference's layout and scene
+    order; pass `arrays=` to bind existing tensors instead (dict with x, v, m,
+    density0, is_dynamic, material, density, k[, divergence]).
+    """
+
+    def __init__(self, scenes: Sequence, device: str = "cuda", options: Optional[EngineOptions] = None,
+                 arrays: Optional[dict] = None, stream: Optional[torch.cuda.Stream] = None,
+                 divergence: bool = False):
+        self.L = _lib.load()
+        self.scenes = list(scenes)
+        self.device = torch.device(device)
+        self.options = options or EngineOptions()
+        self.offsets = np.zeros(len(self.scenes) + 1, np.int64)
+        for i, sc in enumerate(self.scenes):
+            self.offsets[i + 1] = self.offsets[i] + sc.n
+        self.n_total = int(self.offsets[-1])
+        descs = (_lib.SceneDesc * len(self.scenes))()
+        for i, sc in enumerate(self.scenes):
+            descs[i] = scene_desc(sc, int(self.offsets[i]))
+        self._descs = descs
+        opt = self.options.to_c()
+        self._opt = opt
+        nbytes = ctypes.c_size_t(0)
+        check(self.L.ivp_workspace_bytes(descs, len(self.scenes), ctypes.byref(opt), ctypes.byref(nbytes)),
+              "ivp_workspace_bytes")
+        self.workspace_bytes = int(nbytes.value)
+        # 256-byte aligned workspace carved from one uint8 tensor
+        self._ws_raw = torch.empty(self.workspace_bytes + 256, dtype=torch.uint8, device=self.device)
+        base = self._ws_raw.data_ptr()
+        self._ws_ptr = (base + 255) & ~255
+        if arrays is None:
+            arrays = self._alloc_arrays(divergence)
+        self.arrays = arrays
+        self._handle = ctypes.c_void_p()
+        st = _stream_ptr(stream)
+        check(self.L.ivp_engine_create(descs, len(self.scenes), ctypes.byref(opt), ctypes.c_void_p(self._ws_ptr),
+                                       ctypes.c_size_t(self.workspace_bytes), ctypes.c_void_p(st),
+                                       ctypes.byref(self._handle)), "ivp_engine_create")
+        self._bind()
+
+    # ------------------------------------------------------------ arrays
+    def _alloc_arrays(self, divergence: bool) -> dict:
+        dev = self.device
+        x = np.concatenate([sc.x for sc in self.scenes]).astype(np.float32) if self.scenes else np.zeros((0, 3))
+        v = np.concatenate([sc.v for sc in self.scenes]).astype(np.float32)
+        ms = [sc.masses() for sc in self.scenes]
+        m = np.concatenate([a for a, _ in ms]).astype(np.float32)
+        a = {
+            "x": torch.from_numpy(x).to(dev),
+            "v": torch.from_numpy(v).to(dev),
+            "m": torch.from_numpy(m).to(dev),
+            "density0": torch.from_numpy(np.concatenate([sc.density0 for sc in self.scenes])).to(dev),
+            "is_dynamic": torch.from_numpy(np.concatenate([sc.is_dynamic for sc in self.scenes]).astype(np.int32)).to(dev),
+            "material": torch.from_numpy(np.concatenate([sc.material for sc in self.scenes]).astype(np.int32)).to(dev),
+        }
+        a["density"] = a["density0"].clone()
+        a["k"] = torch.zeros(self.n_total, dtype=torch.float32, device=dev)
+        if divergence:
+            a["divergence"] = torch.zeros(self.n_total, dtype=torch.float32, device=dev)
+        return a
+
+    def _bind(self):
+        a = self.arrays
+        for k in ("x", "v"):
+            assert a[k].is_contiguous() and a[k].dtype == torch.float32 and a[k].shape[-1] == 3
+        p = _lib.Particles()
+        p.x = a["x"].data_ptr()
+        p.v = a["v"].data_ptr()
+        p.m = a["m"].data_ptr()
+        p.density0 = a["density0"].data_ptr()
+        p.is_dynamic = a["is_dynamic"].data_ptr()
+        p.material = a["material"].data_ptr()
+        p.density = a["density"].data_ptr()
+        p.kdiag = a["k"].data_ptr()
+        p.divergence = a["divergence"].data_ptr() if a.get("divergence") is not None else None
+        p.n_total = self.n_total
+        check(self.L.ivp_engine_bind(self._handle, ctypes.byref(p)), "ivp_engine_bind")
+
+    def rebind(self, arrays: dict):
+        self.arrays = arrays
+        self._bind()
+
+    def close(self):
+        if getattr(self, "_handle", None) and self._handle.value:
+            self.L.ivp_engine_destroy(self._handle)
+            self._handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------ calls
+    def update_scene(self, i: int, sc, stream=None):
+        d = scene_desc(sc, int(self.offsets[i]))
+        check(self.L.ivp_update_scene(self._handle, i, ctypes.byref(d), ctypes.c_void_p(_stream_ptr(stream))),
+              "ivp_update_scene")
+        self._descs[i] = d
+
+    def build(self, stream=None):
+        """NeighbourSearch.build + build_cache + compute_density + compute_Aii."""
+        check(self.L.ivp_neighbour_build(self._handle, ctypes.c_void_p(_stream_ptr(stream))), "ivp_neighbour_build")
+
+    def compute_density(self, stream=None):
+        check(self.L.ivp_compute_density(self._handle, ctypes.c_void_p(_stream_ptr(stream))), "ivp_compute_density")
+
+    def compute_aii(self, stream=None):
+        check(self.L.ivp_compute_aii(self._handle, ctypes.c_void_p(_stream_ptr(stream))), "ivp_compute_aii")
+
+    def solve(self, stream=None):
+        """IP.solve(dt) of every scene (asynchronous)."""
+        check(self.L.ivp_ip_solve(self._handle, ctypes.c_void_p(_stream_ptr(stream))), "ivp_ip_solve")
+
+    def apply_gravity(self, stream=None):
+        check(self.L.ivp_apply_gravity(self._handle, ctypes.c_void_p(_stream_ptr(stream))), "ivp_apply_gravity")
+
+    def advect(self, stream=None):
+        check(self.L.ivp_advect(self._handle, ctypes.c_void_p(_stream_ptr(stream))), "ivp_advect")
+
+    def step(self, n: int = 1, stream=None):
+        """n Framework.forward() steps of every scene (asynchronous)."""
+        check(self.L.ivp_step(self._handle, int(n), ctypes.c_void_p(_stream_ptr(stream))), "ivp_step")
+
+    def reset_counters(self, stream=None):
+        check(self.L.ivp_reset_counters(self._handle, ctypes.c_void_p(_stream_ptr(stream))), "ivp_reset_counters")
+
+    def profile_step(self, n: int = 1, stream=None) -> dict:
+        """n steps with host-driven launches and CUDA events around each
+        kernel: {kernel name: (total ms, launches)}."""
+        ms = np.zeros(_lib.K_COUNT, np.float64)
+        cnt = np.zeros(_lib.K_COUNT, np.int32)
+        check(self.L.ivp_profile_step(self._handle, int(n), ctypes.c_void_p(_stream_ptr(stream)),
+                                      ms.ctypes.data_as(ctypes.c_void_p), cnt.ctypes.data_as(ctypes.c_void_p)),
+              "ivp_profile_step")
+        return {name: (float(ms[i]), int(cnt[i])) for i, name in enumerate(_lib.KERNEL_NAMES) if cnt[i] > 0}
+
+    def raw_stats(self, scene: int = 0, stream=None) -> _lib.SolveStats:
+        s = _lib.SolveStats()
+        check(self.L.ivp_read_stats(self._handle, scene, ctypes.c_void_p(_stream_ptr(stream)), ctypes.byref(s)),
+              "ivp_read_stats")
+        return s
+
+    def stats(self, scene: int = 0, stream=None) -> Stats:
+        s = self.raw_stats(scene, stream)
+        cap = self.options.max_hist
+        err = np.zeros(cap, np.float64)
+        pcg = np.zeros(cap, np.int32)
+        ne, npc = ctypes.c_int32(0), ctypes.c_int32(0)
+        check(self.L.ivp_read_history(self._handle, scene, ctypes.c_void_p(_stream_ptr(stream)),
+                                      err.ctypes.data_as(ctypes.c_void_p), pcg.ctypes.data_as(ctypes.c_void_p),
+                                      cap, ctypes.byref(ne), ctypes.byref(npc)), "ivp_read_history")
+        return Stats(status=int(s.status), stats_outer_iters=int(s.outer_iters),
+                     stats_final_density_error=float(s.final_density_error),
+                     stats_density_errors=[float(e) for e in err[:ne.value]],
+                     stats_pcg_iters=[int(q) for q in pcg[:npc.value]],
+                     overflow_particles=int(s.overflow_particles), total_pcg_iters=int(s.total_pcg_iters))
+
+    def neighbours(self, scene: int = 0, cache: Optional[int] = None, stream=None):
+        """(count[n], ids[n, cache]) of a scene in the reference layout, local
+        particle indices; rows of static particles are zero."""
+        sc = self.scenes[scene]
+        cache = cache or sc.cache_size
+        n = sc.n
+        count = torch.zeros(n, dtype=torch.int32, device=self.device)
+        ids = torch.full((n, cache), -1, dtype=torch.int32, device=self.device)
+        check(self.L.ivp_export_neighbours(self._handle, scene, ctypes.c_void_p(count.data_ptr()),
+                                           ctypes.c_void_p(ids.data_ptr()), cache,
+                                           ctypes.c_void_p(_stream_ptr(stream))), "ivp_export_neighbours")
+        return count.cpu().numpy(), ids.cpu().numpy()
+
+    # ------------------------------------------------------------ views
+    def scene_slice(self, i: int) -> slice:
+        return slice(int(self.offsets[i]), int(self.offsets[i + 1]))
+
+    def get(self, name: str, scene: int = 0) -> np.ndarray:
+        return self.arrays[name][self.scene_slice(scene)].cpu().numpy()

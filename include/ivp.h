@@ -1,0 +1,199 @@
+/*
+ * ivp.h -- C ABI of the B200 implicit velocity projection (IP) pressure step.
+ *
+ * Drop-in boundary for the reference's IP pressure-solver plugin
+ * (medialab-ku/ImplicitVelocityProjection).  Every entry point names the
+ * reference interface it replaces.  Memory is owned by the caller (PyTorch
+ * tensors in the Python host layer): the engine receives raw device pointers,
+ * counts and a CUDA stream, and allocates no device memory after
+ * ivp_engine_create.  No C++ exceptions cross this boundary; every call
+ * returns an ivp_status.
+ *
+ * Streams are passed as `void*` holding a cudaStream_t (NULL = legacy default
+ * stream).  Calls are stream-ordered and asynchronous unless stated.  One
+ * host thread drives an engine at a time; engines are independent.
+ */
+#ifndef IVP_H
+#define IVP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference raises RuntimeError for NOT_SPD
+ * (scripts/sim/forces/pressure/ip.py:308-309) and NOT_CONVERGED
+ * (scripts/sim/forces/pressure/pressure_base.py:487-495). */
+typedef enum {
+    IVP_OK = 0,
+    IVP_ERR_NOT_SPD = 1,        /* CG saw p^T A p < 0 */
+    IVP_ERR_NOT_CONVERGED = 2,  /* outer-iteration cap reached above densityErrorTol */
+    IVP_ERR_NBR_OVERFLOW = 3,   /* a particle had more neighbours than neighborCacheSize (lists truncated, as the reference does) */
+    IVP_ERR_BAD_ARG = 4,
+    IVP_ERR_CUDA = 5,
+    IVP_ERR_TIMEOUT = 6,
+    IVP_ERR_NOT_BOUND = 7,      /* particle arrays not bound */
+    IVP_ERR_DEVICE_CHECK = 8    /* a device-side bounds check failed (index out of range) */
+} ivp_status;
+
+/* One independent scene.  Its particles occupy [particle_offset,
+ * particle_offset + n_particles) of the bound arrays.  Field meanings follow
+ * the reference's configuration keys (scripts/io/config_builder.py:10-115,
+ * ip.py:228-229, pressure_base.py:314-317, simulation_data.py:157). */
+typedef struct {
+    int32_t particle_offset;
+    int32_t n_particles;
+    int32_t n_dynamic;          /* particles with is_dynamic == 1 in the range */
+    float particle_radius;      /* r: d = 2r, support radius h = 4r */
+    float domain_size[3];       /* domain [0, L) per axis (boundary clamp, grid) */
+    float dt;                   /* timeStepSize */
+    float gravity[3];           /* gravitation */
+    float omega;                /* IP omega (default 10) */
+    double tol_pcg;             /* absolute ||r||^2 tolerance of CG (default 1e-6) */
+    double density_error_tol;   /* densityErrorTol (default 1e-3) */
+    int32_t max_outer_iters;    /* maxOuterIters (default 1000) */
+    int32_t max_iteration_pcg;  /* CG cap (reference hard-codes 1000) */
+    int32_t fixed_outer_iters;  /* fixedOuterIters (0/1) */
+    int32_t cache_size;         /* neighborCacheSize (default 60) */
+    float viscosity_coeff;      /* kinematic viscosity for Weiler18 (viscosityMethod 1) */
+    int32_t viscosity_method;   /* 0 off, 1 Weiler 2018 implicit */
+    int32_t reserved[4];
+} ivp_scene_desc;
+
+typedef struct {
+    int32_t lanes_per_particle;   /* 1, 2, 4 or 8 lanes share one particle's neighbour sum */
+    int32_t particles_per_block;  /* particles per CTA in the neighbour-sum kernels */
+    int32_t list_stride;          /* neighbour-list row stride (>= every scene's cache_size) */
+    int32_t max_hist;             /* per-scene stats history length (outer iterations) */
+    int32_t use_graphs;           /* 1: device-side loops in CUDA graphs with conditional nodes */
+    int32_t reserved[3];
+} ivp_options;
+
+/* Device arrays in the reference's layout and particle order
+ * (scripts/sim/simulation_data.py:165-212).  vec3 arrays are float[N][3]. */
+typedef struct {
+    float* x;              /* positions (read; written by ivp_advect / ivp_step) */
+    float* v;              /* velocities (read/write) */
+    const float* m;        /* masses (static particles carry the reference's x10) */
+    const float* density0; /* rest densities */
+    const int32_t* is_dynamic;
+    const int32_t* material;
+    float* density;        /* out: SPH density (ps.density) */
+    float* kdiag;          /* out: k = 1/(Aii + eps) (PressureBase.k) */
+    float* divergence;     /* out, may be NULL: max(J v, 0) (ps.divergence) */
+    int32_t n_total;       /* particles in the arrays (sum over scenes) */
+} ivp_particles;
+
+/* Per-scene results of the last IP solve (pressure_base.py:331-339). */
+typedef struct {
+    int32_t status;
+    int32_t outer_iters;          /* stats_outer_iters */
+    int32_t n_density_errors;     /* entries of stats_density_errors */
+    int32_t overflow_particles;   /* particles whose neighbour count exceeded cache_size */
+    double final_density_error;   /* stats_final_density_error */
+    double last_density_error;
+    int32_t total_pcg_iters;      /* CG iterations of the last solve */
+    /* counters since ivp_reset_counters (kept on the device, no host sync per step) */
+    int32_t solves;
+    int32_t failed_solves;
+    int32_t last_failure;         /* status of the last failed solve */
+    int64_t sum_outer_iters;
+    int64_t sum_pcg_iters;
+    double max_final_density_error;
+    int64_t neighbour_pairs;      /* pairs in the scene's current neighbour lists */
+} ivp_solve_stats;
+
+/* Kernel ids reported by ivp_profile_step. */
+enum {
+    IVP_K_GRAVITY = 0, IVP_K_SOLVE_BEGIN, IVP_K_PACK, IVP_K_RHS, IVP_K_CG_A, IVP_K_CG_B, IVP_K_SOLVE_END,
+    IVP_K_DIVERGENCE, IVP_K_ADVECT, IVP_K_KEYS, IVP_K_SCAN_LOCAL, IVP_K_SCAN_ADD, IVP_K_PLACE, IVP_K_ORDER,
+    IVP_K_NBR_BUILD, IVP_K_STATIC_OUT, IVP_K_VISC, IVP_K_COUNT = 24
+};
+
+typedef struct ivp_engine ivp_engine;
+
+/* Defaults for ivp_options. */
+void ivp_default_options(ivp_options* opt);
+
+/* Workspace bytes for a set of scenes (no allocation). */
+int ivp_workspace_bytes(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_options* opt, size_t* bytes);
+
+/* Creates an engine over a caller-owned device workspace of
+ * ivp_workspace_bytes bytes (256-byte aligned).  Builds the scene tables on
+ * the device.  Replaces the construction of SimulationData / NeighbourSearch
+ * / IP (scripts/sim/simulation_data.py:118-212, neighbour_search.py:93-114,
+ * ip.py:225-242). */
+int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_options* opt, void* workspace,
+                      size_t workspace_bytes, void* stream, ivp_engine** out);
+int ivp_engine_destroy(ivp_engine* e);
+
+/* Updates the run-time parameters of one scene (dt, gravity, omega, tolerances,
+ * iteration caps, viscosity coefficient) -- the attributes the reference's
+ * GUI and Framework change between steps (gui.py:435-473, IP.solve(dt)).
+ * Geometry fields (particle counts, radius, domain, cache size) must be
+ * unchanged.  Stream-ordered. */
+int ivp_update_scene(ivp_engine* e, int32_t scene, const ivp_scene_desc* desc, void* stream);
+
+/* Binds the particle arrays (replaces the SimulationData arrays). */
+int ivp_engine_bind(ivp_engine* e, const ivp_particles* p);
+
+/* NeighbourSearch.build + build_cache (neighbour_search.py:116-155) fused with
+ * PressureBase.compute_density and compute_Aii (pressure_base.py:341-365):
+ * cell hash, counting sort by cell, reordered particle copies, compact
+ * neighbour lists, density and k.  Also writes density/kdiag of the bound
+ * arrays. */
+int ivp_neighbour_build(ivp_engine* e, void* stream);
+
+/* PressureBase.compute_density / compute_Aii (pressure_base.py:341-365) from
+ * the current lists and the bound positions/masses. */
+int ivp_compute_density(ivp_engine* e, void* stream);
+int ivp_compute_aii(ivp_engine* e, void* stream);
+
+/* IP.solve(dt) (ip.py:331-404) for every scene: outer loop, CG, v = d/dt,
+ * stats.  Asynchronous; read results with ivp_read_stats. */
+int ivp_ip_solve(ivp_engine* e, void* stream);
+
+/* apply_gravity (framework.py:26-41). */
+int ivp_apply_gravity(ivp_engine* e, void* stream);
+
+/* advect_position + enforce_boundary (framework.py:117-136, boundary.py:27-91). */
+int ivp_advect(ivp_engine* e, void* stream);
+
+/* n_steps of Framework.forward() with IP (framework.py:423-544): gravity,
+ * implicit viscosity where a scene enables it, IP solve, advect + clamp,
+ * neighbour rebuild, density, Aii.  The engine must have been built once
+ * (ivp_neighbour_build), as Framework.initialize does (framework.py:323-330). */
+int ivp_step(ivp_engine* e, int32_t n_steps, void* stream);
+
+/* Zeroes the counters reported in ivp_solve_stats (stream-ordered). */
+int ivp_reset_counters(ivp_engine* e, void* stream);
+
+/* Runs n_steps of ivp_step with host-driven launches (no graphs) and CUDA
+ * events around every kernel; accumulates per-kernel device milliseconds and
+ * launch counts into ms[IVP_K_COUNT] and launches[IVP_K_COUNT].  Synchronous.
+ * Same results as ivp_step. */
+int ivp_profile_step(ivp_engine* e, int32_t n_steps, void* stream, double* ms, int32_t* launches);
+
+/* Synchronises the stream and copies one scene's stats of the last solve. */
+int ivp_read_stats(ivp_engine* e, int32_t scene, void* stream, ivp_solve_stats* out);
+
+/* Copies up to `cap` per-outer-iteration density errors / CG iteration counts
+ * of the last solve (stats_density_errors, stats_pcg_iters).  Synchronous. */
+int ivp_read_history(ivp_engine* e, int32_t scene, void* stream, double* errors, int32_t* pcg_iters, int32_t cap,
+                     int32_t* n_errors, int32_t* n_pcg);
+
+/* Exports the neighbour lists of one scene in the reference's cache layout
+ * (neighbor_count[N], neighbor_ids[N*cache]) with original particle indices,
+ * for parity checks.  Synchronous, device pointers. */
+int ivp_export_neighbours(ivp_engine* e, int32_t scene, int32_t* count, int32_t* ids, int32_t cache, void* stream);
+
+const char* ivp_status_string(int32_t status);
+/* Last CUDA error string seen by the engine (thread-local). */
+const char* ivp_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* IVP_H */

