@@ -92,6 +92,8 @@ class SolveStats(ctypes.Structure):
 KERNEL_NAMES = ["gravity", "solve_begin", "pack", "rhs", "cg_a", "cg_b", "solve_end", "divergence", "advect",
                 "keys", "scan_local", "scan_add", "place", "order", "nbr_build", "static_out", "visc"]
 K_COUNT = 24
+NOALLOC_MAX_PARTICLES = 65536
+NOALLOC_MAX_CELLS = 262144
 
 
 # every exported symbol of include/ivp.h with its ctypes signature
@@ -117,6 +119,7 @@ SIGNATURES = {
     "ivp_read_stats": (_I, [_P, _I, _P, ctypes.POINTER(SolveStats)]),
     "ivp_read_history": (_I, [_P, _I, _P, _P, _P, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "ivp_export_neighbours": (_I, [_P, _I, _P, _P, _I, _P]),
+    "ivp_density_aii_noalloc": (_I, [_P, _P, _P, _I, ctypes.c_float, _P, _I, _P, _P, _P]),
     "ivp_status_string": (ctypes.c_char_p, [_I]),
     "ivp_last_error": (ctypes.c_char_p, []),
 }

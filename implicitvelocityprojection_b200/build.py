@@ -16,8 +16,8 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libivp.so")
-SOURCES = ["ivp_engine.cu"]
-DEPS = ["ivp_engine.cu", "ivp_kernels.cuh", "ivp_device.cuh"]
+SOURCES = ["ivp_engine.cu", "ivp_noalloc.cu"]
+DEPS = ["ivp_engine.cu", "ivp_noalloc.cu", "ivp_kernels.cuh", "ivp_device.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

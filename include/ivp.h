@@ -189,6 +189,32 @@ int ivp_read_history(ivp_engine* e, int32_t scene, void* stream, double* errors,
  * for parity checks.  Synchronous, device pointers. */
 int ivp_export_neighbours(ivp_engine* e, int32_t scene, int32_t* count, int32_t* ids, int32_t cache, void* stream);
 
+/* Limits of ivp_density_aii_noalloc. */
+#define IVP_NOALLOC_MAX_PARTICLES 65536
+#define IVP_NOALLOC_MAX_CELLS 262144
+
+/* No counterpart in the reference.  SPH density and k = 1/(Aii + 1e-3) of
+ * every dynamic particle of one scene (k = 0 for static particles), for
+ * callers that cannot allocate device memory: code living inside another
+ * runtime's memory arena, code recorded into a stream capture in global mode
+ * (where cudaMalloc is illegal), or real-time loops that cannot take the
+ * device synchronisation of cudaMalloc/cudaFree.  It allocates nothing and
+ * needs no workspace: its scratch is one fixed device array inside the
+ * library (about 6.3 MB, held on every GPU that loads the library until the
+ * process exits).  Results equal those of ivp_neighbour_build for the same
+ * particles.  Inputs: x float[n][3], m float[n], is_dynamic int[n] (caller
+ * order, device pointers); outputs density[n], kdiag[n] (density of static
+ * particles is left untouched).  At most IVP_NOALLOC_MAX_PARTICLES particles
+ * and IVP_NOALLOC_MAX_CELLS cells of size h = 4 r over the domain; larger
+ * inputs return IVP_ERR_BAD_ARG without touching the device.  All calls share
+ * the scratch array: calls whose GPU work overlaps (other streams or host
+ * threads) race and must be serialised by the caller.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) with that
+ * device current; make that first call before any stream capture. */
+int ivp_density_aii_noalloc(const float* x, const float* m, const int32_t* is_dynamic, int32_t n_particles,
+                            float particle_radius, const float* domain_size, int32_t cache_size, float* density,
+                            float* kdiag, void* stream);
+
 const char* ivp_status_string(int32_t status);
 /* Last CUDA error string seen by the engine (thread-local). */
 const char* ivp_last_error(void);
