@@ -205,7 +205,8 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     sc = make_scene(args.workload)
-    opts = EngineOptions(lanes_per_particle=args.lanes, particles_per_block=128 // args.lanes)
+    opts = EngineOptions(lanes_per_particle=args.lanes,
+                         particles_per_block=args.ppb or 128 // args.lanes, persistent=not args.per_phase)
     eng = Engine([sc], device=str(dev), options=opts, divergence=True)
     eng.build()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
@@ -243,12 +244,18 @@ def run_ours(args, rank, world, local_rank):
     valid = raw.failed_solves == 0 and raw.solves == args.steps and \
         raw.max_final_density_error < sc.density_error_tol
     value = world * sc.n_dynamic * args.steps / (total_ms / 1000.0)
-    n_launch = 12 * args.steps + (raw.sum_outer_iters + args.steps) + raw.sum_outer_iters + 2 * raw.sum_pcg_iters
 
     # per-kernel device time of the same workload (host-driven launches with
     # CUDA events around each kernel, after the timed region)
     prof = eng.profile_step(3)
     pairs = int(eng.raw_stats(0).neighbour_pairs)
+    if "ip_solve" in prof:
+        # gravity, persistent IP solve, advect, keys, 2 scan passes, place,
+        # order, neighbour build, static outputs
+        n_launch = 10 * args.steps
+    else:
+        n_launch = 12 * args.steps + (raw.sum_outer_iters + args.steps) + raw.sum_outer_iters + \
+            2 * raw.sum_pcg_iters
     dom = max(prof.items(), key=lambda kv: kv[1][0])
     dom_name, (dom_ms, dom_n) = dom
     avg_s = dom_ms / dom_n / 1000.0
@@ -270,7 +277,9 @@ def run_ours(args, rank, world, local_rank):
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {**workload_config(sc, args.workload), "parallelism": f"replicas x{world}",
-                           "lanes_per_particle": args.lanes},
+                           "lanes_per_particle": args.lanes,
+                           "particles_per_block": opts.particles_per_block,
+                           "solve": "per-phase launches" if args.per_phase else "persistent cooperative kernel"},
                 "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
                 "valid": bool(valid), "max_final_density_error": raw.max_final_density_error,
                 "outer_iters_per_step": raw.sum_outer_iters / args.steps,
@@ -332,6 +341,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="tall_column")
     ap.add_argument("--lanes", type=int, default=4)
+    ap.add_argument("--ppb", type=int, default=0, help="particles per CTA (default 128 / lanes)")
+    ap.add_argument("--per-phase", action="store_true", help="one launch per solver phase instead of the "
+                    "persistent cooperative solve")
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--cpu-budget-s", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")

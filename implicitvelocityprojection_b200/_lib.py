@@ -50,7 +50,8 @@ class Options(ctypes.Structure):
         ("list_stride", ctypes.c_int32),
         ("max_hist", ctypes.c_int32),
         ("use_graphs", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 3),
+        ("persistent", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 2),
     ]
 
 
@@ -90,7 +91,7 @@ class SolveStats(ctypes.Structure):
 
 # kernel ids of ivp_profile_step (include/ivp.h)
 KERNEL_NAMES = ["gravity", "solve_begin", "pack", "rhs", "cg_a", "cg_b", "solve_end", "divergence", "advect",
-                "keys", "scan_local", "scan_add", "place", "order", "nbr_build", "static_out", "visc"]
+                "keys", "scan_local", "scan_add", "place", "order", "nbr_build", "static_out", "visc", "ip_solve"]
 K_COUNT = 24
 NOALLOC_MAX_PARTICLES = 65536
 NOALLOC_MAX_CELLS = 262144

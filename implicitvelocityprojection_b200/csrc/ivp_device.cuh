@@ -12,10 +12,13 @@
 //     209-213) branch-free with identical rounding;
 //   * per-slot arrays: xm (float4 x,y,z,m), rest density, density, k, c, and
 //     the solver vectors as float4 (16-byte gathers);
-//   * neighbour rows, one per dynamic particle, `stride` entries of int2
-//     {neighbour slot, kernel-gradient weight w} with
-//     grad W_ij = w_ij (x_i - x_j), i.e. the spiky gradient of
-//     sph_kernel.py:52-61 factored as a scalar times the separation;
+//   * neighbour rows, one per dynamic particle, `stride` entries of float4
+//     {J_ij, neighbour slot}: J_ij = m_j grad W_ij, the per-pair vector the
+//     reference forms from its cache (J_ij / val_ij in pressure_base.py:81
+//     and ip.py:54; spiky gradient of sph_kernel.py:52-61).  Every
+//     neighbour sum then streams its row and gathers only the neighbour's
+//     operand: mass-weighted terms use (m_j a_i + m_i a_j) grad W_ij =
+//     (a_i + m_i (a_j / m_j)) J_ij with a_j / m_j stored per particle;
 //   * tiles: (scene, first slot, end slot, first row) -- a CTA never spans
 //     two scenes, so per-scene reductions are per-CTA partials summed in a
 //     fixed order by the scene's last CTA (deterministic FP64).
@@ -40,6 +43,8 @@ struct SceneParams {
     float dt, inv_dt, omega, padding;
     float domain[3];
     float gravity[3];
+    float r2_max;              // largest FP32 d2 with sqrtf(d2) < h: `d2 <= r2_max` is the strict `|r| < h` test
+    float inv_h;
     float W0;                  // cubic_kernel(0, h)
     float cubic_k;             // 8/pi / h^3 (sph_kernel.py:14-15)
     float spiky_k;             // 45 / (pi h^6) (sph_kernel.py:55)
@@ -78,6 +83,8 @@ struct SceneCtl {
     int acc_last_failure;
     int acc_pad;
 };
+
+static_assert(sizeof(SceneCtl) % sizeof(double) == 0, "SceneCtl is read as doubles");
 
 struct Flags {
     int any_outer, any_solve, any_cg, bad;
@@ -135,8 +142,11 @@ struct Dev {
     float* y;
     float* s;
     float* fk;
+    float* inv_m;            // 1/m of dynamic slots (0 for static)
+    float* q;                // fk / m
+    float* z;                // y / m
     // neighbour rows
-    int2* nbr;
+    float4* nbr;
     int* nbr_cnt;
     int stride;
     // reductions
@@ -152,6 +162,10 @@ struct Dev {
     // advect leaves scenes whose last solve raised where they are (the
     // reference raises before advecting, framework.py:483-513)
     int advect_skip_failed;
+    // persistent solve: grid-barrier words and the phase budget
+    unsigned* bar_count;
+    unsigned* bar_gen;
+    long long phase_limit;
 };
 
 // ------------------------------------------------------------------ math
@@ -184,6 +198,27 @@ __device__ __forceinline__ float spiky_w(float rn, float h, float k) {
     float rc = rn < 1e-6f ? 1e-6f : rn;
     float t = h - rc;
     return (-k * (t * t)) / rc;
+}
+
+// |r|^2 rounded exactly as the reference's wp.length computes it before the
+// square root: ((x*x + y*y) + z*z), every product and sum rounded (no FMA).
+__device__ __forceinline__ float norm2_rn(float3 r) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(r.x, r.x), __fmul_rn(r.y, r.y)), __fmul_rn(r.z, r.z));
+}
+
+// cubic spline from q = r/h (sph_kernel.py:8-25)
+__device__ __forceinline__ float cubic_Wq(float q, float k) {
+    float res = 0.0f;
+    if (q <= 1.0f) {
+        if (q <= 0.5f) {
+            const float q2 = q * q;
+            res = k * (6.0f * (q2 * q) - 6.0f * q2 + 1.0f);
+        } else {
+            const float f = 1.0f - q;
+            res = k * 2.0f * f * f * f;
+        }
+    }
+    return res;
 }
 
 __device__ __forceinline__ int cell_coord(float v, float inv, int dim) {

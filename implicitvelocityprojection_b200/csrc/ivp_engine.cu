@@ -62,6 +62,10 @@ struct ivp_engine {
     int n_scenes = 0;
     bool bound = false;
     bool want_divergence = false;
+    // persistent solve
+    bool persistent = false;
+    int coop_grid = 0;
+    size_t coop_smem = 0;
     // graphs
     cudaGraph_t graph_step = nullptr, graph_solve = nullptr, graph_build = nullptr;
     cudaGraphExec_t exec_step = nullptr, exec_solve = nullptr, exec_build = nullptr;
@@ -95,7 +99,15 @@ struct Launcher {
     bool has_last = false;
     Prof* prof = nullptr;
 
-    int kernel(int id, const void* fn, dim3 grid, dim3 block, void** args) {
+    int launch_now(const void* fn, dim3 grid, dim3 block, void** args, size_t smem, bool coop) {
+        if (coop) {
+            CK(cudaLaunchCooperativeKernel(fn, grid, block, args, smem, stream));
+        } else {
+            CK(cudaLaunchKernel(fn, grid, block, args, smem, stream));
+        }
+        return IVP_OK;
+    }
+    int kernel(int id, const void* fn, dim3 grid, dim3 block, void** args, size_t smem = 0, bool coop = false) {
         if (grid.x == 0) return IVP_OK;
         if (!graph) {
             if (prof) {
@@ -106,24 +118,29 @@ struct Launcher {
                     prof->ev.push_back(ev);
                 }
                 CK(cudaEventRecord(prof->ev[2 * k], stream));
-                CK(cudaLaunchKernel(fn, grid, block, args, 0, stream));
+                CKS(launch_now(fn, grid, block, args, smem, coop));
                 CK(cudaEventRecord(prof->ev[2 * k + 1], stream));
                 prof->ids.push_back(id);
                 return IVP_OK;
             }
-            CK(cudaLaunchKernel(fn, grid, block, args, 0, stream));
-            return IVP_OK;
+            return launch_now(fn, grid, block, args, smem, coop);
         }
         cudaKernelNodeParams p;
         memset(&p, 0, sizeof(p));
         p.func = const_cast<void*>(fn);
         p.gridDim = grid;
         p.blockDim = block;
-        p.sharedMemBytes = 0;
+        p.sharedMemBytes = (unsigned)smem;
         p.kernelParams = args;
         p.extra = nullptr;
         cudaGraphNode_t n;
         CK(cudaGraphAddKernelNode(&n, graph, has_last ? &last : nullptr, has_last ? 1 : 0, &p));
+        if (coop) {
+            cudaKernelNodeAttrValue v;
+            memset(&v, 0, sizeof(v));
+            v.cooperative = 1;
+            CK(cudaGraphKernelNodeSetAttribute(n, cudaLaunchAttributeCooperative, &v));
+        }
         last = n;
         has_last = true;
         return IVP_OK;
@@ -167,24 +184,35 @@ struct Kern {
 };
 
 struct KernelSet {
-    DevKernel pack, rhs, cg_a, cg_b, dens, aii, div;
+    DevKernel pack, rhs, cg_a, cg_b, dens, aii, div, persist;
 };
 
-template <int G>
+template <int G, int B>
 KernelSet make_set() {
-    constexpr int B = 128;
     return {Kern<G, B>::pack(), Kern<G, B>::rhs(), Kern<G, B>::cg_a(), Kern<G, B>::cg_b(),
-            Kern<G, B>::dens(), Kern<G, B>::aii(), Kern<G, B>::div()};
+            Kern<G, B>::dens(), Kern<G, B>::aii(), Kern<G, B>::div(), k_ip_persistent<G, B>};
 }
 
-bool kernel_set(int G, KernelSet* out) {
-    switch (G) {
-        case 1: *out = make_set<1>(); return true;
-        case 2: *out = make_set<2>(); return true;
-        case 4: *out = make_set<4>(); return true;
-        case 8: *out = make_set<8>(); return true;
-        default: return false;
+// Instantiated launch shapes: G lanes per particle x {128, 256} threads.
+bool kernel_set(int G, int B, KernelSet* out) {
+    if (B == 128) {
+        switch (G) {
+            case 1: *out = make_set<1, 128>(); return true;
+            case 2: *out = make_set<2, 128>(); return true;
+            case 4: *out = make_set<4, 128>(); return true;
+            case 8: *out = make_set<8, 128>(); return true;
+            default: return false;
+        }
     }
+    if (B == 256) {
+        switch (G) {
+            case 2: *out = make_set<2, 256>(); return true;
+            case 4: *out = make_set<4, 256>(); return true;
+            case 8: *out = make_set<8, 256>(); return true;
+            default: return false;
+        }
+    }
+    return false;
 }
 
 int emit_build(ivp_engine* e, Launcher& L) {
@@ -206,7 +234,14 @@ int emit_build(ivp_engine* e, Launcher& L) {
     }
     CKS(L.dev(IVP_K_PLACE, k_place, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D));
     CKS(L.dev(IVP_K_ORDER, k_order, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D));
-    CKS(L.dev(IVP_K_NBR_BUILD, k_nbr_build, e->n_tiles, e->T, D));
+    {
+        // 8 lanes per particle for the candidate scan (at most 256 threads)
+        DevKernel nb = e->T <= 32 ? (DevKernel)k_nbr_build<8> : e->T <= 64 ? (DevKernel)k_nbr_build<4>
+                                                                             : (DevKernel)k_nbr_build<2>;
+        const int lanes = e->T <= 32 ? 8 : e->T <= 64 ? 4 : 2;
+        if (e->T * lanes > 256) return IVP_ERR_BAD_ARG;
+        CKS(L.dev(IVP_K_NBR_BUILD, nb, e->n_tiles, e->T * lanes, D));
+    }
     CKS(L.dev(IVP_K_STATIC_OUT, k_static_outputs, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D));
     return IVP_OK;
 }
@@ -229,7 +264,7 @@ int add_conditional(cudaGraph_t g, Launcher& L, cudaGraphConditionalHandle h, cu
 // (device-side control) or driven from the host with flag read-backs.
 int emit_solve_loop(ivp_engine* e, Launcher& L) {
     KernelSet K;
-    if (!kernel_set(e->G, &K)) return IVP_ERR_BAD_ARG;
+    if (!kernel_set(e->G, e->BLOCK, &K)) return IVP_ERR_BAD_ARG;
     const int nt = e->n_tiles, B = e->BLOCK;
     if (nt == 0) return IVP_OK;
     if (!L.graph) {
@@ -288,12 +323,21 @@ int emit_solve_loop(ivp_engine* e, Launcher& L) {
 
 int emit_solve(ivp_engine* e, Launcher& L) {
     if (e->n_tiles == 0) return IVP_OK;
+    if (e->persistent) {
+        KernelSet K;
+        kernel_set(e->G, e->BLOCK, &K);
+        CKS(L.memset0(e->D.bar_count, sizeof(unsigned)));
+        Dev copy = e->D;
+        void* args[] = {&copy};
+        return L.kernel(IVP_K_PERSISTENT, (const void*)K.persist, dim3(e->coop_grid), dim3(e->BLOCK), args,
+                        e->coop_smem, true);
+    }
     CKS(L.dev(IVP_K_SOLVE_BEGIN, k_solve_begin, e->n_tiles, e->T, e->D));
     CKS(emit_solve_loop(e, L));
     CKS(L.dev(IVP_K_SOLVE_END, k_solve_end, e->n_tiles, e->T, e->D));
     if (e->want_divergence && e->D.div_out) {
         KernelSet K;
-        kernel_set(e->G, &K);
+        kernel_set(e->G, e->BLOCK, &K);
         CKS(L.dev(IVP_K_DIVERGENCE, K.div, e->n_tiles, e->BLOCK, e->D));
     }
     return IVP_OK;
@@ -355,7 +399,11 @@ int validate(const ivp_scene_desc* sc, int n, const ivp_options* o) {
     if (o->lanes_per_particle != 1 && o->lanes_per_particle != 2 && o->lanes_per_particle != 4 &&
         o->lanes_per_particle != 8)
         return IVP_ERR_BAD_ARG;
-    if (o->particles_per_block <= 0 || o->particles_per_block * o->lanes_per_particle != 128) return IVP_ERR_BAD_ARG;
+    {
+        KernelSet K;
+        if (o->particles_per_block <= 0 || !kernel_set(o->lanes_per_particle, o->particles_per_block * o->lanes_per_particle, &K))
+            return IVP_ERR_BAD_ARG;
+    }
     if (o->list_stride <= 0 || o->max_hist <= 0) return IVP_ERR_BAD_ARG;
     long expect = 0;
     for (int s = 0; s < n; ++s) {
@@ -400,6 +448,15 @@ void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
         const float h = 4.0f * d.particle_radius;  // config_builder.py:51-52
         q.h = h;
         q.cell_inv = 1.0f / h;
+        q.inv_h = 1.0f / h;
+        {
+            // largest float d2 with sqrtf(d2) < h (IEEE sqrt is monotone and
+            // correctly rounded on host and device alike)
+            float t = h * h;
+            while (std::sqrt(t) >= h) t = std::nextafter(t, 0.0f);
+            while (std::sqrt(std::nextafter(t, INFINITY)) < h) t = std::nextafter(t, INFINITY);
+            q.r2_max = t;
+        }
         long ncell = 1;
         for (int a = 0; a < 3; ++a) {
             // neighbour_search.py:105-107
@@ -473,7 +530,7 @@ void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
     P.off[i++] = L.add(sizeof(float) * N);                  // 24 y
     P.off[i++] = L.add(sizeof(float) * N);                  // 25 s
     P.off[i++] = L.add(sizeof(float) * N);                  // 26 fk
-    P.off[i++] = L.add(sizeof(int2) * (size_t)P.n_dyn * (size_t)o->list_stride);  // 27 nbr
+    P.off[i++] = L.add(sizeof(float4) * (size_t)P.n_dyn * (size_t)o->list_stride);  // 27 nbr
     P.off[i++] = L.add(sizeof(int) * std::max<size_t>((size_t)P.n_dyn, 1));       // 28 nbr_cnt
     P.off[i++] = L.add(sizeof(double) * NT);                // 29 partial
     P.off[i++] = L.add(sizeof(int) * S);                    // 30 scene_counter
@@ -482,6 +539,10 @@ void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
     P.off[i++] = L.add(sizeof(double) * S * (size_t)o->max_hist);  // 33 err_hist
     P.off[i++] = L.add(sizeof(int) * S * (size_t)o->max_hist);     // 34 pcg_hist
     P.off[i++] = L.add(sizeof(unsigned long long) * S);            // 35 pairs
+    P.off[i++] = L.add(2 * sizeof(unsigned));                        // 36 barrier words
+    P.off[i++] = L.add(sizeof(float) * N);                           // 37 inv_m
+    P.off[i++] = L.add(sizeof(float) * N);                           // 38 q
+    P.off[i++] = L.add(sizeof(float) * N);                           // 39 z
 }
 
 cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
@@ -564,7 +625,7 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
     D.y = reinterpret_cast<float*>(w + P.off[i++]);
     D.s = reinterpret_cast<float*>(w + P.off[i++]);
     D.fk = reinterpret_cast<float*>(w + P.off[i++]);
-    D.nbr = reinterpret_cast<int2*>(w + P.off[i++]);
+    D.nbr = reinterpret_cast<float4*>(w + P.off[i++]);
     D.nbr_cnt = reinterpret_cast<int*>(w + P.off[i++]);
     D.partial = reinterpret_cast<double*>(w + P.off[i++]);
     D.scene_counter = reinterpret_cast<int*>(w + P.off[i++]);
@@ -573,6 +634,17 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
     D.err_hist = reinterpret_cast<double*>(w + P.off[i++]);
     D.pcg_hist = reinterpret_cast<int*>(w + P.off[i++]);
     D.pairs = reinterpret_cast<unsigned long long*>(w + P.off[i++]);
+    D.bar_count = reinterpret_cast<unsigned*>(w + P.off[i]);
+    D.bar_gen = reinterpret_cast<unsigned*>(w + P.off[i++]) + 1;
+    D.inv_m = reinterpret_cast<float*>(w + P.off[i++]);
+    D.q = reinterpret_cast<float*>(w + P.off[i++]);
+    D.z = reinterpret_cast<float*>(w + P.off[i++]);
+    {
+        long long lim = 64;
+        for (int sc = 0; sc < n_scenes; ++sc)
+            lim += (long long)(scenes[sc].max_outer_iters + 1) * (long long)(2 * scenes[sc].max_iteration_pcg + 3);
+        D.phase_limit = lim;
+    }
     D.n_scenes = n_scenes;
     D.n_tiles = e->n_tiles;
     D.n_keys = e->n_keys;
@@ -605,6 +677,23 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
         return fail(IVP_ERR_CUDA);
     // the host vectors go out of scope: make the copies complete first
     if (cudaStreamSynchronize(s) != cudaSuccess) return fail(IVP_ERR_CUDA);
+    // persistent solve: a co-resident grid of at most one CTA per tile
+    e->persistent = false;
+    if (opt->persistent && e->n_tiles > 0 && n_scenes <= 256) {
+        int dev = 0, coop = 0, nsm = 0, per_sm = 0;
+        KernelSet K;
+        kernel_set(e->G, e->BLOCK, &K);
+        e->coop_smem = (size_t)n_scenes * (sizeof(double) + sizeof(SceneCtl));
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) == cudaSuccess && coop &&
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)K.persist, e->BLOCK, e->coop_smem) ==
+                cudaSuccess &&
+            per_sm > 0) {
+            e->coop_grid = std::min(e->n_tiles, per_sm * nsm);
+            e->persistent = true;
+        }
+    }
     *out = e;
     return IVP_OK;
 }
@@ -677,7 +766,7 @@ int ivp_compute_density(ivp_engine* e, void* stream) {
     if (!e) return IVP_ERR_BAD_ARG;
     if (!e->bound) return IVP_ERR_NOT_BOUND;
     KernelSet K;
-    kernel_set(e->G, &K);
+    kernel_set(e->G, e->BLOCK, &K);
     Launcher L;
     L.stream = as_stream(stream);
     return L.dev(IVP_K_PACK, K.dens, e->n_tiles, e->BLOCK, e->D);
@@ -687,7 +776,7 @@ int ivp_compute_aii(ivp_engine* e, void* stream) {
     if (!e) return IVP_ERR_BAD_ARG;
     if (!e->bound) return IVP_ERR_NOT_BOUND;
     KernelSet K;
-    kernel_set(e->G, &K);
+    kernel_set(e->G, e->BLOCK, &K);
     Launcher L;
     L.stream = as_stream(stream);
     CKS(L.dev(IVP_K_PACK, K.aii, e->n_tiles, e->BLOCK, e->D));

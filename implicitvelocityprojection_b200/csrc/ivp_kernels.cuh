@@ -31,16 +31,16 @@ __device__ __forceinline__ void flag_bad(const Dev& D, int idx, int where) {
 
 // ---------------------------------------------------------------- control
 
-// Scene-level decision after a reduction (runs in one thread of the scene's
-// last CTA).  `s` is the FP64 sum over the scene's dynamic particles.
-__device__ void scene_finalize(const Dev& D, int sc, int kind, double s) {
-    const SceneParams& P = D.scenes[sc];
-    SceneCtl& C = D.ctl[sc];
+// Scene-level decision after a reduction (one thread).  `s` is the FP64 sum
+// over the scene's dynamic particles.  `C` is the scene's control block (in
+// global memory for the launch-per-phase path, a per-CTA shared-memory copy
+// for the persistent path); history is written when `hist` is set.
+__device__ void scene_decide(const Dev& D, const SceneParams& P, SceneCtl& C, int kind, double s, bool hist) {
     if (kind == K_PACK) {
         // pressure_base.py:405-423 average, ip.py:364-370 stopping rule
         const double err = P.n_dyn > 0 ? s / (double)P.n_dyn : 0.0;
         C.err = err;
-        if (C.n_err < D.hist_len) D.err_hist[P.hist_base + C.n_err] = err;
+        if (hist && C.n_err < D.hist_len) D.err_hist[P.hist_base + C.n_err] = err;
         C.n_err += 1;
         const bool converged = err < P.tol_opt && !P.fixed_iters;
         if ((converged && C.outer_it >= 1) || C.outer_it >= P.max_outer) {
@@ -62,7 +62,7 @@ __device__ void scene_finalize(const Dev& D, int sc, int kind, double s) {
             C.cg_active = 1;
         } else {
             C.cg_active = 0;
-            if (C.outer_it < D.hist_len) D.pcg_hist[P.hist_base + C.outer_it] = 0;
+            if (hist && C.outer_it < D.hist_len) D.pcg_hist[P.hist_base + C.outer_it] = 0;
             C.outer_it += 1;
             C.solve_pending = 0;
         }
@@ -85,7 +85,7 @@ __device__ void scene_finalize(const Dev& D, int sc, int kind, double s) {
         C.total_cg += 1;
         if ((rr_new < P.tol_pcg && C.cg_it >= 2) || C.cg_it >= P.max_pcg) {
             C.cg_active = 0;
-            if (C.outer_it < D.hist_len) D.pcg_hist[P.hist_base + C.outer_it] = C.cg_it;
+            if (hist && C.outer_it < D.hist_len) D.pcg_hist[P.hist_base + C.outer_it] = C.cg_it;
             C.outer_it += 1;
             C.solve_pending = 0;
         } else {
@@ -93,6 +93,36 @@ __device__ void scene_finalize(const Dev& D, int sc, int kind, double s) {
             C.rr_old = rr_new;
         }
     }
+}
+
+__device__ void scene_finalize(const Dev& D, int sc, int kind, double s) {
+    scene_decide(D, D.scenes[sc], D.ctl[sc], kind, s, true);
+}
+
+// A scene's sum of its tile partials, one fixed association for every path:
+// lane l of one warp adds tiles tb+l, tb+l+32, ... in order, then an xor tree
+// (valid in every lane).
+__device__ __forceinline__ double scene_sum_warp(const double* partial, int tb, int te) {
+    const int l = threadIdx.x & 31;
+    double s = 0.0;
+    for (int t = tb + l; t < te; t += 32) s += __ldcg(partial + t);
+    return warp_sum_d(s);
+}
+
+// Control-block reset at the start of IP.solve (reset_stats,
+// pressure_base.py:497-502).
+__device__ __forceinline__ void ctl_begin(const SceneParams& P, SceneCtl& C) {
+    C.err = 0.0;
+    C.rr_old = C.pap = C.alpha = C.beta = C.rr0 = 0.0;
+    C.final_err = 0.0;
+    C.outer_it = 0;
+    C.cg_it = 0;
+    C.outer_active = P.n_dyn > 0 ? 1 : 0;
+    C.solve_pending = 0;
+    C.cg_active = 0;
+    C.status = IVP_OK_;
+    C.n_err = 0;
+    C.total_cg = 0;
 }
 
 // Launch-level decision (one thread of the last CTA of the launch).
@@ -148,17 +178,16 @@ __device__ void block_finish(const Dev& D, int sc, bool active, double part, int
         }
     }
     __syncthreads();
-    if (sh_last) {
+    if (sh_last && threadIdx.x < 32) {
         __threadfence();
-        double s = 0.0;
-        for (int t = P.tile_begin + (int)threadIdx.x; t < P.tile_end; t += BLOCK) s += __ldcg(&D.partial[t]);
-        s = block_sum_d<BLOCK>(s, sh);
+        const double s = scene_sum_warp(D.partial, P.tile_begin, P.tile_end);
         if (threadIdx.x == 0) {
             D.scene_counter[sc] = 0;
             scene_finalize(D, sc, kind, s);
             __threadfence();
         }
     }
+    __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
         if (atomicAdd(D.launch_counter, 1) == (int)gridDim.x - 1) {
@@ -282,84 +311,148 @@ __global__ void k_order(const Dev D) {
     if ((slot < P.s_dyn_end) != (D.dyn[p] != 0) || slot < P.s_begin || slot >= P.s_end) flag_bad(D, p, 10);
     D.pid[slot] = p;
     D.inv[p] = slot;
-    D.xm[slot] = make_float4(D.x[3 * p], D.x[3 * p + 1], D.x[3 * p + 2], D.m[p]);
+    const float m = D.m[p];
+    D.xm[slot] = make_float4(D.x[3 * p], D.x[3 * p + 1], D.x[3 * p + 2], m);
     D.rho0s[slot] = D.rho0[p];
+    D.inv_m[slot] = D.dyn[p] ? __frcp_rn(m) : 0.0f;  // the reference's m_inv (simulation_data.py:53-56)
 }
 
 // Neighbour lists of every dynamic particle (build_neighbor_cache,
 // neighbour_search.py:10-51: j != i, |x_i - x_j| < h strict, first
 // cache_size kept) fused with the density sum (pressure_base.py:12-46), the
 // diagonal k = 1/(Aii + 1e-3) (pressure_base.py:49-87) and the constraint
-// c = rho - rho0 (pressure_base.py:169-184).  One thread per particle; the
-// 3 x-adjacent cells of a (y, z) row are one contiguous slot range.
-__global__ void k_nbr_build(const Dev D) {
+// c = rho - rho0 (pressure_base.py:169-184).
+//
+// G lanes share one particle: the 3 x-adjacent cells of each (y, z) row are
+// one contiguous slot range, which the group walks G candidates at a time
+// (coalesced float4 loads).  A group ballot orders the hits of each round by
+// slot, so the list keeps the exact sequential candidate order (rows dz, dy
+// ascending; dynamic cells before static cells; slots ascending) and the
+// first-cache_size truncation of the sequential scan.
+template <int G>
+__global__ void __launch_bounds__(256, 4) k_nbr_build(const Dev D) {
+    constexpr int NG = 256 / G;  // groups (particles) per CTA at most
+    __shared__ int2 sh_rng[NG][18];
+    __shared__ int sh_pairs;
     const int4 tile = D.tiles[blockIdx.x];
-    const int i = tile.y + threadIdx.x;
-    if (i >= tile.z) return;
+    const int g = threadIdx.x / G, lane = threadIdx.x % G;
+    const int i = tile.y + g;
+    const bool valid = i < tile.z;
     const int sc = tile.x;
     const SceneParams& P = D.scenes[sc];
-    const float4 xi4 = D.xm[i];
-    const float3 xi = f3(xi4);
-    const float mi = xi4.w;
-    const float h = P.h;
-    const int cx = cell_coord(xi.x, P.cell_inv, P.dims[0]);
-    const int cy = cell_coord(xi.y, P.cell_inv, P.dims[1]);
-    const int cz = cell_coord(xi.z, P.cell_inv, P.dims[2]);
-    const int row = tile.w + threadIdx.x;
-    int2* out = D.nbr + (size_t)row * D.stride;
-    const int cap = P.cache < D.stride ? P.cache : D.stride;
-    float rho = 0.0f;
-    rho = rho + mi * P.W0;
-    float aii = 0.0f;
-    float3 jii = make_float3(0.0f, 0.0f, 0.0f);
-    int cnt = 0, found = 0;
-    const int x0 = cx > 0 ? cx - 1 : 0;
-    const int x1 = cx < P.dims[0] - 1 ? cx + 1 : P.dims[0] - 1;
-    for (int dz = -1; dz <= 1; ++dz) {
-        const int z = cz + dz;
-        if (z < 0 || z >= P.dims[2]) continue;
-        for (int dy = -1; dy <= 1; ++dy) {
-            const int yy = cy + dy;
-            if (yy < 0 || yy >= P.dims[1]) continue;
-            const int cb = (z * P.dims[1] + yy) * P.dims[0];
-#pragma unroll 1
-            for (int pass = 0; pass < 2; ++pass) {
-                const int kb = P.key_base + (pass ? P.ncell : 0) + cb;
-                const int jb = D.cell_start[kb + x0], je = D.cell_start[kb + x1 + 1];
-                for (int j = jb; j < je; ++j) {
-                    if (j == i) continue;
-                    const float4 xj4 = D.xm[j];
-                    const float3 r = sub3(xi, f3(xj4));
-                    const float rn = sqrtf(dot3(r, r));
-                    if (rn < h) {
-                        ++found;
-                        if (cnt < cap) {
-                            const float w = spiky_w(rn, h, P.spiky_k);
-                            out[cnt] = make_int2(j, __float_as_int(w));
-                            const float mj = xj4.w;
-                            rho += mj * cubic_W(rn, h, P.cubic_k);
-                            const float3 g = scale3(w, r);
-                            const float3 J = scale3(mj, g);
-                            if (j < P.s_dyn_end) aii += dot3(J, J) * (1.0f / mj);
-                            jii = sub3(jii, J);
-                            ++cnt;
-                        }
-                    }
-                }
+    const int wl = threadIdx.x & 31;
+    const int gshift = wl & ~(G - 1);
+    const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << gshift;
+    const unsigned below = (1u << lane) - 1u;
+    if (threadIdx.x == 0) sh_pairs = 0;
+    float3 xi = make_float3(0.f, 0.f, 0.f);
+    float mi = 1.0f;
+    int cx = 0, cy = 0, cz = 0;
+    if (valid) {
+        const float4 xi4 = D.xm[i];
+        xi = f3(xi4);
+        mi = xi4.w;
+        cx = cell_coord(xi.x, P.cell_inv, P.dims[0]);
+        cy = cell_coord(xi.y, P.cell_inv, P.dims[1]);
+        cz = cell_coord(xi.z, P.cell_inv, P.dims[2]);
+    }
+    // the 9 (dy, dz) rows x {dynamic, static} slot ranges, loaded together
+    {
+        const int x0 = cx > 0 ? cx - 1 : 0;
+        const int x1 = cx < P.dims[0] - 1 ? cx + 1 : P.dims[0] - 1;
+        for (int q = lane; q < 18; q += G) {
+            const int rr = q >> 1, pass = q & 1;
+            const int z = cz + rr / 3 - 1, yy = cy + rr % 3 - 1;
+            int2 rg = make_int2(0, 0);
+            if (valid && z >= 0 && z < P.dims[2] && yy >= 0 && yy < P.dims[1]) {
+                const int kb = P.key_base + (pass ? P.ncell : 0) + (z * P.dims[1] + yy) * P.dims[0];
+                rg = make_int2(__ldg(D.cell_start + kb + x0), __ldg(D.cell_start + kb + x1 + 1));
             }
+            sh_rng[g][q] = rg;
         }
     }
-    aii += dot3(jii, jii) * (1.0f / mi);
-    const float kd = 1.0f / (aii + 1e-3f);
-    D.nbr_cnt[row] = cnt;
-    D.dens[i] = rho;
-    D.kd[i] = kd;
-    D.c[i] = rho - D.rho0s[i];
-    const int p = D.pid[i];
-    D.density_out[p] = rho;
-    D.k_out[p] = kd;
-    if (found > cap) atomicAdd(&D.overflow[sc], 1);
-    atomicAdd(&D.pairs[sc], (unsigned long long)cnt);
+    __syncthreads();
+    const float h = P.h, inv_h = P.inv_h, r2max = P.r2_max, spk = P.spiky_k, ck = P.cubic_k;
+    const int dyn_end = P.s_dyn_end;
+    const int row = tile.w + g;
+    float4* out = D.nbr + (size_t)row * D.stride;
+    const int cap = P.cache < D.stride ? P.cache : D.stride;
+    float rho = 0.0f, aii = 0.0f;
+    float3 jii = make_float3(0.0f, 0.0f, 0.0f);
+    int cnt = 0, found = 0;
+    // candidate j: test, then (in slot order, via the group ballot) store
+    auto visit = [&](int j, int je) {
+        bool hit = false;
+        float4 xj4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        float3 r = make_float3(0.f, 0.f, 0.f);
+        float d2 = 0.0f;
+        if (j < je && j != i) {
+            xj4 = __ldg(D.xm + j);
+            r = sub3(xi, f3(xj4));
+            d2 = norm2_rn(r);
+            hit = d2 <= r2max;
+        }
+        const unsigned ball = (__ballot_sync(gmask, hit) >> gshift);
+        const int pos = cnt + __popc(ball & below);
+        if (hit && pos < cap) {
+            // spiky gradient (sph_kernel.py:52-61): -k (h - |r|)^2 r / |r|
+            const float rn = sqrtf(d2);
+            const float rc = rn < 1e-6f ? 1e-6f : rn;
+            const float t = h - rc;
+            const float sg = -spk * (t * t);
+            const float ir = __frcp_rn(rc);
+            const float mj = xj4.w;
+            const float3 J = make_float3(mj * (sg * (r.x * ir)), mj * (sg * (r.y * ir)), mj * (sg * (r.z * ir)));
+            out[pos] = make_float4(J.x, J.y, J.z, __int_as_float(j));
+            rho += mj * cubic_Wq(rn * inv_h, ck);
+            if (j < dyn_end) aii += dot3(J, J) * __frcp_rn(mj);
+            jii = sub3(jii, J);
+        }
+        const int nh = __popc(ball);
+        found += nh;
+        cnt = min(cnt + nh, cap);
+    };
+    if (valid) {
+#pragma unroll 1
+        for (int q = 0; q < 18; ++q) {
+            const int2 rg = sh_rng[g][q];
+            const int jb = rg.x, je = rg.y;
+            int base = jb;
+            // two candidate rounds per iteration keep two loads in flight
+            for (; base + G < je; base += 2 * G) {
+                visit(base + lane, je);
+                visit(base + G + lane, je);
+            }
+            if (base < je) visit(base + lane, je);
+        }
+    }
+    rho = group_sum<G>(rho);
+    aii = group_sum<G>(aii);
+    jii.x = group_sum<G>(jii.x);
+    jii.y = group_sum<G>(jii.y);
+    jii.z = group_sum<G>(jii.z);
+    if (valid && lane == 0) {
+        float dens = 0.0f;
+        dens = dens + mi * P.W0;
+        dens += rho;
+        aii += dot3(jii, jii) * __frcp_rn(mi);
+        const float kd = __frcp_rn(aii + 1e-3f);
+        D.nbr_cnt[row] = cnt;
+        D.dens[i] = dens;
+        D.kd[i] = kd;
+        D.c[i] = dens - D.rho0s[i];
+        const int p = D.pid[i];
+        D.density_out[p] = dens;
+        D.k_out[p] = kd;
+        if (found > cap) atomicAdd(&D.overflow[sc], 1);
+    }
+    // one pair-count atomic per CTA (every tile belongs to one scene)
+    int c = (valid && lane == 0) ? cnt : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(&sh_pairs, c);
+    __syncthreads();
+    if (threadIdx.x == 0 && sh_pairs) atomicAdd(&D.pairs[sc], (unsigned long long)sh_pairs);
 }
 
 // Static particles: the reference zeroes their k (pressure_base.py:65-67) and
@@ -382,7 +475,7 @@ __global__ void __launch_bounds__(BLOCK) k_density(const Dev D) {
     const bool valid = i < tile.z;
     const int row = tile.w + g;
     const int cnt = valid ? D.nbr_cnt[row] : 0;
-    const int2* nb = D.nbr + (size_t)row * D.stride;
+    const float4* nb = D.nbr + (size_t)row * D.stride;
     float3 xi = make_float3(0.f, 0.f, 0.f);
     int pi = 0;
     if (valid) {
@@ -391,7 +484,7 @@ __global__ void __launch_bounds__(BLOCK) k_density(const Dev D) {
     }
     float acc = 0.0f;
     for (int k = lane; k < cnt; k += G) {
-        const int j = nb[k].x;
+        const int j = __float_as_int(nb[k].w);
         const int pj = D.pid[j];
         const float3 r = sub3(xi, make_float3(D.x[3 * pj], D.x[3 * pj + 1], D.x[3 * pj + 2]));
         acc += D.m[pj] * cubic_W(sqrtf(dot3(r, r)), P.h, P.cubic_k);
@@ -417,15 +510,14 @@ __global__ void __launch_bounds__(BLOCK) k_aii(const Dev D) {
     const bool valid = i < tile.z;
     const int row = tile.w + g;
     const int cnt = valid ? D.nbr_cnt[row] : 0;
-    const int2* nb = D.nbr + (size_t)row * D.stride;
+    const float4* nb = D.nbr + (size_t)row * D.stride;
     const float4 xi4 = valid ? D.xm[i] : make_float4(0.f, 0.f, 0.f, 1.f);
     float aii = 0.0f, jx = 0.0f, jy = 0.0f, jz = 0.0f;
     for (int k = lane; k < cnt; k += G) {
-        const int2 e = nb[k];
-        const float4 xj = D.xm[e.x];
-        const float3 gw = scale3(__int_as_float(e.y), sub3(f3(xi4), f3(xj)));
-        const float3 J = scale3(xj.w, gw);
-        if (e.x < P.s_dyn_end) aii += dot3(J, J) * (1.0f / xj.w);
+        const float4 e = nb[k];
+        const int j = __float_as_int(e.w);
+        const float3 J = f3(e);
+        if (j < P.s_dyn_end) aii += dot3(J, J) * __frcp_rn(D.xm[j].w);
         jx -= J.x;
         jy -= J.y;
         jz -= J.z;
@@ -436,8 +528,8 @@ __global__ void __launch_bounds__(BLOCK) k_aii(const Dev D) {
     jz = group_sum<G>(jz);
     if (valid && lane == 0) {
         const float3 jii = make_float3(jx, jy, jz);
-        aii += dot3(jii, jii) * (1.0f / xi4.w);
-        const float kd = 1.0f / (aii + 1e-3f);
+        aii += dot3(jii, jii) * __frcp_rn(xi4.w);
+        const float kd = __frcp_rn(aii + 1e-3f);
         D.kd[i] = kd;
         D.k_out[D.pid[i]] = kd;
     }
@@ -469,20 +561,7 @@ __global__ void k_solve_begin(const Dev D) {
         D.flags->launches = 0;
         D.flags->timeout = 0;
     }
-    if (blockIdx.x == P.tile_begin && threadIdx.x == 0) {
-        SceneCtl& C = D.ctl[tile.x];
-        C.err = 0.0;
-        C.rr_old = C.pap = C.alpha = C.beta = C.rr0 = 0.0;
-        C.final_err = 0.0;
-        C.outer_it = 0;
-        C.cg_it = 0;
-        C.outer_active = P.n_dyn > 0 ? 1 : 0;
-        C.solve_pending = 0;
-        C.cg_active = 0;
-        C.status = IVP_OK_;
-        C.n_err = 0;
-        C.total_cg = 0;
-    }
+    if (blockIdx.x == P.tile_begin && threadIdx.x == 0) ctl_begin(P, D.ctl[tile.x]);
     const int i = tile.y + threadIdx.x;
     if (i >= tile.z) return;
     const int p = D.pid[i];
@@ -564,7 +643,36 @@ __global__ void k_advect(const Dev D) {
 
 // ------------------------------------------------------------- IP solve
 
-// Shared prologue of the neighbour-sum kernels: tile, scene, activity flag.
+// Pair-loop unroll: each lane loads PU list entries before gathering, so PU
+// independent gather chains are in flight.  Entries past the row end become
+// (self, w = 0), which contributes exactly 0; entries outside the scene are
+// redirected to self and reported once after the loop.
+constexpr int PU = 4;
+
+struct PairBatch {
+    int j[PU];
+    float3 J[PU];
+};
+
+template <int G>
+__device__ __forceinline__ bool load_pairs(const float4* __restrict__ nb, int k0, int cnt, int self, int lo, int hi,
+                                           PairBatch& b) {
+    bool bad = false;
+#pragma unroll
+    for (int u = 0; u < PU; ++u) {
+        const int k = k0 + u * G;
+        float4 e = make_float4(0.f, 0.f, 0.f, __int_as_float(self));
+        if (k < cnt) e = __ldg(nb + k);
+        const int j = __float_as_int(e.w);
+        const bool ok = j >= lo && j < hi;
+        bad |= !ok;
+        b.j[u] = ok ? j : self;
+        b.J[u] = ok ? f3(e) : make_float3(0.f, 0.f, 0.f);
+    }
+    return bad;
+}
+
+// Shared prologue of the neighbour-sum kernels: tile, scene, particle.
 struct TileCtx {
     int4 tile;
     int sc;
@@ -573,25 +681,243 @@ struct TileCtx {
 };
 
 template <int G>
-__device__ __forceinline__ TileCtx tile_ctx(const Dev& D) {
-    TileCtx t;
-    t.tile = D.tiles[blockIdx.x];
-    t.sc = t.tile.x;
-    t.g = threadIdx.x / G;
-    t.lane = threadIdx.x % G;
-    t.i = t.tile.y + t.g;
-    t.row = t.tile.w + t.g;
-    t.valid = t.i < t.tile.z;
-    return t;
+__device__ __forceinline__ TileCtx tile_ctx(const Dev& D, int t) {
+    TileCtx c;
+    c.tile = __ldg(D.tiles + t);
+    c.sc = c.tile.x;
+    c.g = threadIdx.x / G;
+    c.lane = threadIdx.x % G;
+    c.i = c.tile.y + c.g;
+    c.row = c.tile.w + c.g;
+    c.valid = c.i < c.tile.z;
+    return c;
 }
+
+// ---- per-tile bodies (return this thread's contribution to the FP64 partial)
 
 // ip_pack_fused (ip.py:124-171) + coef_wise_div + the average density error
 // (pressure_base.py:187-203), with the previous outer update d -= sol
-// (ip.py:389) applied on the fly.  Writes s = dfdt k and fk = f k for the
-// rhs and CG kernels.
+// (ip.py:389) applied on the fly (it = updates applied so far).  Writes
+// s = dfdt k and fk = f k for the rhs and CG phases.
+template <int G>
+__device__ __forceinline__ double pack_tile(const Dev& D, const SceneParams& P, const TileCtx& T, int it) {
+    const bool upd = it >= 1;
+    const float4* src = (upd && ((it - 1) & 1)) ? D.d1 : D.d0;
+    float4* dst = (it & 1) ? D.d1 : D.d0;
+    const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
+    const float4* nb = D.nbr + (size_t)T.row * D.stride;
+    float3 xi = make_float3(0.f, 0.f, 0.f), di = xi;
+    if (T.valid) {
+        xi = f3(D.xm[T.i]);
+        di = f3(src[T.i]);
+        if (upd) di = sub3(di, f3(D.sol[T.i]));
+    }
+    float acc = 0.0f;
+    bool bad = false;
+    const int self = T.valid ? T.i : P.s_begin;
+    for (int k0 = T.lane; k0 < cnt; k0 += G * PU) {
+        PairBatch b;
+        bad |= load_pairs<G>(nb, k0, cnt, self, P.s_begin, P.s_end, b);
+#pragma unroll
+        for (int u = 0; u < PU; ++u) {
+            const int j = b.j[u];
+            float3 dj = f3(__ldcg(src + j));
+            if (upd) dj = sub3(dj, f3(__ldcg(D.sol + j)));
+            acc += dot3(sub3(di, dj), b.J[u]);
+        }
+    }
+    if (bad) flag_bad(D, T.i, 1);
+    acc = group_sum<G>(acc);
+    double part = 0.0;
+    if (T.valid && T.lane == 0) {
+        if (upd) dst[T.i] = make_float4(di.x, di.y, di.z, 0.0f);
+        const float t = acc + D.c[T.i];
+        const float f = t > 0.0f ? t : 0.0f;
+        const float kd = D.kd[T.i];
+        D.s[T.i] = (t >= 1e-6f) ? kd : 0.0f;
+        const float fk = f * kd;
+        D.fk[T.i] = fk;
+        D.q[T.i] = fk * D.inv_m[T.i];
+        const float r0 = D.rho0s[T.i];
+        const float q = f / (r0 < 1e-6f ? 1e-6f : r0);
+        part = (double)(q > 0.0f ? q : 0.0f);
+    }
+    return part;
+}
+
+// ip_rhs_fused (ip.py:174-215) fused with the CG start: sol = 0 (ip.py:384),
+// r = rhs, p_prev = 0, rr = r.r (ip.py:293-296).
+template <int G>
+__device__ __forceinline__ double rhs_tile(const Dev& D, const SceneParams& P, const TileCtx& T) {
+    const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
+    const float4* nb = D.nbr + (size_t)T.row * D.stride;
+    float3 xi = make_float3(0.f, 0.f, 0.f);
+    float fki = 0.0f, mi = 0.0f;
+    if (T.valid) {
+        const float4 a = D.xm[T.i];
+        xi = f3(a);
+        mi = a.w;
+        fki = D.fk[T.i];
+    }
+    float ax = 0.0f, ay = 0.0f, az = 0.0f;
+    bool bad = false;
+    const int self = T.valid ? T.i : P.s_begin;
+    for (int k0 = T.lane; k0 < cnt; k0 += G * PU) {
+        PairBatch b;
+        bad |= load_pairs<G>(nb, k0, cnt, self, P.s_begin, P.s_end, b);
+#pragma unroll
+        for (int u = 0; u < PU; ++u) {
+            const float wgt = fki + mi * __ldcg(D.q + b.j[u]);
+            ax += wgt * b.J[u].x;
+            ay += wgt * b.J[u].y;
+            az += wgt * b.J[u].z;
+        }
+    }
+    if (bad) flag_bad(D, T.i, 2);
+    ax = group_sum<G>(ax);
+    ay = group_sum<G>(ay);
+    az = group_sum<G>(az);
+    double part = 0.0;
+    if (T.valid && T.lane == 0) {
+        const float om = P.omega;
+        const float4 rhs = make_float4(om * ax, om * ay, om * az, 0.0f);
+        D.r[T.i] = rhs;
+        D.sol[T.i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        D.p0[T.i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        part = (double)dot3(f3(rhs), f3(rhs));
+    }
+    return part;
+}
+
+// CG phase A: p = r + beta p_prev (ip.py:323-327, formed on the fly for the
+// neighbours too), y = dfdt k (J p) (compute_Jx_pcg, ip.py:19-60), and the
+// FP64 partials of p^T A p = sum m |p|^2 + omega sum y (J p) (the value
+// dot(p, A p) of ip.py:307: the gather-form transpose is the exact transpose
+// of J for symmetric lists).
+template <int G>
+__device__ __forceinline__ double cga_tile(const Dev& D, const SceneParams& P, const TileCtx& T, float beta,
+                                           int cg_it) {
+    const float4* pp = (cg_it & 1) ? D.p1 : D.p0;
+    float4* pn = (cg_it & 1) ? D.p0 : D.p1;
+    const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
+    const float4* nb = D.nbr + (size_t)T.row * D.stride;
+    float3 xi = make_float3(0.f, 0.f, 0.f), pi = xi;
+    float mi = 0.0f;
+    if (T.valid) {
+        const float4 a = D.xm[T.i];
+        xi = f3(a);
+        mi = a.w;
+        const float4 ri = D.r[T.i], qi = pp[T.i];
+        pi = make_float3(ri.x + beta * qi.x, ri.y + beta * qi.y, ri.z + beta * qi.z);
+    }
+    float acc = 0.0f;
+    bool bad = false;
+    const int self = T.valid ? T.i : P.s_begin;
+    for (int k0 = T.lane; k0 < cnt; k0 += G * PU) {
+        PairBatch b;
+        bad |= load_pairs<G>(nb, k0, cnt, self, P.s_begin, P.s_end, b);
+#pragma unroll
+        for (int u = 0; u < PU; ++u) {
+            const int j = b.j[u];
+            const float4 rj = __ldcg(D.r + j), qj = __ldcg(pp + j);
+            const float3 pj = make_float3(rj.x + beta * qj.x, rj.y + beta * qj.y, rj.z + beta * qj.z);
+            acc += dot3(sub3(pi, pj), b.J[u]);
+        }
+    }
+    if (bad) flag_bad(D, T.i, 3);
+    acc = group_sum<G>(acc);
+    double part = 0.0;
+    if (T.valid && T.lane == 0) {
+        const float yi = acc * D.s[T.i];
+        D.y[T.i] = yi;
+        D.z[T.i] = yi * D.inv_m[T.i];
+        pn[T.i] = make_float4(pi.x, pi.y, pi.z, 0.0f);
+        part = (double)(mi * dot3(pi, pi)) + (double)P.omega * (double)yi * (double)acc;
+    }
+    return part;
+}
+
+// CG phase B: Ap = m p + omega J^T y in gather form (compute_Ax_part1/2,
+// ip.py:63-121, as pressure_base.py:130-166 writes J^T), x += alpha p,
+// r -= alpha Ap (pcg_update_x_r_scalar, math_utils.py:181-195), rr = r.r.
+template <int G>
+__device__ __forceinline__ double cgb_tile(const Dev& D, const SceneParams& P, const TileCtx& T, float alpha,
+                                           int cg_it) {
+    const float4* pc = (cg_it & 1) ? D.p0 : D.p1;
+    const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
+    const float4* nb = D.nbr + (size_t)T.row * D.stride;
+    float3 xi = make_float3(0.f, 0.f, 0.f);
+    float mi = 0.0f, yi = 0.0f;
+    if (T.valid) {
+        const float4 a = D.xm[T.i];
+        xi = f3(a);
+        mi = a.w;
+        yi = D.y[T.i];
+    }
+    float ax = 0.0f, ay = 0.0f, az = 0.0f;
+    bool bad = false;
+    const int self = T.valid ? T.i : P.s_begin;
+    for (int k0 = T.lane; k0 < cnt; k0 += G * PU) {
+        PairBatch b;
+        bad |= load_pairs<G>(nb, k0, cnt, self, P.s_begin, P.s_end, b);
+#pragma unroll
+        for (int u = 0; u < PU; ++u) {
+            const float wgt = yi + mi * __ldcg(D.z + b.j[u]);
+            ax += wgt * b.J[u].x;
+            ay += wgt * b.J[u].y;
+            az += wgt * b.J[u].z;
+        }
+    }
+    if (bad) flag_bad(D, T.i, 4);
+    ax = group_sum<G>(ax);
+    ay = group_sum<G>(ay);
+    az = group_sum<G>(az);
+    double part = 0.0;
+    if (T.valid && T.lane == 0) {
+        const float om = P.omega;
+        const float4 p4 = pc[T.i];
+        const float3 ap = make_float3(mi * p4.x + om * ax, mi * p4.y + om * ay, mi * p4.z + om * az);
+        float4 xs = D.sol[T.i], rs = D.r[T.i];
+        xs.x = xs.x + alpha * p4.x;
+        xs.y = xs.y + alpha * p4.y;
+        xs.z = xs.z + alpha * p4.z;
+        rs.x = rs.x - alpha * ap.x;
+        rs.y = rs.y - alpha * ap.y;
+        rs.z = rs.z - alpha * ap.z;
+        D.sol[T.i] = xs;
+        D.r[T.i] = rs;
+        part = (double)dot3(f3(rs), f3(rs));
+    }
+    return part;
+}
+
+// compute_divergence (pressure_base.py:449-457): max(J v, 0) with v = d/dt.
+template <int G>
+__device__ __forceinline__ void div_tile(const Dev& D, const SceneParams& P, const TileCtx& T, int outer_it) {
+    const float4* dc = (outer_it & 1) ? D.d1 : D.d0;
+    const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
+    const float4* nb = D.nbr + (size_t)T.row * D.stride;
+    const float s = P.inv_dt;
+    float3 xi = make_float3(0.f, 0.f, 0.f), vi = xi;
+    if (T.valid) {
+        xi = f3(D.xm[T.i]);
+        vi = scale3(s, f3(dc[T.i]));
+    }
+    float acc = 0.0f;
+    for (int k = T.lane; k < cnt; k += G) {
+        const float4 e = __ldg(nb + k);
+        const float3 vj = scale3(s, f3(__ldcg(dc + __float_as_int(e.w))));
+        acc += dot3(sub3(vi, vj), f3(e));
+    }
+    acc = group_sum<G>(acc);
+    if (T.valid && T.lane == 0 && D.div_out) D.div_out[D.pid[T.i]] = acc > 0.0f ? acc : 0.0f;
+}
+
+// ---- one launch per phase (device-side control through graph conditionals)
+
 template <int G, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_pack(const Dev D) {
-    const TileCtx T = tile_ctx<G>(D);
+    const TileCtx T = tile_ctx<G>(D, blockIdx.x);
     __shared__ int sh_active, sh_it;
     if (threadIdx.x == 0) {
         sh_active = D.ctl[T.sc].outer_active;
@@ -600,104 +926,25 @@ __global__ void __launch_bounds__(BLOCK) k_pack(const Dev D) {
     __syncthreads();
     const bool active = sh_active != 0;
     double part = 0.0;
-    if (active) {
-        const SceneParams& P = D.scenes[T.sc];
-        const int it = sh_it;
-        const bool upd = it >= 1;
-        const float4* src = (upd && ((it - 1) & 1)) ? D.d1 : D.d0;
-        float4* dst = (it & 1) ? D.d1 : D.d0;
-        const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
-        const int2* nb = D.nbr + (size_t)T.row * D.stride;
-        float3 xi = make_float3(0.f, 0.f, 0.f), di = xi;
-        if (T.valid) {
-            xi = f3(D.xm[T.i]);
-            di = f3(src[T.i]);
-            if (upd) di = sub3(di, f3(D.sol[T.i]));
-        }
-        float acc = 0.0f;
-        for (int k = T.lane; k < cnt; k += G) {
-            const int2 e = nb[k];
-            const int j = e.x;
-            if (j < P.s_begin || j >= P.s_end) { flag_bad(D, j, 1); continue; }
-            const float4 xj = D.xm[j];
-            const float3 gw = scale3(__int_as_float(e.y), sub3(xi, f3(xj)));
-            float3 dj = f3(src[j]);
-            if (upd) dj = sub3(dj, f3(D.sol[j]));
-            acc += xj.w * dot3(sub3(di, dj), gw);
-        }
-        acc = group_sum<G>(acc);
-        if (T.valid && T.lane == 0) {
-            if (upd) dst[T.i] = make_float4(di.x, di.y, di.z, 0.0f);
-            const float t = acc + D.c[T.i];
-            const float f = t > 0.0f ? t : 0.0f;
-            const float kd = D.kd[T.i];
-            D.s[T.i] = (t >= 1e-6f) ? kd : 0.0f;
-            D.fk[T.i] = f * kd;
-            const float r0 = D.rho0s[T.i];
-            const float q = f / (r0 < 1e-6f ? 1e-6f : r0);
-            part = (double)(q > 0.0f ? q : 0.0f);
-        }
-    }
+    if (active) part = pack_tile<G>(D, D.scenes[T.sc], T, sh_it);
     block_finish<BLOCK>(D, T.sc, active, part, K_PACK);
 }
 
-// ip_rhs_fused (ip.py:174-215) fused with the CG start: sol = 0 (ip.py:384),
-// r = rhs, p_prev = 0, rr = r.r (ip.py:293-296).
 template <int G, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_rhs(const Dev D) {
-    const TileCtx T = tile_ctx<G>(D);
+    const TileCtx T = tile_ctx<G>(D, blockIdx.x);
     __shared__ int sh_active;
     if (threadIdx.x == 0) sh_active = D.ctl[T.sc].solve_pending;
     __syncthreads();
     const bool active = sh_active != 0;
     double part = 0.0;
-    if (active) {
-        const SceneParams& P = D.scenes[T.sc];
-        const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
-        const int2* nb = D.nbr + (size_t)T.row * D.stride;
-        float3 xi = make_float3(0.f, 0.f, 0.f);
-        float fki = 0.0f, mi = 0.0f;
-        if (T.valid) {
-            const float4 a = D.xm[T.i];
-            xi = f3(a);
-            mi = a.w;
-            fki = D.fk[T.i];
-        }
-        float ax = 0.0f, ay = 0.0f, az = 0.0f;
-        for (int k = T.lane; k < cnt; k += G) {
-            const int2 e = nb[k];
-            const int j = e.x;
-            if (j < P.s_begin || j >= P.s_end) { flag_bad(D, j, 2); continue; }
-            const float4 xj = D.xm[j];
-            const float3 gw = scale3(__int_as_float(e.y), sub3(xi, f3(xj)));
-            const float wgt = xj.w * fki + mi * D.fk[j];
-            ax += wgt * gw.x;
-            ay += wgt * gw.y;
-            az += wgt * gw.z;
-        }
-        ax = group_sum<G>(ax);
-        ay = group_sum<G>(ay);
-        az = group_sum<G>(az);
-        if (T.valid && T.lane == 0) {
-            const float om = P.omega;
-            const float4 rhs = make_float4(om * ax, om * ay, om * az, 0.0f);
-            D.r[T.i] = rhs;
-            D.sol[T.i] = make_float4(0.f, 0.f, 0.f, 0.f);
-            D.p0[T.i] = make_float4(0.f, 0.f, 0.f, 0.f);
-            part = (double)dot3(f3(rhs), f3(rhs));
-        }
-    }
+    if (active) part = rhs_tile<G>(D, D.scenes[T.sc], T);
     block_finish<BLOCK>(D, T.sc, active, part, K_RHS);
 }
 
-// CG launch A: p = r + beta p_prev (ip.py:323-327, formed on the fly for the
-// neighbours too), y = dfdt k (J p) (compute_Jx_pcg, ip.py:19-60), and the
-// FP64 partials of p^T A p = sum m |p|^2 + omega sum y (J p) (the value
-// dot(p, A p) of ip.py:307, using that the gather-form transpose is the exact
-// transpose of J for symmetric lists).
 template <int G, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_cg_a(const Dev D) {
-    const TileCtx T = tile_ctx<G>(D);
+    const TileCtx T = tile_ctx<G>(D, blockIdx.x);
     __shared__ int sh_active, sh_it;
     __shared__ float sh_beta;
     if (threadIdx.x == 0) {
@@ -709,50 +956,13 @@ __global__ void __launch_bounds__(BLOCK) k_cg_a(const Dev D) {
     __syncthreads();
     const bool active = sh_active != 0;
     double part = 0.0;
-    if (active) {
-        const SceneParams& P = D.scenes[T.sc];
-        const float beta = sh_beta;
-        const float4* pp = (sh_it & 1) ? D.p1 : D.p0;
-        float4* pn = (sh_it & 1) ? D.p0 : D.p1;
-        const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
-        const int2* nb = D.nbr + (size_t)T.row * D.stride;
-        float3 xi = make_float3(0.f, 0.f, 0.f), pi = xi;
-        float mi = 0.0f;
-        if (T.valid) {
-            const float4 a = D.xm[T.i];
-            xi = f3(a);
-            mi = a.w;
-            const float4 ri = D.r[T.i], qi = pp[T.i];
-            pi = make_float3(ri.x + beta * qi.x, ri.y + beta * qi.y, ri.z + beta * qi.z);
-        }
-        float acc = 0.0f;
-        for (int k = T.lane; k < cnt; k += G) {
-            const int2 e = nb[k];
-            const int j = e.x;
-            if (j < P.s_begin || j >= P.s_end) { flag_bad(D, j, 3); continue; }
-            const float4 xj = D.xm[j];
-            const float3 gw = scale3(__int_as_float(e.y), sub3(xi, f3(xj)));
-            const float4 rj = D.r[j], qj = pp[j];
-            const float3 pj = make_float3(rj.x + beta * qj.x, rj.y + beta * qj.y, rj.z + beta * qj.z);
-            acc += dot3(sub3(pi, pj), scale3(xj.w, gw));
-        }
-        acc = group_sum<G>(acc);
-        if (T.valid && T.lane == 0) {
-            const float yi = acc * D.s[T.i];
-            D.y[T.i] = yi;
-            pn[T.i] = make_float4(pi.x, pi.y, pi.z, 0.0f);
-            part = (double)(mi * dot3(pi, pi)) + (double)P.omega * (double)yi * (double)acc;
-        }
-    }
+    if (active) part = cga_tile<G>(D, D.scenes[T.sc], T, sh_beta, sh_it);
     block_finish<BLOCK>(D, T.sc, active, part, K_CG_A);
 }
 
-// CG launch B: Ap = m p + omega J^T y in gather form (compute_Ax_part1/2,
-// ip.py:63-121, as pressure_base.py:130-166 writes J^T), x += alpha p,
-// r -= alpha Ap (pcg_update_x_r_scalar, math_utils.py:181-195), rr = r.r.
 template <int G, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_cg_b(const Dev D) {
-    const TileCtx T = tile_ctx<G>(D);
+    const TileCtx T = tile_ctx<G>(D, blockIdx.x);
     __shared__ int sh_active, sh_it;
     __shared__ float sh_alpha;
     if (threadIdx.x == 0) {
@@ -764,78 +974,218 @@ __global__ void __launch_bounds__(BLOCK) k_cg_b(const Dev D) {
     __syncthreads();
     const bool active = sh_active != 0;
     double part = 0.0;
-    if (active) {
-        const SceneParams& P = D.scenes[T.sc];
-        const float4* pc = (sh_it & 1) ? D.p0 : D.p1;
-        const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
-        const int2* nb = D.nbr + (size_t)T.row * D.stride;
-        float3 xi = make_float3(0.f, 0.f, 0.f);
-        float mi = 0.0f, yi = 0.0f;
-        if (T.valid) {
-            const float4 a = D.xm[T.i];
-            xi = f3(a);
-            mi = a.w;
-            yi = D.y[T.i];
-        }
-        float ax = 0.0f, ay = 0.0f, az = 0.0f;
-        for (int k = T.lane; k < cnt; k += G) {
-            const int2 e = nb[k];
-            const int j = e.x;
-            if (j < P.s_begin || j >= P.s_end) { flag_bad(D, j, 4); continue; }
-            const float4 xj = D.xm[j];
-            const float3 gw = scale3(__int_as_float(e.y), sub3(xi, f3(xj)));
-            const float wgt = xj.w * yi + mi * D.y[j];
-            ax += wgt * gw.x;
-            ay += wgt * gw.y;
-            az += wgt * gw.z;
-        }
-        ax = group_sum<G>(ax);
-        ay = group_sum<G>(ay);
-        az = group_sum<G>(az);
-        if (T.valid && T.lane == 0) {
-            const float om = P.omega, alpha = sh_alpha;
-            const float4 p4 = pc[T.i];
-            const float3 ap = make_float3(mi * p4.x + om * ax, mi * p4.y + om * ay, mi * p4.z + om * az);
-            float4 xs = D.sol[T.i], rs = D.r[T.i];
-            xs.x = xs.x + alpha * p4.x;
-            xs.y = xs.y + alpha * p4.y;
-            xs.z = xs.z + alpha * p4.z;
-            rs.x = rs.x - alpha * ap.x;
-            rs.y = rs.y - alpha * ap.y;
-            rs.z = rs.z - alpha * ap.z;
-            D.sol[T.i] = xs;
-            D.r[T.i] = rs;
-            part = (double)dot3(f3(rs), f3(rs));
-        }
-    }
+    if (active) part = cgb_tile<G>(D, D.scenes[T.sc], T, sh_alpha, sh_it);
     block_finish<BLOCK>(D, T.sc, active, part, K_CG_B);
 }
 
-// compute_divergence (pressure_base.py:449-457): max(J v, 0) with v = d/dt.
 template <int G, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_divergence(const Dev D) {
-    const TileCtx T = tile_ctx<G>(D);
-    const SceneParams& P = D.scenes[T.sc];
-    const SceneCtl& C = D.ctl[T.sc];
-    const float4* dc = (C.outer_it & 1) ? D.d1 : D.d0;
-    const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
-    const int2* nb = D.nbr + (size_t)T.row * D.stride;
-    const float s = P.inv_dt;
-    float3 xi = make_float3(0.f, 0.f, 0.f), vi = xi;
-    if (T.valid) {
-        xi = f3(D.xm[T.i]);
-        vi = scale3(s, f3(dc[T.i]));
+    const TileCtx T = tile_ctx<G>(D, blockIdx.x);
+    div_tile<G>(D, D.scenes[T.sc], T, D.ctl[T.sc].outer_it);
+}
+
+// ---- the whole IP.solve in one persistent cooperative launch
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Grid-wide barrier of a co-resident (cooperative) grid, fused with the
+// phase's reduction: the last CTA to arrive sums every active scene's tile
+// partials (scene_sum_warp, the same association as the per-phase path),
+// applies the scene decisions to the control blocks in global memory and only
+// then releases the others.  Control blocks are read past L1 (other CTAs
+// write them).  The wait is bounded: after kBarrierLimitNs a CTA sets the
+// timeout flag and reports failure, so a fault can never keep the kernel
+// spinning.
+constexpr unsigned long long kBarrierLimitNs = 2000000000ull;
+
+__device__ __forceinline__ bool phase_active(const SceneCtl& C, int kind) {
+    return kind == K_PACK ? C.outer_active != 0 : kind == K_RHS ? C.solve_pending != 0 : C.cg_active != 0;
+}
+
+__device__ __forceinline__ SceneCtl ctl_load(const SceneCtl* p) {
+    SceneCtl c;
+    const double* ds = reinterpret_cast<const double*>(p);
+    double* dd = reinterpret_cast<double*>(&c);
+#pragma unroll
+    for (int k = 0; k < (int)(sizeof(SceneCtl) / sizeof(double)); ++k) dd[k] = __ldcg(ds + k);
+    return c;
+}
+
+__device__ bool grid_reduce_barrier(const Dev& D, int kind, int* sh_flag, double* sum_sh) {
+    unsigned g = 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        g = *((volatile unsigned*)D.bar_gen);
+        __threadfence();
+        sh_flag[0] = atomicAdd(D.bar_count, 1u) == gridDim.x - 1;
+        sh_flag[1] = 1;
     }
-    float acc = 0.0f;
-    for (int k = T.lane; k < cnt; k += G) {
-        const int2 e = nb[k];
-        const float4 xj = D.xm[e.x];
-        const float3 gw = scale3(__int_as_float(e.y), sub3(xi, f3(xj)));
-        const float3 vj = scale3(s, f3(dc[e.x]));
-        acc += xj.w * dot3(sub3(vi, vj), gw);
+    __syncthreads();
+    if (sh_flag[0]) {
+        __threadfence();
+        if (kind >= 0) {
+            const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+            for (int s = warp; s < D.n_scenes; s += nwarps) {
+                if (!phase_active(ctl_load(D.ctl + s), kind)) continue;
+                const SceneParams& P = D.scenes[s];
+                const double v = scene_sum_warp(D.partial, P.tile_begin, P.tile_end);
+                if ((threadIdx.x & 31) == 0) sum_sh[s] = v;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0)
+                for (int s = 0; s < D.n_scenes; ++s) {
+                    SceneCtl c = ctl_load(D.ctl + s);
+                    if (!phase_active(c, kind)) continue;
+                    scene_decide(D, D.scenes[s], c, kind, sum_sh[s], true);
+                    D.ctl[s] = c;
+                }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            *D.bar_count = 0;
+            __threadfence();
+            atomicAdd(D.bar_gen, 1u);
+        }
+    } else if (threadIdx.x == 0) {
+        // the generation advances only after every CTA arrived, so g (read
+        // before arriving) is the current one
+        volatile unsigned* gen = D.bar_gen;
+        const unsigned long long t0 = globaltimer_ns();
+        while (*gen == g) {
+            __nanosleep(32);
+            if (globaltimer_ns() - t0 > kBarrierLimitNs) {
+                sh_flag[1] = 0;
+                D.flags->timeout = 1;
+                break;
+            }
+        }
+        __threadfence();
     }
-    acc = group_sum<G>(acc);
-    if (T.valid && T.lane == 0 && D.div_out) D.div_out[D.pid[T.i]] = acc > 0.0f ? acc : 0.0f;
+    __syncthreads();
+    return sh_flag[1] != 0;
+}
+
+template <int G, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_ip_persistent(const Dev D) {
+    extern __shared__ double dyn_sh[];
+    double* sum_sh = dyn_sh;                                             // [n_scenes]
+    SceneCtl* sc_sh = reinterpret_cast<SceneCtl*>(dyn_sh + D.n_scenes);  // [n_scenes]
+    __shared__ double red_sh[32];
+    __shared__ int flag_sh[2], any_sh;
+    const int t0 = (int)(((long long)blockIdx.x * D.n_tiles) / gridDim.x);
+    const int t1 = (int)(((long long)(blockIdx.x + 1) * D.n_tiles) / gridDim.x);
+    // CTA 0 starts every scene's control block (reset_stats); the first
+    // barrier publishes it
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        for (int s = 0; s < D.n_scenes; ++s) ctl_begin(D.scenes[s], D.ctl[s]);
+    // d = dt v (ip.py:343) for the owned particles
+    for (int t = t0; t < t1; ++t) {
+        const int4 tile = __ldg(D.tiles + t);
+        const SceneParams& P = D.scenes[tile.x];
+        for (int i = tile.y + threadIdx.x; i < tile.z; i += BLOCK) {
+            const int p = D.pid[i];
+            const float dt = P.dt;
+            D.d0[i] = make_float4(dt * D.v[3 * p], dt * D.v[3 * p + 1], dt * D.v[3 * p + 2], 0.0f);
+        }
+    }
+    if (!grid_reduce_barrier(D, -1, flag_sh, sum_sh)) return;
+    // local copies of the control blocks, refreshed after every phase
+    auto refresh = [&]() {
+        for (int s = threadIdx.x; s < D.n_scenes; s += BLOCK) sc_sh[s] = ctl_load(D.ctl + s);
+        __syncthreads();
+    };
+    refresh();
+    long long phases = 0;
+    const long long limit = D.phase_limit;
+    auto run_phase = [&](int kind) -> bool {
+        for (int t = t0; t < t1; ++t) {
+            const TileCtx T = tile_ctx<G>(D, t);
+            const SceneCtl& C = sc_sh[T.sc];
+            if (!phase_active(C, kind)) continue;
+            const SceneParams& P = D.scenes[T.sc];
+            double part;
+            if (kind == K_PACK) part = pack_tile<G>(D, P, T, C.outer_it);
+            else if (kind == K_RHS) part = rhs_tile<G>(D, P, T);
+            else if (kind == K_CG_A) part = cga_tile<G>(D, P, T, (float)C.beta, C.cg_it);
+            else part = cgb_tile<G>(D, P, T, (float)C.alpha, C.cg_it);
+            const double tot = block_sum_d<BLOCK>(part, red_sh);
+            if (threadIdx.x == 0) D.partial[t] = tot;
+        }
+        if (!grid_reduce_barrier(D, kind, flag_sh, sum_sh)) return false;
+        if (++phases > limit) {
+            // guard: every CTA reaches the same count; CTA 0 stops the scenes,
+            // a barrier publishes it
+            if (blockIdx.x == 0 && threadIdx.x == 0) {
+                for (int s = 0; s < D.n_scenes; ++s) {
+                    SceneCtl c = ctl_load(D.ctl + s);
+                    if (c.outer_active || c.solve_pending || c.cg_active) {
+                        c.status = IVP_TIMEOUT_;
+                        c.outer_active = c.solve_pending = c.cg_active = 0;
+                        D.ctl[s] = c;
+                    }
+                }
+                D.flags->timeout = 1;
+            }
+            if (!grid_reduce_barrier(D, -1, flag_sh, sum_sh)) return false;
+        }
+        refresh();
+        return true;
+    };
+    auto any = [&](int kind) -> bool {
+        if (threadIdx.x == 0) {
+            int a = 0;
+            for (int s = 0; s < D.n_scenes; ++s) a |= phase_active(sc_sh[s], kind) ? 1 : 0;
+            any_sh = a;
+        }
+        __syncthreads();
+        const bool r = any_sh != 0;
+        __syncthreads();
+        return r;
+    };
+    while (any(K_PACK)) {
+        if (!run_phase(K_PACK)) return;
+        if (!any(K_RHS)) break;
+        if (!run_phase(K_RHS)) return;
+        while (any(K_CG_A)) {
+            if (!run_phase(K_CG_A)) return;
+            if (!any(K_CG_B)) break;
+            if (!run_phase(K_CG_B)) return;
+        }
+    }
+    // epilogue (ip.py:394-404): v = d/dt for scenes that did not raise,
+    // divergence, statistics
+    for (int t = t0; t < t1; ++t) {
+        const TileCtx T = tile_ctx<G>(D, t);
+        const SceneCtl& C = sc_sh[T.sc];
+        const SceneParams& P = D.scenes[T.sc];
+        if (C.status == IVP_OK_ && T.lane == 0 && T.valid) {
+            const float4 d = (C.outer_it & 1) ? D.d1[T.i] : D.d0[T.i];
+            const int p = D.pid[T.i];
+            const float s = P.inv_dt;
+            D.v[3 * p] = s * d.x;
+            D.v[3 * p + 1] = s * d.y;
+            D.v[3 * p + 2] = s * d.z;
+        }
+        if (D.div_out) div_tile<G>(D, P, T, C.outer_it);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        for (int s = 0; s < D.n_scenes; ++s) {
+            SceneCtl c = ctl_load(D.ctl + s);
+            c.acc_solves += 1;
+            c.acc_outer += c.outer_it;
+            c.acc_cg += c.total_cg;
+            if (c.final_err > c.acc_max_final_err) c.acc_max_final_err = c.final_err;
+            if (c.status != IVP_OK_) {
+                c.acc_failed += 1;
+                c.acc_last_failure = c.status;
+            }
+            D.ctl[s] = c;
+        }
+    }
 }
 
 __global__ void k_reset_counters(const Dev D) {
@@ -855,7 +1205,7 @@ __global__ void k_export(const Dev D, int scene, int* count, int* ids, int cache
     const int p = D.pid[i] - P.p_begin;
     const int cnt = D.nbr_cnt[row];
     count[p] = cnt;
-    for (int k = 0; k < cnt && k < cache; ++k) ids[(size_t)p * cache + k] = D.pid[D.nbr[(size_t)row * D.stride + k].x] - P.p_begin;
+    for (int k = 0; k < cnt && k < cache; ++k) ids[(size_t)p * cache + k] = D.pid[__float_as_int(D.nbr[(size_t)row * D.stride + k].w)] - P.p_begin;
 }
 
 }  // namespace ivp

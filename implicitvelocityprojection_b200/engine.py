@@ -30,6 +30,7 @@ class EngineOptions:
     list_stride: int = 64
     max_hist: int = 128
     use_graphs: bool = True
+    persistent: bool = True
 
     def to_c(self) -> _lib.Options:
         o = _lib.Options()
@@ -38,6 +39,7 @@ class EngineOptions:
         o.list_stride = self.list_stride
         o.max_hist = self.max_hist
         o.use_graphs = int(self.use_graphs)
+        o.persistent = int(self.persistent)
         return o
 
 

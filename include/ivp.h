@@ -67,8 +67,10 @@ typedef struct {
     int32_t particles_per_block;  /* particles per CTA in the neighbour-sum kernels */
     int32_t list_stride;          /* neighbour-list row stride (>= every scene's cache_size) */
     int32_t max_hist;             /* per-scene stats history length (outer iterations) */
-    int32_t use_graphs;           /* 1: device-side loops in CUDA graphs with conditional nodes */
-    int32_t reserved[3];
+    int32_t use_graphs;           /* 1: whole steps as CUDA graphs (device-side control, no host sync) */
+    int32_t persistent;           /* 1: the IP solve as one persistent cooperative kernel with grid barriers;
+                                     0: one launch per phase, loops as conditional graph nodes */
+    int32_t reserved[2];
 } ivp_options;
 
 /* Device arrays in the reference's layout and particle order
@@ -109,7 +111,7 @@ typedef struct {
 enum {
     IVP_K_GRAVITY = 0, IVP_K_SOLVE_BEGIN, IVP_K_PACK, IVP_K_RHS, IVP_K_CG_A, IVP_K_CG_B, IVP_K_SOLVE_END,
     IVP_K_DIVERGENCE, IVP_K_ADVECT, IVP_K_KEYS, IVP_K_SCAN_LOCAL, IVP_K_SCAN_ADD, IVP_K_PLACE, IVP_K_ORDER,
-    IVP_K_NBR_BUILD, IVP_K_STATIC_OUT, IVP_K_VISC, IVP_K_COUNT = 24
+    IVP_K_NBR_BUILD, IVP_K_STATIC_OUT, IVP_K_VISC, IVP_K_PERSISTENT, IVP_K_COUNT = 24
 };
 
 typedef struct ivp_engine ivp_engine;

@@ -209,10 +209,13 @@ def test_multi_scene_bitwise_equal_to_alone():
         assert a.stats_density_errors == b.stats_density_errors
 
 
-def test_deterministic_and_graph_equals_host_loop(small):
+def test_deterministic_across_execution_paths(small):
+    """Persistent cooperative solve, one launch per phase in conditional
+    graphs, and host-driven launches share the tile code and the reduction
+    order: results are bit-identical, and repeatable."""
     outs = []
-    for use_graphs in (True, True, False):
-        eng = _engine([small], use_graphs=use_graphs)
+    for use_graphs, persistent in ((True, True), (True, True), (True, False), (False, False), (False, True)):
+        eng = _engine([small], use_graphs=use_graphs, persistent=persistent)
         eng.build()
         eng.step(4)
         outs.append((eng.get("x"), eng.get("v"), eng.stats(0).stats_density_errors))
@@ -220,6 +223,19 @@ def test_deterministic_and_graph_equals_host_loop(small):
         assert np.array_equal(o[0], outs[0][0])
         assert np.array_equal(o[1], outs[0][1])
         assert o[2] == outs[0][2]
+
+
+def test_multi_scene_persistent_equals_per_phase():
+    scs = [S.random_column(2500, 1.5, seed=21), S.small_dam_break(4000, seed=22), S.random_column(900, 3.0, seed=23)]
+    a = _engine(scs, persistent=True)
+    b = _engine(scs, persistent=False)
+    for e in (a, b):
+        e.build()
+        e.step(3)
+    for i in range(len(scs)):
+        assert np.array_equal(a.get("x", i), b.get("x", i))
+        assert np.array_equal(a.get("v", i), b.get("v", i))
+        assert a.stats(i).stats_pcg_iters == b.stats(i).stats_pcg_iters
 
 
 @pytest.mark.parametrize("lanes", [1, 2, 8])
