@@ -3,7 +3,10 @@
 density error, on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload tall_column|small_column|dam_break]
+                    [--workload tall_column|tall_column_ip|small_column|dam_break]
+
+Default workload: 102,400 fluid particles (40 x 64 x 40) in a 0.8 x 3.0 x 0.8 m
+box, Weiler 2018 implicit viscosity nu = 1e-3 m^2/s, dt = 1 ms.
 
 One step = one full Framework.forward() of every replica's scene (gravity,
 implicit viscosity where the workload enables it, the IP solve with its CG,
@@ -41,9 +44,9 @@ UNIT = "particle-steps/s"
 def make_scene(name: str):
     from implicitvelocityprojection_b200 import scenes as S
     if name == "tall_column":
-        return S.tall_column(viscosity=False)
-    if name == "tall_column_visc":
         return S.tall_column(viscosity=True)
+    if name == "tall_column_ip":
+        return S.tall_column(viscosity=False)
     if name == "small_column":
         return S.small_column()
     if name == "dam_break":
@@ -53,7 +56,7 @@ def make_scene(name: str):
 
 
 def workload_config(sc, name: str) -> dict:
-    return {"workload": sc.name if name != "tall_column" else "tall_column_102k_ip",
+    return {"workload": sc.name + ("_ip_only" if name == "tall_column_ip" else ""),
             "fluid_particles": sc.n_dynamic, "boundary_particles": sc.n - sc.n_dynamic,
             "spacing_m": sc.particle_diameter, "dt_s": sc.dt, "densityErrorTol": sc.density_error_tol,
             "viscosity": ("weiler18 nu=%g" % sc.viscosity_coeff) if sc.viscosity_method == 1 else "off",
@@ -64,7 +67,7 @@ def workload_config(sc, name: str) -> dict:
 # ----------------------------------------------------------------- clocks
 
 class ClockSampler:
-    """nvidia-smi samples during the timed region (200 ms period)."""
+    """nvidia-smi samples during the timed region (50 ms period)."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -79,7 +82,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except Exception:
@@ -117,11 +120,21 @@ class ClockSampler:
 
 # ----------------------------------------------------------------- roofline
 
-def algorithmic_bytes(kernel: str, n_dyn: int, n_all: int, pairs: int) -> float:
+def algorithmic_bytes(kernel: str, n_dyn: int, n_all: int, pairs: int, it=None) -> float:
     """Algorithmic bytes of one launch, per the byte model of the path: 16 B
     per stored neighbour pair (4 B id + 12 B gradient, the reference's cache
-    entry) and each per-particle stream counted once per pass."""
+    entry) and each per-particle stream counted once per pass.  `it` gives the
+    per-step phase counts for the persistent solve (outer updates, CG and
+    viscosity-CG iterations)."""
     P = float(pairs)
+    if kernel == "ip_solve":
+        L, I, V = it["outer"], it["cg"], it["visc"]
+        b = (L + 1) * algorithmic_bytes("pack", n_dyn, n_all, pairs) + L * algorithmic_bytes("rhs", n_dyn, n_all, pairs)
+        b += I * (algorithmic_bytes("cg_a", n_dyn, n_all, pairs) + algorithmic_bytes("cg_b", n_dyn, n_all, pairs))
+        b += algorithmic_bytes("divergence", n_dyn, n_all, pairs) + 48 * n_dyn  # d = dt v, v = d / dt
+        if it.get("visc_on"):
+            b += 16 * P + 120 * n_dyn + V * ((16 * P + 64 * n_dyn) + 120 * n_dyn)
+        return b
     if kernel == "cg_a":
         return 16 * P + 48 * n_dyn
     if kernel == "cg_b":
@@ -259,7 +272,9 @@ def run_ours(args, rank, world, local_rank):
     dom = max(prof.items(), key=lambda kv: kv[1][0])
     dom_name, (dom_ms, dom_n) = dom
     avg_s = dom_ms / dom_n / 1000.0
-    alg = algorithmic_bytes(dom_name, sc.n_dynamic, sc.n, pairs)
+    it = {"outer": raw.sum_outer_iters / args.steps, "cg": raw.sum_pcg_iters / args.steps,
+          "visc": raw.sum_visc_iters / args.steps, "visc_on": sc.viscosity_method == 1}
+    alg = algorithmic_bytes(dom_name, sc.n_dynamic, sc.n, pairs, it)
     peak, peak_kind = load_peaks()
     achieved = alg / avg_s / 1e9 if avg_s > 0 else 0.0
     roof = {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -284,6 +299,7 @@ def run_ours(args, rank, world, local_rank):
                 "valid": bool(valid), "max_final_density_error": raw.max_final_density_error,
                 "outer_iters_per_step": raw.sum_outer_iters / args.steps,
                 "cg_iters_per_step": raw.sum_pcg_iters / args.steps,
+                "visc_cg_iters_per_step": raw.sum_visc_iters / args.steps,
                 "mean_neighbours": pairs / max(sc.n_dynamic, 1),
                 "wall_s": wall, "gpu_launches": int(n_launch), "clocks": clk, "roofline": roof,
                 "cpu_baseline": cpu, "e2e": e2e}
@@ -336,7 +352,7 @@ def run_e2e(args, sc, dev):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="tall_column")

@@ -86,6 +86,7 @@ class SolveStats(ctypes.Structure):
         ("sum_pcg_iters", ctypes.c_int64),
         ("max_final_density_error", ctypes.c_double),
         ("neighbour_pairs", ctypes.c_int64),
+        ("sum_visc_iters", ctypes.c_int64),
     ]
 
 
@@ -112,6 +113,7 @@ SIGNATURES = {
     "ivp_compute_density": (_I, [_P, _P]),
     "ivp_compute_aii": (_I, [_P, _P]),
     "ivp_ip_solve": (_I, [_P, _P]),
+    "ivp_viscosity_solve": (_I, [_P, _P]),
     "ivp_apply_gravity": (_I, [_P, _P]),
     "ivp_advect": (_I, [_P, _P]),
     "ivp_step": (_I, [_P, _I, _P]),

@@ -74,6 +74,15 @@ struct SceneCtl {
     int status;
     int n_err;
     int total_cg;
+    // Weiler 2018 implicit viscosity CG (weiler18.py:298-365)
+    double v_rz;         // r.z of the current iterate
+    double v_alpha;
+    double v_beta;
+    double v_pap;
+    int v_active;        // CG running
+    int v_it;            // CG iterations of this solve
+    int v_total;         // CG iterations of the last step (stats)
+    int v_on;            // viscosity enabled for this scene (set at the start of a step)
     // sticky counters since the last reset (ivp_reset_counters)
     double acc_max_final_err;
     int acc_solves;
@@ -81,13 +90,14 @@ struct SceneCtl {
     int acc_cg;
     int acc_failed;
     int acc_last_failure;
-    int acc_pad;
+    int acc_visc;        // viscosity CG iterations
 };
 
 static_assert(sizeof(SceneCtl) % sizeof(double) == 0, "SceneCtl is read as doubles");
 
 struct Flags {
     int any_outer, any_solve, any_cg, bad;
+    int any_visc, pad_v;
     int bad_index, bad_where;
     // loop guard: decision launches of the current solve and their budget;
     // past the budget every active scene stops with IVP_ERR_TIMEOUT, so a
@@ -143,6 +153,11 @@ struct Dev {
     float* s;
     float* fk;
     float* inv_m;            // 1/m of dynamic slots (0 for static)
+    float* rflu;             // 1/rho of fluid slots (0 for non-fluid): viscosity neighbour weight
+    float4* vs;              // viscosity: slot-ordered velocity
+    float4* vz;              // viscosity: preconditioned residual
+    float4* vap;             // viscosity: A p
+    float4* pinv;            // viscosity: 3x3 block-Jacobi inverse, 3 rows per slot
     float* q;                // fk / m
     float* z;                // y / m
     // neighbour rows
@@ -158,10 +173,12 @@ struct Dev {
     int* pcg_hist;
     int hist_len;
     // graph conditionals (0 = not inside a conditional graph)
-    unsigned long long h_outer, h_solve, h_cg;
+    unsigned long long h_outer, h_solve, h_cg, h_visc;
     // advect leaves scenes whose last solve raised where they are (the
     // reference raises before advecting, framework.py:483-513)
     int advect_skip_failed;
+    // the persistent solve runs the viscosity phases (set on step launches)
+    int visc_enabled;
     // persistent solve: grid-barrier words and the phase budget
     unsigned* bar_count;
     unsigned* bar_gen;

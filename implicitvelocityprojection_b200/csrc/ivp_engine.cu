@@ -62,6 +62,7 @@ struct ivp_engine {
     int n_scenes = 0;
     bool bound = false;
     bool want_divergence = false;
+    bool any_visc = false;
     // persistent solve
     bool persistent = false;
     int coop_grid = 0;
@@ -184,13 +185,14 @@ struct Kern {
 };
 
 struct KernelSet {
-    DevKernel pack, rhs, cg_a, cg_b, dens, aii, div, persist;
+    DevKernel pack, rhs, cg_a, cg_b, dens, aii, div, persist, v_setup, v_a, v_b, v_end;
 };
 
 template <int G, int B>
 KernelSet make_set() {
     return {Kern<G, B>::pack(), Kern<G, B>::rhs(), Kern<G, B>::cg_a(), Kern<G, B>::cg_b(),
-            Kern<G, B>::dens(), Kern<G, B>::aii(), Kern<G, B>::div(), k_ip_persistent<G, B>};
+            Kern<G, B>::dens(), Kern<G, B>::aii(), Kern<G, B>::div(), k_ip_persistent<G, B>,
+            k_visc_setup<G, B>, k_visc_a<G, B>, k_visc_b<G, B>, k_visc_end<G, B>};
 }
 
 // Instantiated launch shapes: G lanes per particle x {128, 256} threads.
@@ -321,13 +323,48 @@ int emit_solve_loop(ivp_engine* e, Launcher& L) {
     return IVP_OK;
 }
 
-int emit_solve(ivp_engine* e, Launcher& L) {
+// Weiler 2018 viscosity, one launch per phase (the persistent solve runs the
+// same phases itself).
+int emit_visc(ivp_engine* e, Launcher& L) {
+    if (e->n_tiles == 0 || !e->any_visc) return IVP_OK;
+    KernelSet K;
+    if (!kernel_set(e->G, e->BLOCK, &K)) return IVP_ERR_BAD_ARG;
+    const int nt = e->n_tiles, B = e->BLOCK;
+    CKS(L.dev(IVP_K_VISC, k_visc_begin, nt, e->T, e->D));
+    if (!L.graph) {
+        CKS(L.dev(IVP_K_VISC, K.v_setup, nt, B, e->D));
+        CK(cudaMemcpyAsync(e->h_flags, e->D.flags, sizeof(Flags), cudaMemcpyDeviceToHost, L.stream));
+        CK(cudaStreamSynchronize(L.stream));
+        for (int guard = 0; e->h_flags->any_visc && guard < 1000000; ++guard) {
+            CKS(L.dev(IVP_K_VISC, K.v_a, nt, B, e->D));
+            CKS(L.dev(IVP_K_VISC, K.v_b, nt, B, e->D));
+            CK(cudaMemcpyAsync(e->h_flags, e->D.flags, sizeof(Flags), cudaMemcpyDeviceToHost, L.stream));
+            CK(cudaStreamSynchronize(L.stream));
+        }
+    } else {
+        cudaGraphConditionalHandle h;
+        CK(cudaGraphConditionalHandleCreate(&h, L.graph, 0, 0));
+        Dev d = e->D;
+        d.h_visc = (unsigned long long)h;
+        CKS(L.dev(IVP_K_VISC, K.v_setup, nt, B, d));
+        cudaGraph_t body;
+        CKS(add_conditional(L.graph, L, h, cudaGraphCondTypeWhile, &body));
+        Launcher Lb;
+        Lb.graph = body;
+        CKS(Lb.dev(IVP_K_VISC, K.v_a, nt, B, d));
+        CKS(Lb.dev(IVP_K_VISC, K.v_b, nt, B, d));
+    }
+    return L.dev(IVP_K_VISC, K.v_end, nt, B, e->D);
+}
+
+int emit_solve(ivp_engine* e, Launcher& L, bool with_visc = false) {
     if (e->n_tiles == 0) return IVP_OK;
     if (e->persistent) {
         KernelSet K;
         kernel_set(e->G, e->BLOCK, &K);
         CKS(L.memset0(e->D.bar_count, sizeof(unsigned)));
         Dev copy = e->D;
+        copy.visc_enabled = with_visc ? 1 : 0;
         void* args[] = {&copy};
         return L.kernel(IVP_K_PERSISTENT, (const void*)K.persist, dim3(e->coop_grid), dim3(e->BLOCK), args,
                         e->coop_smem, true);
@@ -349,7 +386,8 @@ int emit_advect(ivp_engine* e, Launcher& L) {
 
 int emit_step(ivp_engine* e, Launcher& L) {
     CKS(L.dev(IVP_K_GRAVITY, k_gravity, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, e->D));
-    CKS(emit_solve(e, L));
+    if (!e->persistent) CKS(emit_visc(e, L));
+    CKS(emit_solve(e, L, true));
     {
         Dev d = e->D;
         d.advect_skip_failed = 1;
@@ -426,7 +464,7 @@ struct Plan {
     std::vector<SceneParams> hp;
     std::vector<int4> tiles;
     int n_total = 0, n_dyn = 0, n_keys = 0, scan_blocks = 0;
-    size_t off[40];
+    size_t off[48];
     Layout lay;
 };
 
@@ -532,7 +570,7 @@ void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
     P.off[i++] = L.add(sizeof(float) * N);                  // 26 fk
     P.off[i++] = L.add(sizeof(float4) * (size_t)P.n_dyn * (size_t)o->list_stride);  // 27 nbr
     P.off[i++] = L.add(sizeof(int) * std::max<size_t>((size_t)P.n_dyn, 1));       // 28 nbr_cnt
-    P.off[i++] = L.add(sizeof(double) * NT);                // 29 partial
+    P.off[i++] = L.add(2 * sizeof(double) * NT);            // 29 partial (two per tile)
     P.off[i++] = L.add(sizeof(int) * S);                    // 30 scene_counter
     P.off[i++] = L.add(sizeof(int));                        // 31 launch_counter
     P.off[i++] = L.add(sizeof(Flags));                      // 32 flags
@@ -543,6 +581,11 @@ void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
     P.off[i++] = L.add(sizeof(float) * N);                           // 37 inv_m
     P.off[i++] = L.add(sizeof(float) * N);                           // 38 q
     P.off[i++] = L.add(sizeof(float) * N);                           // 39 z
+    P.off[i++] = L.add(sizeof(float) * N);                           // 40 rflu
+    P.off[i++] = L.add(sizeof(float4) * N);                          // 41 vs
+    P.off[i++] = L.add(sizeof(float4) * N);                          // 42 vz
+    P.off[i++] = L.add(sizeof(float4) * N);                          // 43 vap
+    P.off[i++] = L.add(3 * sizeof(float4) * N);                      // 44 pinv
 }
 
 cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
@@ -595,6 +638,9 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
     e->n_tiles = (int)P.tiles.size();
     e->scan_blocks = P.scan_blocks;
     e->n_scenes = n_scenes;
+    for (int sc = 0; sc < n_scenes; ++sc)
+        if (scenes[sc].viscosity_method == 1 && scenes[sc].viscosity_coeff > 0.0f && scenes[sc].n_dynamic > 0)
+            e->any_visc = true;
     char* w = static_cast<char*>(workspace);
     Dev& D = e->D;
     int i = 0;
@@ -639,10 +685,16 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
     D.inv_m = reinterpret_cast<float*>(w + P.off[i++]);
     D.q = reinterpret_cast<float*>(w + P.off[i++]);
     D.z = reinterpret_cast<float*>(w + P.off[i++]);
+    D.rflu = reinterpret_cast<float*>(w + P.off[i++]);
+    D.vs = reinterpret_cast<float4*>(w + P.off[i++]);
+    D.vz = reinterpret_cast<float4*>(w + P.off[i++]);
+    D.vap = reinterpret_cast<float4*>(w + P.off[i++]);
+    D.pinv = reinterpret_cast<float4*>(w + P.off[i++]);
     {
         long long lim = 64;
         for (int sc = 0; sc < n_scenes; ++sc)
-            lim += (long long)(scenes[sc].max_outer_iters + 1) * (long long)(2 * scenes[sc].max_iteration_pcg + 3);
+            lim += (long long)(scenes[sc].max_outer_iters + 1) * (long long)(2 * scenes[sc].max_iteration_pcg + 3) +
+                   2 * 1000 + 4;
         D.phase_limit = lim;
     }
     D.n_scenes = n_scenes;
@@ -683,7 +735,7 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
         int dev = 0, coop = 0, nsm = 0, per_sm = 0;
         KernelSet K;
         kernel_set(e->G, e->BLOCK, &K);
-        e->coop_smem = (size_t)n_scenes * (sizeof(double) + sizeof(SceneCtl));
+        e->coop_smem = (size_t)n_scenes * (2 * sizeof(double) + sizeof(SceneCtl));
         if (cudaGetDevice(&dev) == cudaSuccess &&
             cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) == cudaSuccess && coop &&
             cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&
@@ -783,9 +835,19 @@ int ivp_compute_aii(ivp_engine* e, void* stream) {
     return L.dev(IVP_K_STATIC_OUT, k_static_outputs, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, e->D);
 }
 
+int emit_ip_only(ivp_engine* e, Launcher& L) { return emit_solve(e, L, false); }
+
 int ivp_ip_solve(ivp_engine* e, void* stream) {
     if (!e) return IVP_ERR_BAD_ARG;
-    return run(e, emit_solve, &e->graph_solve, &e->exec_solve, as_stream(stream));
+    return run(e, emit_ip_only, &e->graph_solve, &e->exec_solve, as_stream(stream));
+}
+
+int ivp_viscosity_solve(ivp_engine* e, void* stream) {
+    if (!e) return IVP_ERR_BAD_ARG;
+    if (!e->bound) return IVP_ERR_NOT_BOUND;
+    Launcher L;
+    L.stream = as_stream(stream);
+    return emit_visc(e, L);
 }
 
 int ivp_apply_gravity(ivp_engine* e, void* stream) {
@@ -834,6 +896,11 @@ int ivp_read_stats(ivp_engine* e, int32_t scene, void* stream, ivp_solve_stats* 
     out->sum_pcg_iters = C.acc_cg;
     out->max_final_density_error = C.acc_max_final_err;
     out->neighbour_pairs = (int64_t)e->h_pairs[scene];
+    out->sum_visc_iters = C.acc_visc;
+    if (e->h_flags->timeout) {
+        g_err = "a solve exceeded its iteration budget or a grid barrier timed out";
+        out->status = IVP_ERR_TIMEOUT;
+    }
     if (e->h_flags->bad) {
         char buf[128];
         snprintf(buf, sizeof(buf), "device bounds check failed: index %d at site %d", e->h_flags->bad_index,

@@ -14,7 +14,7 @@
 
 namespace ivp {
 
-enum Kind { K_PACK = 0, K_RHS = 1, K_CG_A = 2, K_CG_B = 3, K_FINAL = 4 };
+enum Kind { K_PACK = 0, K_RHS = 1, K_CG_A = 2, K_CG_B = 3, K_V_SETUP = 4, K_V_A = 5, K_V_B = 6 };
 
 constexpr int IVP_OK_ = 0, IVP_NOT_SPD_ = 1, IVP_NOT_CONVERGED_ = 2, IVP_TIMEOUT_ = 6;
 
@@ -35,7 +35,42 @@ __device__ __forceinline__ void flag_bad(const Dev& D, int idx, int where) {
 // over the scene's dynamic particles.  `C` is the scene's control block (in
 // global memory for the launch-per-phase path, a per-CTA shared-memory copy
 // for the persistent path); history is written when `hist` is set.
-__device__ void scene_decide(const Dev& D, const SceneParams& P, SceneCtl& C, int kind, double s, bool hist) {
+// Weiler 2018 CG caps (weiler18.py:208-209)
+constexpr int kViscMaxIter = 1000;
+constexpr double kViscTol = 1e-5;
+
+__device__ __forceinline__ bool visc_on(const SceneParams& P) { return P.visc_method == 1 && P.visc_coeff > 0.0f; }
+
+__device__ void scene_decide(const Dev& D, const SceneParams& P, SceneCtl& C, int kind, double s, bool hist,
+                             double s2 = 0.0) {
+    if (kind == K_V_SETUP) {
+        // weiler18.py:327-330: iterate only if r.z > 1e-12
+        C.v_rz = s;
+        C.v_it = 0;
+        C.v_beta = 0.0;
+        C.v_total = 0;
+        C.v_active = s > 1e-12 ? 1 : 0;
+        return;
+    }
+    if (kind == K_V_A) {
+        // weiler18.py:332-338 (pAp <= 0 ends the solve without an error)
+        C.v_pap = s;
+        if (s <= 0.0) C.v_active = 0;
+        else C.v_alpha = C.v_rz / (s > 1e-12 ? s : 1e-12);
+        return;
+    }
+    if (kind == K_V_B) {
+        // weiler18.py:349-365: s = r.r (stop test), s2 = r.z (beta)
+        C.v_it += 1;
+        C.v_total = C.v_it;
+        if ((s < kViscTol && C.v_it >= 2) || C.v_it >= kViscMaxIter) {
+            C.v_active = 0;
+        } else {
+            C.v_beta = s2 / (C.v_rz > 1e-12 ? C.v_rz : 1e-12);
+            C.v_rz = s2;
+        }
+        return;
+    }
     if (kind == K_PACK) {
         // pressure_base.py:405-423 average, ip.py:364-370 stopping rule
         const double err = P.n_dyn > 0 ? s / (double)P.n_dyn : 0.0;
@@ -109,6 +144,17 @@ __device__ __forceinline__ double scene_sum_warp(const double* partial, int tb, 
     return warp_sum_d(s);
 }
 
+// Budget of decision launches for one solve sequence (per-phase path): past
+// it launch_finalize stops every scene with IVP_ERR_TIMEOUT.  The timeout
+// flag stays set until the host clears it (ivp_reset_counters).
+__device__ __forceinline__ void guard_begin(const Dev& D) {
+    long lim = 64;
+    for (int s = 0; s < D.n_scenes; ++s)
+        lim += (long)(D.scenes[s].max_outer + 1) * (long)(2 * D.scenes[s].max_pcg + 3) + 2 * kViscMaxIter + 4;
+    D.flags->limit = lim > 0x3fffffff ? 0x3fffffff : (int)lim;
+    D.flags->launches = 0;
+}
+
 // Control-block reset at the start of IP.solve (reset_stats,
 // pressure_base.py:497-502).
 __device__ __forceinline__ void ctl_begin(const SceneParams& P, SceneCtl& C) {
@@ -133,45 +179,52 @@ __device__ void launch_finalize(const Dev& D, int kind) {
         F->timeout = 1;
         for (int s = 0; s < D.n_scenes; ++s) {
             volatile SceneCtl* C = D.ctl + s;
-            if (C->outer_active || C->cg_active || C->solve_pending) {
+            if (C->outer_active || C->cg_active || C->solve_pending || C->v_active) {
                 C->status = IVP_TIMEOUT_;
                 C->outer_active = 0;
                 C->solve_pending = 0;
                 C->cg_active = 0;
+                C->v_active = 0;
             }
         }
     }
-    int any_outer = 0, any_solve = 0, any_cg = 0;
+    int any_outer = 0, any_solve = 0, any_cg = 0, any_visc = 0;
     // other CTAs wrote these during this launch: read past L1
     for (int s = 0; s < D.n_scenes; ++s) {
         const volatile SceneCtl* C = D.ctl + s;
         any_outer |= C->outer_active;
         any_solve |= C->solve_pending;
         any_cg |= C->cg_active;
+        any_visc |= C->v_active;
     }
     D.flags->any_outer = any_outer;
     D.flags->any_solve = any_solve;
     D.flags->any_cg = any_cg;
+    D.flags->any_visc = any_visc;
     if (kind == K_PACK) {
         set_cond(D.h_outer, any_outer);
         set_cond(D.h_solve, any_solve);
     } else if (kind == K_RHS || kind == K_CG_B) {
         set_cond(D.h_cg, any_cg);
+    } else if (kind == K_V_SETUP || kind == K_V_B) {
+        set_cond(D.h_visc, any_visc);
     }
 }
 
 // Reduce `part` over the CTA, hand it to the scene (last CTA of the scene
 // sums the scene's partials in tile order) and to the launch.
 template <int BLOCK>
-__device__ void block_finish(const Dev& D, int sc, bool active, double part, int kind) {
+__device__ void block_finish(const Dev& D, int sc, bool active, double part, int kind, double part2 = 0.0) {
     __shared__ double sh[32];
     __shared__ int sh_last;
     const double total = block_sum_d<BLOCK>(part, sh);
+    const double total2 = kind == K_V_B ? block_sum_d<BLOCK>(part2, sh) : 0.0;
     const SceneParams& P = D.scenes[sc];
     if (threadIdx.x == 0) {
         sh_last = 0;
         if (active) {
             D.partial[blockIdx.x] = total;
+            D.partial[D.n_tiles + blockIdx.x] = total2;
             __threadfence();
             const int ntiles = P.tile_end - P.tile_begin;
             if (atomicAdd(&D.scene_counter[sc], 1) == ntiles - 1) sh_last = 1;
@@ -181,9 +234,10 @@ __device__ void block_finish(const Dev& D, int sc, bool active, double part, int
     if (sh_last && threadIdx.x < 32) {
         __threadfence();
         const double s = scene_sum_warp(D.partial, P.tile_begin, P.tile_end);
+        const double s2 = kind == K_V_B ? scene_sum_warp(D.partial + D.n_tiles, P.tile_begin, P.tile_end) : 0.0;
         if (threadIdx.x == 0) {
             D.scene_counter[sc] = 0;
-            scene_finalize(D, sc, kind, s);
+            scene_decide(D, D.scenes[sc], D.ctl[sc], kind, s, true, s2);
             __threadfence();
         }
     }
@@ -442,6 +496,7 @@ __global__ void __launch_bounds__(256, 4) k_nbr_build(const Dev D) {
         D.kd[i] = kd;
         D.c[i] = dens - D.rho0s[i];
         const int p = D.pid[i];
+        D.rflu[i] = D.material[p] == 1 ? __frcp_rn(dens) : 0.0f;
         D.density_out[p] = dens;
         D.k_out[p] = kd;
         if (found > cap) atomicAdd(&D.overflow[sc], 1);
@@ -497,6 +552,7 @@ __global__ void __launch_bounds__(BLOCK) k_density(const Dev D) {
         D.dens[i] = rho;
         D.c[i] = rho - D.rho0s[i];
         D.density_out[pi] = rho;
+        D.rflu[i] = D.material[pi] == 1 ? __frcp_rn(rho) : 0.0f;
     }
 }
 
@@ -553,14 +609,7 @@ __global__ void k_gravity(const Dev D) {
 __global__ void k_solve_begin(const Dev D) {
     const int4 tile = D.tiles[blockIdx.x];
     const SceneParams& P = D.scenes[tile.x];
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        long lim = 64;
-        for (int s = 0; s < D.n_scenes; ++s)
-            lim += (long)(D.scenes[s].max_outer + 1) * (long)(2 * D.scenes[s].max_pcg + 3);
-        D.flags->limit = lim > 0x3fffffff ? 0x3fffffff : (int)lim;
-        D.flags->launches = 0;
-        D.flags->timeout = 0;
-    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) guard_begin(D);
     if (blockIdx.x == P.tile_begin && threadIdx.x == 0) ctl_begin(P, D.ctl[tile.x]);
     const int i = tile.y + threadIdx.x;
     if (i >= tile.z) return;
@@ -581,6 +630,7 @@ __global__ void k_solve_end(const Dev D) {
         W.acc_solves += 1;
         W.acc_outer += C.outer_it;
         W.acc_cg += C.total_cg;
+        W.acc_visc += C.v_total;
         if (C.final_err > W.acc_max_final_err) W.acc_max_final_err = C.final_err;
         if (C.status != IVP_OK_) {
             W.acc_failed += 1;
@@ -913,6 +963,193 @@ __device__ __forceinline__ void div_tile(const Dev& D, const SceneParams& P, con
     if (T.valid && T.lane == 0 && D.div_out) D.div_out[D.pid[T.i]] = acc > 0.0f ? acc : 0.0f;
 }
 
+// ---- Weiler 2018 implicit viscosity (weiler18.py:21-401), slot order
+
+// L_i(u) over fluid neighbours (weiler18.py:150-169):
+//   d (m_j / rho_j) (u_ij . x_ij) / (|x_ij|^2 + 0.01 h^2) grad W_ij
+// = d (1/rho_j) (u_ij . x_ij) / (|x_ij|^2 + 0.01 h^2) J_ij,  d = 10;
+// rflu_j = 1/rho_j for fluid j, 0 otherwise (the reference's `continue`).
+__device__ __forceinline__ float visc_factor(const Dev& D, const SceneParams& P, int i) {
+    const float mu = P.visc_coeff * D.rho0s[i];  // weiler18.py:146
+    return P.dt * mu / D.dens[i];
+}
+
+// Setup (weiler18.py:381-396): 3x3 block-Jacobi inverse M_i^-1 of
+// I - dt mu_i/rho_i L_ii (weiler18.py:21-85), rhs = v - A v, r = rhs,
+// z = M^-1 r, dv = 0, p_prev = 0; partial r.z.
+template <int G>
+__device__ __forceinline__ double visc_setup_tile(const Dev& D, const SceneParams& P, const TileCtx& T) {
+    const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
+    const float4* nb = D.nbr + (size_t)T.row * D.stride;
+    const bool fluid = T.valid && D.rflu[T.i] != 0.0f;
+    float3 xi = make_float3(0.f, 0.f, 0.f), vi = xi;
+    if (T.valid) {
+        xi = f3(D.xm[T.i]);
+        const int p = D.pid[T.i];
+        vi = make_float3(D.v[3 * p], D.v[3 * p + 1], D.v[3 * p + 2]);
+        D.vs[T.i] = make_float4(vi.x, vi.y, vi.z, 0.0f);
+    }
+    const float eps2 = 0.01f * P.h * P.h;
+    float L[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) L[q] = 0.0f;
+    float lx = 0.0f, ly = 0.0f, lz = 0.0f;
+    bool bad = false;
+    const int self = T.valid ? T.i : P.s_begin;
+    for (int k0 = T.lane; k0 < (fluid ? cnt : 0); k0 += G * PU) {
+        PairBatch b;
+        bad |= load_pairs<G>(nb, k0, cnt, self, P.s_begin, P.s_end, b);
+#pragma unroll
+        for (int u = 0; u < PU; ++u) {
+            const int j = b.j[u];
+            const float3 xij = sub3(xi, f3(__ldg(D.xm + j)));
+            const int pj = D.pid[j];
+            const float3 vij = sub3(vi, make_float3(__ldcg(D.v + 3 * pj), __ldcg(D.v + 3 * pj + 1), __ldcg(D.v + 3 * pj + 2)));
+            const float rsq = dot3(xij, xij);
+            const float c = (10.0f * __ldg(D.rflu + j)) * __frcp_rn(rsq + eps2);
+            const float3 J = b.J[u];
+            const float Jv[3] = {J.x, J.y, J.z}, Xv[3] = {xij.x, xij.y, xij.z};
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int q = 0; q < 3; ++q) L[3 * r + q] += c * (Jv[r] * Xv[q]);
+            const float s = c * dot3(vij, xij);
+            lx += s * J.x;
+            ly += s * J.y;
+            lz += s * J.z;
+        }
+    }
+    if (bad) flag_bad(D, T.i, 5);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) L[q] = group_sum<G>(L[q]);
+    lx = group_sum<G>(lx);
+    ly = group_sum<G>(ly);
+    lz = group_sum<G>(lz);
+    double part = 0.0;
+    if (T.valid && T.lane == 0) {
+        float M[9];
+        float3 av = vi;
+        if (fluid) {
+            const float f = visc_factor(D, P, T.i);
+#pragma unroll
+            for (int q = 0; q < 9; ++q) M[q] = ((q % 4 == 0) ? 1.0f : 0.0f) - f * L[q];
+            av = make_float3(vi.x - f * lx, vi.y - f * ly, vi.z - f * lz);
+        } else {
+#pragma unroll
+            for (int q = 0; q < 9; ++q) M[q] = (q % 4 == 0) ? 1.0f : 0.0f;
+        }
+        // inverse by the adjugate (wp.inverse)
+        const float c00 = M[4] * M[8] - M[5] * M[7], c01 = M[5] * M[6] - M[3] * M[8], c02 = M[3] * M[7] - M[4] * M[6];
+        const float id = 1.0f / (M[0] * c00 + M[1] * c01 + M[2] * c02);
+        const float4 r0 = make_float4(c00 * id, (M[2] * M[7] - M[1] * M[8]) * id, (M[1] * M[5] - M[2] * M[4]) * id, 0.f);
+        const float4 r1 = make_float4(c01 * id, (M[0] * M[8] - M[2] * M[6]) * id, (M[2] * M[3] - M[0] * M[5]) * id, 0.f);
+        const float4 r2 = make_float4(c02 * id, (M[1] * M[6] - M[0] * M[7]) * id, (M[0] * M[4] - M[1] * M[3]) * id, 0.f);
+        D.pinv[3 * T.i] = r0;
+        D.pinv[3 * T.i + 1] = r1;
+        D.pinv[3 * T.i + 2] = r2;
+        const float3 rh = make_float3(vi.x + (-1.0f) * av.x, vi.y + (-1.0f) * av.y, vi.z + (-1.0f) * av.z);
+        const float3 z = make_float3(dot3(f3(r0), rh), dot3(f3(r1), rh), dot3(f3(r2), rh));
+        D.r[T.i] = make_float4(rh.x, rh.y, rh.z, 0.f);
+        D.vz[T.i] = make_float4(z.x, z.y, z.z, 0.f);
+        D.sol[T.i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        D.p0[T.i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        part = (double)dot3(rh, z);
+    }
+    return part;
+}
+
+// CG phase A (weiler18.py:332-333, 361-364): p = z + beta p_prev (formed on
+// the fly for the neighbours), A p = p - dt mu/rho L(p); partial p.Ap.
+template <int G>
+__device__ __forceinline__ double visc_a_tile(const Dev& D, const SceneParams& P, const TileCtx& T, float beta,
+                                              int it) {
+    const float4* pp = (it & 1) ? D.p1 : D.p0;
+    float4* pn = (it & 1) ? D.p0 : D.p1;
+    const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
+    const float4* nb = D.nbr + (size_t)T.row * D.stride;
+    const bool fluid = T.valid && D.rflu[T.i] != 0.0f;
+    float3 xi = make_float3(0.f, 0.f, 0.f), pi = xi;
+    if (T.valid) {
+        xi = f3(D.xm[T.i]);
+        const float4 zi = D.vz[T.i], qi = pp[T.i];
+        pi = make_float3(zi.x + beta * qi.x, zi.y + beta * qi.y, zi.z + beta * qi.z);
+    }
+    const float eps2 = 0.01f * P.h * P.h;
+    float lx = 0.0f, ly = 0.0f, lz = 0.0f;
+    bool bad = false;
+    const int self = T.valid ? T.i : P.s_begin;
+    for (int k0 = T.lane; k0 < (fluid ? cnt : 0); k0 += G * PU) {
+        PairBatch b;
+        bad |= load_pairs<G>(nb, k0, cnt, self, P.s_begin, P.s_end, b);
+#pragma unroll
+        for (int u = 0; u < PU; ++u) {
+            const int j = b.j[u];
+            const float3 xij = sub3(xi, f3(__ldg(D.xm + j)));
+            const float4 zj = __ldcg(D.vz + j), qj = __ldcg(pp + j);
+            const float3 pj = make_float3(zj.x + beta * qj.x, zj.y + beta * qj.y, zj.z + beta * qj.z);
+            const float rsq = dot3(xij, xij);
+            const float s = (10.0f * __ldg(D.rflu + j)) * __frcp_rn(rsq + eps2) * dot3(sub3(pi, pj), xij);
+            lx += s * b.J[u].x;
+            ly += s * b.J[u].y;
+            lz += s * b.J[u].z;
+        }
+    }
+    if (bad) flag_bad(D, T.i, 6);
+    lx = group_sum<G>(lx);
+    ly = group_sum<G>(ly);
+    lz = group_sum<G>(lz);
+    double part = 0.0;
+    if (T.valid && T.lane == 0) {
+        float3 ap = pi;
+        if (fluid) {
+            const float f = visc_factor(D, P, T.i);
+            ap = make_float3(pi.x - f * lx, pi.y - f * ly, pi.z - f * lz);
+        }
+        pn[T.i] = make_float4(pi.x, pi.y, pi.z, 0.f);
+        D.vap[T.i] = make_float4(ap.x, ap.y, ap.z, 0.f);
+        part = (double)dot3(pi, ap);
+    }
+    return part;
+}
+
+// CG phase B (weiler18.py:340-359), no neighbours: dv += alpha p,
+// r -= alpha Ap, z = M^-1 r; partials r.r and r.z.
+template <int G>
+__device__ __forceinline__ void visc_b_tile(const Dev& D, const TileCtx& T, float alpha, int it, double* part,
+                                            double* part2) {
+    *part = 0.0;
+    *part2 = 0.0;
+    if (!(T.valid && T.lane == 0)) return;
+    const float4* pc = (it & 1) ? D.p0 : D.p1;
+    const float4 p4 = pc[T.i], ap = D.vap[T.i];
+    float4 x = D.sol[T.i], r = D.r[T.i];
+    x.x = x.x + alpha * p4.x;
+    x.y = x.y + alpha * p4.y;
+    x.z = x.z + alpha * p4.z;
+    const float na = -alpha;
+    r.x = r.x + na * ap.x;
+    r.y = r.y + na * ap.y;
+    r.z = r.z + na * ap.z;
+    D.sol[T.i] = x;
+    D.r[T.i] = r;
+    const float3 rr = f3(r);
+    const float3 z = make_float3(dot3(f3(D.pinv[3 * T.i]), rr), dot3(f3(D.pinv[3 * T.i + 1]), rr),
+                                 dot3(f3(D.pinv[3 * T.i + 2]), rr));
+    D.vz[T.i] = make_float4(z.x, z.y, z.z, 0.f);
+    *part = (double)dot3(rr, rr);
+    *part2 = (double)dot3(rr, z);
+}
+
+// End (weiler18.py:398-401): v += dv, back to the caller's order.
+__device__ __forceinline__ void visc_end_tile(const Dev& D, const TileCtx& T) {
+    if (!(T.valid && T.lane == 0)) return;
+    const int p = D.pid[T.i];
+    const float4 dv = D.sol[T.i];
+    D.v[3 * p] = D.v[3 * p] + 1.0f * dv.x;
+    D.v[3 * p + 1] = D.v[3 * p + 1] + 1.0f * dv.y;
+    D.v[3 * p + 2] = D.v[3 * p + 2] + 1.0f * dv.z;
+}
+
 // ---- one launch per phase (device-side control through graph conditionals)
 
 template <int G, int BLOCK>
@@ -984,6 +1221,73 @@ __global__ void __launch_bounds__(BLOCK) k_divergence(const Dev D) {
     div_tile<G>(D, D.scenes[T.sc], T, D.ctl[T.sc].outer_it);
 }
 
+// viscosity, one launch per phase
+__global__ void k_visc_begin(const Dev D) {
+    const int4 tile = D.tiles[blockIdx.x];
+    const SceneParams& P = D.scenes[tile.x];
+    if (blockIdx.x == 0 && threadIdx.x == 0) guard_begin(D);
+    if (blockIdx.x == P.tile_begin && threadIdx.x == 0) {
+        SceneCtl& C = D.ctl[tile.x];
+        C.v_on = (visc_on(P) && P.n_dyn > 0) ? 1 : 0;
+        C.v_active = 0;
+        C.v_total = 0;
+    }
+}
+
+template <int G, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_visc_setup(const Dev D) {
+    const TileCtx T = tile_ctx<G>(D, blockIdx.x);
+    __shared__ int sh_active;
+    if (threadIdx.x == 0) sh_active = D.ctl[T.sc].v_on;
+    __syncthreads();
+    const bool active = sh_active != 0;
+    double part = 0.0;
+    if (active) part = visc_setup_tile<G>(D, D.scenes[T.sc], T);
+    block_finish<BLOCK>(D, T.sc, active, part, K_V_SETUP);
+}
+
+template <int G, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_visc_a(const Dev D) {
+    const TileCtx T = tile_ctx<G>(D, blockIdx.x);
+    __shared__ int sh_active, sh_it;
+    __shared__ float sh_beta;
+    if (threadIdx.x == 0) {
+        const SceneCtl& C = D.ctl[T.sc];
+        sh_active = C.v_active;
+        sh_it = C.v_it;
+        sh_beta = (float)C.v_beta;
+    }
+    __syncthreads();
+    const bool active = sh_active != 0;
+    double part = 0.0;
+    if (active) part = visc_a_tile<G>(D, D.scenes[T.sc], T, sh_beta, sh_it);
+    block_finish<BLOCK>(D, T.sc, active, part, K_V_A);
+}
+
+template <int G, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_visc_b(const Dev D) {
+    const TileCtx T = tile_ctx<G>(D, blockIdx.x);
+    __shared__ int sh_active, sh_it;
+    __shared__ float sh_alpha;
+    if (threadIdx.x == 0) {
+        const SceneCtl& C = D.ctl[T.sc];
+        sh_active = C.v_active;
+        sh_it = C.v_it;
+        sh_alpha = (float)C.v_alpha;
+    }
+    __syncthreads();
+    const bool active = sh_active != 0;
+    double part = 0.0, part2 = 0.0;
+    if (active) visc_b_tile<G>(D, T, sh_alpha, sh_it, &part, &part2);
+    block_finish<BLOCK>(D, T.sc, active, part, K_V_B, part2);
+}
+
+template <int G, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_visc_end(const Dev D) {
+    const TileCtx T = tile_ctx<G>(D, blockIdx.x);
+    if (D.ctl[T.sc].v_on) visc_end_tile(D, T);
+}
+
 // ---- the whole IP.solve in one persistent cooperative launch
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
@@ -1003,7 +1307,14 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
 constexpr unsigned long long kBarrierLimitNs = 2000000000ull;
 
 __device__ __forceinline__ bool phase_active(const SceneCtl& C, int kind) {
-    return kind == K_PACK ? C.outer_active != 0 : kind == K_RHS ? C.solve_pending != 0 : C.cg_active != 0;
+    switch (kind) {
+        case K_PACK: return C.outer_active != 0;
+        case K_RHS: return C.solve_pending != 0;
+        case K_CG_A:
+        case K_CG_B: return C.cg_active != 0;
+        case K_V_SETUP: return C.v_on != 0;
+        default: return C.v_active != 0;
+    }
 }
 
 __device__ __forceinline__ SceneCtl ctl_load(const SceneCtl* p) {
@@ -1015,7 +1326,7 @@ __device__ __forceinline__ SceneCtl ctl_load(const SceneCtl* p) {
     return c;
 }
 
-__device__ bool grid_reduce_barrier(const Dev& D, int kind, int* sh_flag, double* sum_sh) {
+__device__ bool grid_reduce_barrier(const Dev& D, int kind, int* sh_flag, double* sum_sh, double* sum_sh2) {
     unsigned g = 0;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -1033,14 +1344,18 @@ __device__ bool grid_reduce_barrier(const Dev& D, int kind, int* sh_flag, double
                 if (!phase_active(ctl_load(D.ctl + s), kind)) continue;
                 const SceneParams& P = D.scenes[s];
                 const double v = scene_sum_warp(D.partial, P.tile_begin, P.tile_end);
-                if ((threadIdx.x & 31) == 0) sum_sh[s] = v;
+                const double v2 = kind == K_V_B ? scene_sum_warp(D.partial + D.n_tiles, P.tile_begin, P.tile_end) : 0.0;
+                if ((threadIdx.x & 31) == 0) {
+                    sum_sh[s] = v;
+                    sum_sh2[s] = v2;
+                }
             }
             __syncthreads();
             if (threadIdx.x == 0)
                 for (int s = 0; s < D.n_scenes; ++s) {
                     SceneCtl c = ctl_load(D.ctl + s);
                     if (!phase_active(c, kind)) continue;
-                    scene_decide(D, D.scenes[s], c, kind, sum_sh[s], true);
+                    scene_decide(D, D.scenes[s], c, kind, sum_sh[s], true, sum_sh2[s]);
                     D.ctl[s] = c;
                 }
         }
@@ -1072,8 +1387,9 @@ __device__ bool grid_reduce_barrier(const Dev& D, int kind, int* sh_flag, double
 template <int G, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_ip_persistent(const Dev D) {
     extern __shared__ double dyn_sh[];
-    double* sum_sh = dyn_sh;                                             // [n_scenes]
-    SceneCtl* sc_sh = reinterpret_cast<SceneCtl*>(dyn_sh + D.n_scenes);  // [n_scenes]
+    double* sum_sh = dyn_sh;                                                 // [n_scenes]
+    double* sum_sh2 = dyn_sh + D.n_scenes;                                   // [n_scenes]
+    SceneCtl* sc_sh = reinterpret_cast<SceneCtl*>(dyn_sh + 2 * D.n_scenes);  // [n_scenes]
     __shared__ double red_sh[32];
     __shared__ int flag_sh[2], any_sh;
     const int t0 = (int)(((long long)blockIdx.x * D.n_tiles) / gridDim.x);
@@ -1081,18 +1397,14 @@ __global__ void __launch_bounds__(BLOCK) k_ip_persistent(const Dev D) {
     // CTA 0 starts every scene's control block (reset_stats); the first
     // barrier publishes it
     if (blockIdx.x == 0 && threadIdx.x == 0)
-        for (int s = 0; s < D.n_scenes; ++s) ctl_begin(D.scenes[s], D.ctl[s]);
-    // d = dt v (ip.py:343) for the owned particles
-    for (int t = t0; t < t1; ++t) {
-        const int4 tile = __ldg(D.tiles + t);
-        const SceneParams& P = D.scenes[tile.x];
-        for (int i = tile.y + threadIdx.x; i < tile.z; i += BLOCK) {
-            const int p = D.pid[i];
-            const float dt = P.dt;
-            D.d0[i] = make_float4(dt * D.v[3 * p], dt * D.v[3 * p + 1], dt * D.v[3 * p + 2], 0.0f);
+        for (int s = 0; s < D.n_scenes; ++s) {
+            const SceneParams& P = D.scenes[s];
+            ctl_begin(P, D.ctl[s]);
+            D.ctl[s].v_on = (D.visc_enabled && visc_on(P) && P.n_dyn > 0) ? 1 : 0;
+            D.ctl[s].v_active = 0;
+            D.ctl[s].v_total = 0;
         }
-    }
-    if (!grid_reduce_barrier(D, -1, flag_sh, sum_sh)) return;
+    if (!grid_reduce_barrier(D, -1, flag_sh, sum_sh, sum_sh2)) return;
     // local copies of the control blocks, refreshed after every phase
     auto refresh = [&]() {
         for (int s = threadIdx.x; s < D.n_scenes; s += BLOCK) sc_sh[s] = ctl_load(D.ctl + s);
@@ -1107,30 +1419,37 @@ __global__ void __launch_bounds__(BLOCK) k_ip_persistent(const Dev D) {
             const SceneCtl& C = sc_sh[T.sc];
             if (!phase_active(C, kind)) continue;
             const SceneParams& P = D.scenes[T.sc];
-            double part;
+            double part, part2 = 0.0;
             if (kind == K_PACK) part = pack_tile<G>(D, P, T, C.outer_it);
             else if (kind == K_RHS) part = rhs_tile<G>(D, P, T);
             else if (kind == K_CG_A) part = cga_tile<G>(D, P, T, (float)C.beta, C.cg_it);
-            else part = cgb_tile<G>(D, P, T, (float)C.alpha, C.cg_it);
+            else if (kind == K_CG_B) part = cgb_tile<G>(D, P, T, (float)C.alpha, C.cg_it);
+            else if (kind == K_V_SETUP) part = visc_setup_tile<G>(D, P, T);
+            else if (kind == K_V_A) part = visc_a_tile<G>(D, P, T, (float)C.v_beta, C.v_it);
+            else visc_b_tile<G>(D, T, (float)C.v_alpha, C.v_it, &part, &part2);
             const double tot = block_sum_d<BLOCK>(part, red_sh);
-            if (threadIdx.x == 0) D.partial[t] = tot;
+            const double tot2 = kind == K_V_B ? block_sum_d<BLOCK>(part2, red_sh) : 0.0;
+            if (threadIdx.x == 0) {
+                D.partial[t] = tot;
+                D.partial[D.n_tiles + t] = tot2;
+            }
         }
-        if (!grid_reduce_barrier(D, kind, flag_sh, sum_sh)) return false;
+        if (!grid_reduce_barrier(D, kind, flag_sh, sum_sh, sum_sh2)) return false;
         if (++phases > limit) {
             // guard: every CTA reaches the same count; CTA 0 stops the scenes,
             // a barrier publishes it
             if (blockIdx.x == 0 && threadIdx.x == 0) {
                 for (int s = 0; s < D.n_scenes; ++s) {
                     SceneCtl c = ctl_load(D.ctl + s);
-                    if (c.outer_active || c.solve_pending || c.cg_active) {
+                    if (c.outer_active || c.solve_pending || c.cg_active || c.v_active) {
                         c.status = IVP_TIMEOUT_;
-                        c.outer_active = c.solve_pending = c.cg_active = 0;
+                        c.outer_active = c.solve_pending = c.cg_active = c.v_active = 0;
                         D.ctl[s] = c;
                     }
                 }
                 D.flags->timeout = 1;
             }
-            if (!grid_reduce_barrier(D, -1, flag_sh, sum_sh)) return false;
+            if (!grid_reduce_barrier(D, -1, flag_sh, sum_sh, sum_sh2)) return false;
         }
         refresh();
         return true;
@@ -1146,6 +1465,30 @@ __global__ void __launch_bounds__(BLOCK) k_ip_persistent(const Dev D) {
         __syncthreads();
         return r;
     };
+    // implicit viscosity (framework.py:421), then v -> d (ip.py:343)
+    if (any(K_V_SETUP)) {
+        if (!run_phase(K_V_SETUP)) return;
+        while (any(K_V_A)) {
+            if (!run_phase(K_V_A)) return;
+            if (!any(K_V_B)) break;
+            if (!run_phase(K_V_B)) return;
+        }
+        for (int t = t0; t < t1; ++t) {
+            const TileCtx T = tile_ctx<G>(D, t);
+            if (sc_sh[T.sc].v_on) visc_end_tile(D, T);
+        }
+        __syncthreads();
+    }
+    for (int t = t0; t < t1; ++t) {
+        const int4 tile = __ldg(D.tiles + t);
+        const SceneParams& P = D.scenes[tile.x];
+        for (int i = tile.y + threadIdx.x; i < tile.z; i += BLOCK) {
+            const int p = D.pid[i];
+            const float dt = P.dt;
+            D.d0[i] = make_float4(dt * D.v[3 * p], dt * D.v[3 * p + 1], dt * D.v[3 * p + 2], 0.0f);
+        }
+    }
+    if (!grid_reduce_barrier(D, -1, flag_sh, sum_sh, sum_sh2)) return;
     while (any(K_PACK)) {
         if (!run_phase(K_PACK)) return;
         if (!any(K_RHS)) break;
@@ -1178,6 +1521,7 @@ __global__ void __launch_bounds__(BLOCK) k_ip_persistent(const Dev D) {
             c.acc_solves += 1;
             c.acc_outer += c.outer_it;
             c.acc_cg += c.total_cg;
+            c.acc_visc += c.v_on ? c.v_total : 0;
             if (c.final_err > c.acc_max_final_err) c.acc_max_final_err = c.final_err;
             if (c.status != IVP_OK_) {
                 c.acc_failed += 1;
@@ -1193,7 +1537,8 @@ __global__ void k_reset_counters(const Dev D) {
     if (s >= D.n_scenes) return;
     SceneCtl& C = D.ctl[s];
     C.acc_max_final_err = 0.0;
-    C.acc_solves = C.acc_outer = C.acc_cg = C.acc_failed = C.acc_last_failure = 0;
+    C.acc_solves = C.acc_outer = C.acc_cg = C.acc_failed = C.acc_last_failure = C.acc_visc = 0;
+    if (s == 0) D.flags->timeout = 0;
 }
 
 // Neighbour lists of one scene in the reference layout, original indices.

@@ -196,6 +196,10 @@ class Engine:
         """IP.solve(dt) of every scene (asynchronous)."""
         check(self.L.ivp_ip_solve(self._handle, ctypes.c_void_p(_stream_ptr(stream))), "ivp_ip_solve")
 
+    def viscosity_solve(self, stream=None):
+        """Weiler18.solve(coeff, dt) of every scene with implicit viscosity."""
+        check(self.L.ivp_viscosity_solve(self._handle, ctypes.c_void_p(_stream_ptr(stream))), "ivp_viscosity_solve")
+
     def apply_gravity(self, stream=None):
         check(self.L.ivp_apply_gravity(self._handle, ctypes.c_void_p(_stream_ptr(stream))), "ivp_apply_gravity")
 

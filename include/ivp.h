@@ -105,6 +105,7 @@ typedef struct {
     int64_t sum_pcg_iters;
     double max_final_density_error;
     int64_t neighbour_pairs;      /* pairs in the scene's current neighbour lists */
+    int64_t sum_visc_iters;       /* implicit-viscosity CG iterations */
 } ivp_solve_stats;
 
 /* Kernel ids reported by ivp_profile_step. */
@@ -156,6 +157,12 @@ int ivp_compute_aii(ivp_engine* e, void* stream);
 /* IP.solve(dt) (ip.py:331-404) for every scene: outer loop, CG, v = d/dt,
  * stats.  Asynchronous; read results with ivp_read_stats. */
 int ivp_ip_solve(ivp_engine* e, void* stream);
+
+/* Weiler18.solve(coeff, dt) (scripts/sim/forces/non_pressure/viscosity/
+ * weiler18.py:371-401): implicit viscosity with block-Jacobi PCG for every
+ * scene whose viscosity_method is 1 and viscosity_coeff > 0; updates the bound
+ * velocities.  Uses the current neighbour lists and densities. */
+int ivp_viscosity_solve(ivp_engine* e, void* stream);
 
 /* apply_gravity (framework.py:26-41). */
 int ivp_apply_gravity(ivp_engine* e, void* stream);

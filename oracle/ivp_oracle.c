@@ -549,17 +549,183 @@ void orc_advect_and_clamp(int n, float* x, float* v, const int* dyn, float dt, c
     }
 }
 
+/* ----------------------------------------------- Weiler 2018 viscosity */
+
+/* wp.inverse of a 3x3 matrix: adjugate / determinant in FP32 */
+static void inv33(const float* a, float* o) {
+    float c00 = a[4] * a[8] - a[5] * a[7], c01 = a[5] * a[6] - a[3] * a[8], c02 = a[3] * a[7] - a[4] * a[6];
+    float det = a[0] * c00 + a[1] * c01 + a[2] * c02;
+    float id = 1.0f / det;
+    o[0] = c00 * id;
+    o[1] = (a[2] * a[7] - a[1] * a[8]) * id;
+    o[2] = (a[1] * a[5] - a[2] * a[4]) * id;
+    o[3] = c01 * id;
+    o[4] = (a[0] * a[8] - a[2] * a[6]) * id;
+    o[5] = (a[2] * a[3] - a[0] * a[5]) * id;
+    o[6] = c02 * id;
+    o[7] = (a[1] * a[6] - a[0] * a[7]) * id;
+    o[8] = (a[0] * a[4] - a[1] * a[3]) * id;
+}
+
+typedef struct {
+    float visc;        /* kinematic viscosity (viscosityCoeff) */
+    float dt;
+    float h;
+    int cache;
+    int max_iter;      /* weiler18.py:208 */
+    double tol;        /* weiler18.py:209, absolute on r.r */
+    int fast;          /* FP64 dots (1) or FP32 in index order (0) */
+} orc_visc_params;
+
+/* compute_precond_weiler18 (weiler18.py:21-85): inverse of the 3x3 diagonal
+ * block of I - dt mu / rho L over fluid neighbours */
+static void visc_precond(int n, const orc_visc_params* V, const float* x, const float* m, const float* density,
+                         const float* rho0, const int* material, const int* dyn, const int* count, const int* ids,
+                         const float* gradW, float* pinv) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) {
+        float* o = pinv + 9 * (size_t)i;
+        if (!dyn[i] || material[i] != 1) {
+            for (int q = 0; q < 9; ++q) o[q] = (q % 4 == 0) ? 1.0f : 0.0f;
+            continue;
+        }
+        float eps2 = 0.01f * V->h * V->h;
+        float d = 10.0f;
+        float mu = V->visc * rho0[i];
+        float factor = V->dt * mu / density[i];
+        float L[9] = {0};
+        int cnt = clamp_cnt(count[i], V->cache);
+        for (int k = 0; k < cnt; ++k) {
+            long b = (long)i * V->cache + k;
+            int j = ids[b];
+            if (material[j] != 1) continue;
+            float xij[3] = {x[3 * i] - x[3 * j], x[3 * i + 1] - x[3 * j + 1], x[3 * i + 2] - x[3 * j + 2]};
+            float rsq = dot3(xij, xij);
+            const float* g = gradW + 3 * b;
+            float c = d * (m[j] / density[j]) / (rsq + eps2);
+            for (int r = 0; r < 3; ++r)
+                for (int q = 0; q < 3; ++q) L[3 * r + q] = L[3 * r + q] + c * (g[r] * xij[q]);
+        }
+        float M[9];
+        for (int q = 0; q < 9; ++q) M[q] = ((q % 4 == 0) ? 1.0f : 0.0f) - factor * L[q];
+        inv33(M, o);
+    }
+}
+
+/* compute_Av_weiler18 (weiler18.py:103-172): (A v)_i = v_i - dt mu_i / rho_i L_i(v) */
+static void visc_Av(int n, const orc_visc_params* V, const float* x, const float* vin, const float* m,
+                    const float* density, const float* rho0, const int* material, const int* dyn, const int* count,
+                    const int* ids, const float* gradW, float* av) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) {
+        const float* vi = vin + 3 * i;
+        if (!dyn[i] || material[i] != 1) {
+            for (int c = 0; c < 3; ++c) av[3 * i + c] = vi[c];
+            continue;
+        }
+        float eps2 = 0.01f * V->h * V->h;
+        float d = 10.0f;
+        float mu = V->visc * rho0[i];
+        float factor = V->dt * mu / density[i];
+        float lap[3] = {0.0f, 0.0f, 0.0f};
+        int cnt = clamp_cnt(count[i], V->cache);
+        for (int k = 0; k < cnt; ++k) {
+            long b = (long)i * V->cache + k;
+            int j = ids[b];
+            if (material[j] != 1) continue;
+            float xij[3] = {x[3 * i] - x[3 * j], x[3 * i + 1] - x[3 * j + 1], x[3 * i + 2] - x[3 * j + 2]};
+            float vij[3] = {vi[0] - vin[3 * j], vi[1] - vin[3 * j + 1], vi[2] - vin[3 * j + 2]};
+            float rsq = dot3(xij, xij);
+            float vx = dot3(vij, xij);
+            float s = d * (m[j] / density[j]) * (vx / (rsq + eps2));
+            const float* g = gradW + 3 * b;
+            for (int c = 0; c < 3; ++c) lap[c] += s * g[c];
+        }
+        for (int c = 0; c < 3; ++c) av[3 * i + c] = vi[c] - factor * lap[c];
+    }
+}
+
+static void mat33_vec(const float* M, const float* v, float* o) {
+    for (int r = 0; r < 3; ++r) o[r] = M[3 * r] * v[0] + M[3 * r + 1] * v[1] + M[3 * r + 2] * v[2];
+}
+
+/* Weiler18.solve (weiler18.py:371-401) with its block-Jacobi PCG
+ * (weiler18.py:298-365): v += dv, A dv = v - A v, dv_0 = 0.  Returns the CG
+ * iterations. */
+int orc_weiler18_solve(int n, const orc_visc_params* V, const float* x, float* v, const float* m,
+                       const float* density, const float* rho0, const int* material, const int* dyn,
+                       const int* count, const int* ids, const float* gradW) {
+    size_t n3 = 3 * (size_t)n;
+    float* pinv = (float*)calloc(9 * (size_t)n, sizeof(float));
+    float* dv = (float*)calloc(n3, sizeof(float));
+    float* r = (float*)calloc(n3, sizeof(float));
+    float* z = (float*)calloc(n3, sizeof(float));
+    float* p = (float*)calloc(n3, sizeof(float));
+    float* ap = (float*)calloc(n3, sizeof(float));
+    float* rhs = (float*)calloc(n3, sizeof(float));
+    visc_precond(n, V, x, m, density, rho0, material, dyn, count, ids, gradW, pinv);
+    visc_Av(n, V, x, v, m, density, rho0, material, dyn, count, ids, gradW, ap);
+    for (int i = 0; i < n; ++i)
+        if (dyn[i])
+            for (int c = 0; c < 3; ++c) rhs[3 * i + c] = v[3 * i + c] + (-1.0f) * ap[3 * i + c];
+    memcpy(r, rhs, sizeof(float) * n3);
+    for (int i = 0; i < n; ++i)
+        if (dyn[i]) mat33_vec(pinv + 9 * (size_t)i, r + 3 * i, z + 3 * i);
+    memcpy(p, z, sizeof(float) * n3);
+    double rz_old = dot_dyn(n, r, z, dyn, V->fast);
+    int it = 0;
+    if (rz_old > 1e-12) {
+        for (;;) {
+            visc_Av(n, V, x, p, m, density, rho0, material, dyn, count, ids, gradW, ap);
+            double pap = dot_dyn(n, p, ap, dyn, V->fast);
+            if (pap <= 0.0) break;
+            double alpha = rz_old / (pap > 1e-12 ? pap : 1e-12);
+            float af = (float)alpha;
+            for (int i = 0; i < n; ++i)
+                if (dyn[i])
+                    for (int c = 0; c < 3; ++c) dv[3 * i + c] = dv[3 * i + c] + af * p[3 * i + c];
+            float naf = (float)(-alpha);
+            for (int i = 0; i < n; ++i)
+                if (dyn[i])
+                    for (int c = 0; c < 3; ++c) r[3 * i + c] = r[3 * i + c] + naf * ap[3 * i + c];
+            double rr = dot_dyn(n, r, r, dyn, V->fast);
+            ++it;
+            if ((rr < V->tol && it >= 2) || it >= V->max_iter) break;
+            for (int i = 0; i < n; ++i)
+                if (dyn[i]) mat33_vec(pinv + 9 * (size_t)i, r + 3 * i, z + 3 * i);
+            double rz_new = dot_dyn(n, r, z, dyn, V->fast);
+            double beta = rz_new / (rz_old > 1e-12 ? rz_old : 1e-12);
+            float bf = (float)beta;
+            for (int i = 0; i < n; ++i)
+                if (dyn[i])
+                    for (int c = 0; c < 3; ++c) p[3 * i + c] = z[3 * i + c] + bf * p[3 * i + c];
+            rz_old = rz_new;
+        }
+    }
+    for (int i = 0; i < n; ++i)
+        if (dyn[i])
+            for (int c = 0; c < 3; ++c) v[3 * i + c] = v[3 * i + c] + 1.0f * dv[3 * i + c];
+    free(pinv); free(dv); free(r); free(z); free(p); free(ap); free(rhs);
+    return it;
+}
+
 /*
- * One Framework.forward() step with IP and no viscosity / surface tension
- * (framework.py:423-544): gravity, IP.solve, advect + clamp, neighbour
- * rebuild, density, Aii.  `count/ids/gradW/density/kd` must hold the state of
+ * One Framework.forward() step with IP (framework.py:423-544): gravity,
+ * Weiler18 implicit viscosity when `visc` > 0 (no surface tension), IP.solve,
+ * advect + clamp, neighbour rebuild, density, Aii.  `count/ids/gradW/density/kd` must hold the state of
  * the previous rebuild (Framework.initialize, framework.py:282-290).
  */
 int orc_step(int n, const orc_params* P, float dt, const float* g, const float* domain, float* x, float* v,
              const float* rho0, const float* m, const float* m_inv, const int* dyn, int* count, int* ids,
              float* gradW, float* density, float* kd, double* err_hist, int* pcg_hist, orc_stats* st,
-             long* overflow) {
+             long* overflow, const int* material, float visc, int* visc_iters) {
     orc_apply_gravity(n, v, dyn, g, dt);
+    if (material && visc > 0.0f) {
+        /* Weiler18 implicit viscosity (framework.py:400-421) */
+        orc_visc_params V = {visc, dt, P->h, P->cache_size, 1000, 1e-5, P->fast};
+        int it = orc_weiler18_solve(n, &V, x, v, m, density, rho0, material, dyn, count, ids, gradW);
+        if (visc_iters) *visc_iters = it;
+    }
     int status = orc_ip_solve(n, P, dt, density, rho0, m, dyn, count, ids, gradW, kd, v, err_hist, pcg_hist,
                               NULL, NULL, st);
     orc_advect_and_clamp(n, x, v, dyn, dt, domain, P->h);

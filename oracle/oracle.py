@@ -36,6 +36,18 @@ class Params(ctypes.Structure):
     ]
 
 
+class ViscParams(ctypes.Structure):
+    _fields_ = [
+        ("visc", ctypes.c_float),
+        ("dt", ctypes.c_float),
+        ("h", ctypes.c_float),
+        ("cache", ctypes.c_int),
+        ("max_iter", ctypes.c_int),
+        ("tol", ctypes.c_double),
+        ("fast", ctypes.c_int),
+    ]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [
         ("outer_iters", ctypes.c_int),
@@ -73,7 +85,9 @@ def lib():
         L.orc_apply_gravity.argtypes = [i, P, P, P, f]
         L.orc_advect_and_clamp.argtypes = [i, P, P, P, f, P, f]
         L.orc_step.argtypes = [i, ctypes.POINTER(Params), f, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P,
-                               ctypes.POINTER(Stats), ctypes.POINTER(l)]
+                               ctypes.POINTER(Stats), ctypes.POINTER(l), P, f, P]
+        L.orc_weiler18_solve.argtypes = [i, ctypes.POINTER(ViscParams), P, P, P, P, P, P, P, P, P, P]
+        L.orc_weiler18_solve.restype = i
         L.orc_step.restype = i
         L.orc_cg_f64.argtypes = [i, f, i, P, P, P, P, P, P, P, P, d, i, P]
         L.orc_cg_f64.restype = i
@@ -140,6 +154,9 @@ class State:
     max_outer: int = 1000
     max_pcg: int = 1000
     fixed_iters: bool = False
+    material: Optional[np.ndarray] = None
+    viscosity: float = 0.0        # Weiler18 kinematic viscosity (0 = off)
+    visc_iters: int = 0
     count: Optional[np.ndarray] = None
     ids: Optional[np.ndarray] = None
     gradW: Optional[np.ndarray] = None
@@ -161,7 +178,9 @@ class State:
                   cache_size=sc.cache_size, domain_size=_f32(sc.domain_size),
                   gravity=_f32(sc.gravity), dt=sc.dt, omega=sc.omega, tol_pcg=sc.tol_pcg,
                   tol_opt=sc.density_error_tol, max_outer=sc.max_outer_iters,
-                  max_pcg=sc.max_iteration_pcg, fixed_iters=sc.fixed_outer_iters)
+                  max_pcg=sc.max_iteration_pcg, fixed_iters=sc.fixed_outer_iters,
+                  material=_i32(sc.material),
+                  viscosity=float(sc.viscosity_coeff) if int(sc.viscosity_method) == 1 else 0.0)
         kw.update(over)
         return cls(**kw)
 
@@ -227,14 +246,25 @@ class State:
         pcg = np.zeros(max(self.max_outer, 1), np.int32)
         st = Stats()
         ov = ctypes.c_long(0)
+        vit = ctypes.c_int(0)
         status = lib().orc_step(n, ctypes.byref(P), float(self.dt), _p(self.gravity), _p(self.domain_size),
                                 _p(self.x), _p(self.v), _p(self.density0), _p(self.m), _p(self.m_inv),
                                 _p(self.is_dynamic), _p(self.count), _p(self.ids), _p(self.gradW),
-                                _p(self.density), _p(self.k), _p(err), _p(pcg), ctypes.byref(st), ctypes.byref(ov))
+                                _p(self.density), _p(self.k), _p(err), _p(pcg), ctypes.byref(st), ctypes.byref(ov),
+                                _p(self.material), float(self.viscosity), ctypes.byref(vit))
+        self.visc_iters = int(vit.value)
         self._record(st, err, pcg)
         self.overflow = int(ov.value)
         self.status = int(status)
         return int(status)
+
+    # --- Weiler18.solve (weiler18.py:371-401) on the current lists
+    def viscosity_solve(self, coeff: float, fast: bool = True) -> int:
+        V = ViscParams(visc=float(coeff), dt=float(self.dt), h=self.h, cache=self.cache_size, max_iter=1000,
+                       tol=1e-5, fast=int(fast))
+        return int(lib().orc_weiler18_solve(self.n, ctypes.byref(V), _p(self.x), _p(self.v), _p(self.m),
+                                            _p(self.density), _p(self.density0), _p(self.material),
+                                            _p(self.is_dynamic), _p(self.count), _p(self.ids), _p(self.gradW)))
 
     # --- one outer-iteration linear system and its FP64 solution
     def system(self, d: np.ndarray):

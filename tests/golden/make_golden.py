@@ -12,6 +12,9 @@ tests read.
 Fixtures
 --------
 kernels.npz       cubic_kernel / spiky_kernel_derivative at sampled radii;
+visc_solve.npz    one Weiler18 implicit-viscosity solve (weiler18.py:371-401) on
+                  the moving block;
+column_visc_steps.npz  Framework.forward() steps with Weiler18 viscosity on;
 block_solve.npz   one IP solve (ip.py:331-404) from a compressed, moving block
                   inside a static box, after the reference's neighbour build,
                   density and Aii;
@@ -67,7 +70,7 @@ class _Cfg:
     """Stand-in for config_builder.SimConfig with the keys the hot path reads."""
 
 
-def _make_objects(sc):
+def _make_objects(sc, viscosity_method=0, viscosity_coeff=0.0):
     from scripts.io.config_builder import SimConfig
     from scripts.sim.simulation_data import SimulationData
     from scripts.sim.neighbour_search import NeighbourSearch
@@ -75,8 +78,8 @@ def _make_objects(sc):
     conf = sc.config()
     cfg = SimConfig(domain_size=tuple(float(s) for s in sc.domain_size), domain_start=(0.0, 0.0, 0.0),
                     particle_radius=sc.particle_radius, dt=sc.dt, density0=1000.0,
-                    gravity=tuple(sc.gravity), viscosity_method=0, surface_tension_method=0,
-                    viscosity_coeff=0.0, surface_tension_coeff=0.0,
+                    gravity=tuple(sc.gravity), viscosity_method=viscosity_method, surface_tension_method=0,
+                    viscosity_coeff=viscosity_coeff, surface_tension_coeff=0.0,
                     scene_data={"Configuration": conf})
     ps = SimulationData(cfg)
     ps.allocate(sc.n)
@@ -150,12 +153,36 @@ class _NoForce:
         pass
 
 
-def make_column_steps(out, steps):
+def make_visc_solve(out, coeff=0.05):
+    """One Weiler18.solve (weiler18.py:371-401) on the moving block."""
+    from scripts.sim.forces.pressure.ip import IP
+    from scripts.sim.forces.non_pressure.viscosity.weiler18 import Weiler18
+    sc = _scene_block()
+    cfg, ps, ns = _make_objects(sc, 1, coeff)
+    solver = IP(ps, ns, cfg)
+    ns.build(ps.x, ps.particle_num)
+    ns.build_cache(ps.x, ps.particle_num, int(ps.cache_size), ps.neighbor_count, ps.neighbor_ids,
+                   ps.neighbor_gradW)
+    solver.compute_density()
+    visc = Weiler18(ps, ns, cfg)
+    v_before = ps.v.numpy().copy()
+    t0 = time.time()
+    visc.solve(coeff, sc.dt)
+    print(f"visc_solve: {time.time() - t0:.1f}s")
+    np.savez_compressed(
+        out, x=sc.x, v0=v_before, is_dynamic=sc.is_dynamic, material=sc.material, density0=sc.density0,
+        particle_radius=np.float64(sc.particle_radius), domain_size=sc.domain_size, dt=np.float64(sc.dt),
+        coeff=np.float64(coeff), density=ps.density.numpy().copy(), v=ps.v.numpy().copy(),
+        dv=visc.dv.numpy().copy())
+
+
+def make_column_steps(out, steps, viscosity=0.0):
     from scripts.framework import Framework
     sc = _scene_column()
-    cfg, ps, ns = _make_objects(sc)
+    cfg, ps, ns = _make_objects(sc, 1 if viscosity > 0 else 0, viscosity)
     fw = Framework(ps, ns, cfg)
-    fw.viscosity = _NoForce()
+    if viscosity <= 0:
+        fw.viscosity = _NoForce()
     fw.surface_tension = _NoForce()
     fw.initialize()
     nd = sc.n_dynamic
@@ -190,7 +217,7 @@ def make_column_steps(out, steps):
     np.savez_compressed(
         out, x0=sc.x, v0=sc.v, is_dynamic=sc.is_dynamic, material=sc.material, density0=sc.density0,
         particle_radius=np.float64(sc.particle_radius), domain_size=sc.domain_size, dt=np.float64(sc.dt),
-        gravity=np.asarray(sc.gravity, np.float32),
+        gravity=np.asarray(sc.gravity, np.float32), viscosity=np.float64(viscosity),
         x=np.stack(rec["x"]), v=np.stack(rec["v"]), density=np.stack(rec["density"]), k=np.stack(rec["k"]),
         err=err, err_off=err_off, pcg=pcg, pcg_off=pcg_off, outer=np.array(rec["outer"], np.int32),
         final_err=np.array(rec["final_err"], np.float64), nbr_count=np.stack(rec["cnt"]),
@@ -208,7 +235,10 @@ def main():
     _setup(a.reference)
     jobs = {"kernels": lambda: make_kernels(os.path.join(HERE, "kernels.npz")),
             "block_solve": lambda: make_block_solve(os.path.join(HERE, "block_solve.npz")),
-            "column_steps": lambda: make_column_steps(os.path.join(HERE, "column_steps.npz"), a.steps)}
+            "column_steps": lambda: make_column_steps(os.path.join(HERE, "column_steps.npz"), a.steps),
+            "visc_solve": lambda: make_visc_solve(os.path.join(HERE, "visc_solve.npz")),
+            "column_visc_steps": lambda: make_column_steps(os.path.join(HERE, "column_visc_steps.npz"), 10,
+                                                           viscosity=0.01)}
     for name, job in jobs.items():
         if a.only and name != a.only:
             continue

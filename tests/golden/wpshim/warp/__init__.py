@@ -57,6 +57,38 @@ class _VecType:
         return np.array([f32(a) for a in args], dtype=f32)
 
 
+class Mat(np.ndarray):
+    """Square FP32 matrix value: `M * v` is the matrix-vector product and
+    `M * N` the matrix product (Warp's operator semantics); with a scalar it
+    scales."""
+
+    def _mv(self, v):
+        a = np.asarray(self, dtype=f32)
+        n = a.shape[0]
+        out = np.zeros(n, dtype=f32)
+        for r in range(n):
+            acc = a[r, 0] * v[0]
+            for c in range(1, n):
+                acc = acc + a[r, c] * v[c]
+            out[r] = acc
+        return out
+
+    def __mul__(self, other):
+        o = np.asarray(other)
+        if o.ndim == 1:
+            return self._mv(o.astype(f32))
+        if o.ndim == 2:
+            return np.stack([self._mv(o[:, c].astype(f32)) for c in range(o.shape[1])], axis=1).view(Mat)
+        return np.multiply(np.asarray(self), o).astype(f32).view(Mat)
+
+    def __rmul__(self, other):
+        return np.multiply(np.asarray(other), np.asarray(self)).astype(f32).view(Mat)
+
+
+def _mat(a):
+    return np.asarray(a, dtype=f32).copy().view(Mat)
+
+
 class _MatType:
     def __init__(self, n, name):
         self.n = n
@@ -64,12 +96,12 @@ class _MatType:
 
     def __call__(self, *args):
         if len(args) == 0:
-            return np.zeros((self.n, self.n), dtype=f32)
+            return _mat(np.zeros((self.n, self.n)))
         if len(args) == self.n * self.n:
-            return np.array([f32(a) for a in args], dtype=f32).reshape(self.n, self.n)
+            return _mat(np.array([f32(a) for a in args], dtype=f32).reshape(self.n, self.n))
         if len(args) == self.n:
-            return np.stack([np.asarray(a, dtype=f32) for a in args], axis=1)
-        return np.asarray(args[0], dtype=f32).reshape(self.n, self.n).copy()
+            return _mat(np.stack([np.asarray(a, dtype=f32) for a in args], axis=1))
+        return _mat(np.asarray(args[0], dtype=f32).reshape(self.n, self.n))
 
 
 vec2 = _VecType(2, "vec2")
@@ -124,7 +156,7 @@ class ShimArray:
             return ShimArray(self.data[idx], self.dtype)
         v = self.data[int(idx)]
         if isinstance(v, np.ndarray):
-            return v.copy()
+            return _mat(v) if isinstance(self.dtype, _MatType) else v.copy()
         return v
 
     def __setitem__(self, idx, val):
@@ -312,11 +344,11 @@ def cross(a, b):
 
 
 def outer(a, b):
-    return np.outer(np.asarray(a, dtype=f32), np.asarray(b, dtype=f32)).astype(f32)
+    return _mat(np.outer(np.asarray(a, dtype=f32), np.asarray(b, dtype=f32)))
 
 
 def inverse(m):
-    return np.linalg.inv(np.asarray(m, dtype=np.float64)).astype(f32)
+    return _mat(np.linalg.inv(np.asarray(m, dtype=np.float64)))
 
 
 def determinant(m):

@@ -277,3 +277,68 @@ def test_not_converged_status(small):
     assert s.status == 2
     # the reference raises before v = d / dt, so v is unchanged
     assert np.array_equal(eng.get("v"), v0)
+
+
+# ----------------------------------------------------------- Weiler18 viscosity
+
+def _visc_scene(g, x, v, coeff):
+    sc = _scene_from_golden(g, x, v)
+    sc.viscosity_method = 1
+    sc.viscosity_coeff = float(coeff)
+    return sc
+
+
+def test_viscosity_solve_vs_golden(golden_dir):
+    g = _load(golden_dir, "visc_solve.npz")
+    sc = _visc_scene(g, g["x"], g["v0"], g["coeff"])
+    eng = _engine([sc])
+    eng.build()
+    dyn = sc.is_dynamic == 1
+    np.testing.assert_allclose(eng.get("density")[dyn], g["density"][dyn], rtol=RTOL)
+    eng.viscosity_solve()
+    v = eng.get("v")
+    assert _rel(v[dyn], g["v"][dyn]) < RTOL
+    assert _rel(v[dyn] - g["v0"][dyn], g["dv"][dyn]) < 1e-3
+
+
+@pytest.mark.parametrize("persistent", [True, False])
+def test_column_visc_steps_vs_golden(golden_dir, persistent):
+    g = _load(golden_dir, "column_visc_steps.npz")
+    dyn = g["is_dynamic"] == 1
+    for s in range(g["x"].shape[0]):
+        x_prev = g["x0"] if s == 0 else g["x"][s - 1]
+        v_prev = g["v0"] if s == 0 else g["v"][s - 1]
+        sc = _visc_scene(g, x_prev, v_prev, g["viscosity"])
+        sc.gravity = tuple(float(a) for a in g["gravity"])
+        eng = _engine([sc], persistent=persistent)
+        eng.build()
+        eng.step(1)
+        st = eng.stats(0)
+        assert st.status == 0
+        if st.stats_outer_iters != int(g["outer"][s]):
+            continue
+        assert _rel(eng.get("v")[dyn], g["v"][s][dyn]) < RTOL, s
+        assert np.abs(eng.get("x")[dyn] - g["x"][s][dyn]).max() < 1e-6, s
+
+
+def test_viscous_column_vs_oracle_and_paths():
+    """The tall-column physics (Weiler18 nu = 1e-3) on a smaller column: each
+    step restarted from the oracle's state, and persistent vs per-phase paths
+    bit-identical."""
+    sc = S.column_in_box((12, 24, 12), 0.02, (0.4, 1.0, 0.4), seed=4, viscosity_method=1, viscosity_coeff=1e-3)
+    st = O.State.from_scene(sc)
+    st.rebuild()
+    dyn = sc.is_dynamic == 1
+    for s in range(6):
+        cur = S.Scene(**{**sc.__dict__, "x": st.x.copy(), "v": st.v.copy()})
+        a = _engine([cur], persistent=True)
+        b = _engine([cur], persistent=False)
+        for e in (a, b):
+            e.build()
+            e.step(1)
+        st.step(fast=True)
+        assert np.array_equal(a.get("v"), b.get("v"))
+        ga = a.stats(0)
+        assert ga.status == 0 and st.status == 0
+        if ga.stats_outer_iters == st.stats_outer_iters and ga.stats_pcg_iters == st.stats_pcg_iters:
+            assert _rel(a.get("v")[dyn], st.v[dyn]) < RTOL, s

@@ -185,3 +185,43 @@ def test_fp64_cg_matches_dense_solve():
     x_cg, it = st.cg_f64(dfdt, rhs, rel_tol=1e-14)
     assert it > 0
     np.testing.assert_allclose(x_cg[dyn].ravel(), x_dense, rtol=1e-8, atol=1e-12 * np.abs(x_dense).max())
+
+
+# ----------------------------------------------------------- Weiler18 viscosity
+
+def _visc_state(g, x, v, visc):
+    sc = S.Scene(x=np.array(x, np.float32), v=np.array(v, np.float32), is_dynamic=g["is_dynamic"],
+                 material=g["material"], density0=g["density0"], particle_radius=float(g["particle_radius"]),
+                 domain_size=g["domain_size"], dt=float(g["dt"]), viscosity_method=1, viscosity_coeff=visc)
+    return O.State.from_scene(sc)
+
+
+@pytest.mark.parametrize("fast", [False, True])
+def test_viscosity_solve_golden(golden_dir, fast):
+    g = _load(golden_dir, "visc_solve.npz")
+    st = _visc_state(g, g["x"], g["v0"], float(g["coeff"]))
+    st.rebuild()
+    dyn = st.is_dynamic == 1
+    np.testing.assert_allclose(st.density[dyn], g["density"][dyn], rtol=RTOL)
+    it = st.viscosity_solve(float(g["coeff"]), fast=fast)
+    assert it >= 2
+    assert _rel(st.v[dyn], g["v"][dyn]) < RTOL
+    dv = st.v[dyn] - g["v0"][dyn]
+    assert _rel(dv, g["dv"][dyn]) < 1e-3  # the correction itself, relative to its own size
+
+
+def test_column_visc_steps_one_step_parity(golden_dir):
+    g = _load(golden_dir, "column_visc_steps.npz")
+    dyn = g["is_dynamic"] == 1
+    visc = float(g["viscosity"])
+    for s in range(g["x"].shape[0]):
+        x_prev = g["x0"] if s == 0 else g["x"][s - 1]
+        v_prev = g["v0"] if s == 0 else g["v"][s - 1]
+        st = _visc_state(g, x_prev, v_prev, visc)
+        st.rebuild()
+        st.step(fast=True)
+        assert st.status == O.OK
+        if st.stats_outer_iters != int(g["outer"][s]):
+            continue
+        assert _rel(st.v[dyn], g["v"][s][dyn]) < RTOL, s
+        assert np.abs(st.x[dyn] - g["x"][s][dyn]).max() < 1e-6, s
