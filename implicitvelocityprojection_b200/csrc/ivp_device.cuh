@@ -123,6 +123,8 @@ struct Dev {
     int n_scenes;
     SceneCtl* ctl;
     const int4* tiles;       // (scene, slot begin, slot end, row begin)
+    const int4* segs;        // neighbour-build cell segments (scene, cy, cz, x_lo)
+    int n_segs;
     int n_tiles;
     const int* pscene;       // scene of each particle
     // sort
@@ -243,6 +245,15 @@ __device__ __forceinline__ int cell_coord(float v, float inv, int dim) {
     c = fmaxf(c, 0.0f);                       // NaN -> 0
     c = fminf(c, (float)(dim - 1));
     return (int)c;
+}
+
+// Sum over the G lanes of a group that may have diverged from the rest of
+// the warp (only the group's lanes take part).
+template <int G>
+__device__ __forceinline__ float group_sum_masked(float v, unsigned gmask) {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(gmask, v, o);
+    return v;
 }
 
 template <int G>

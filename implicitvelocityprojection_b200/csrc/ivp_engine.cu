@@ -58,14 +58,14 @@ struct ivp_engine {
     ivp_options opt{};
     Dev D{};
     int G = 4, BLOCK = 128, T = 32;
-    int n_total = 0, n_dyn_total = 0, n_keys = 0, n_tiles = 0, scan_blocks = 0;
+    int n_total = 0, n_dyn_total = 0, n_keys = 0, n_tiles = 0, scan_blocks = 0, n_segs = 0;
     int n_scenes = 0;
     bool bound = false;
     bool want_divergence = false;
     bool any_visc = false;
     // persistent solve
     bool persistent = false;
-    int coop_grid = 0;
+    int coop_grid = 0, coop_grid_visc = 0;
     size_t coop_smem = 0;
     // graphs
     cudaGraph_t graph_step = nullptr, graph_solve = nullptr, graph_build = nullptr;
@@ -185,14 +185,14 @@ struct Kern {
 };
 
 struct KernelSet {
-    DevKernel pack, rhs, cg_a, cg_b, dens, aii, div, persist, v_setup, v_a, v_b, v_end;
+    DevKernel pack, rhs, cg_a, cg_b, dens, aii, div, persist, v_setup, v_a, v_b, v_end, v_persist;
 };
 
 template <int G, int B>
 KernelSet make_set() {
     return {Kern<G, B>::pack(), Kern<G, B>::rhs(), Kern<G, B>::cg_a(), Kern<G, B>::cg_b(),
             Kern<G, B>::dens(), Kern<G, B>::aii(), Kern<G, B>::div(), k_ip_persistent<G, B>,
-            k_visc_setup<G, B>, k_visc_a<G, B>, k_visc_b<G, B>, k_visc_end<G, B>};
+            k_visc_setup<G, B>, k_visc_a<G, B>, k_visc_b<G, B>, k_visc_end<G, B>, k_visc_persistent<G, B>};
 }
 
 // Instantiated launch shapes: G lanes per particle x {128, 256} threads.
@@ -237,12 +237,11 @@ int emit_build(ivp_engine* e, Launcher& L) {
     CKS(L.dev(IVP_K_PLACE, k_place, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D));
     CKS(L.dev(IVP_K_ORDER, k_order, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D));
     {
-        // 8 lanes per particle for the candidate scan (at most 256 threads)
-        DevKernel nb = e->T <= 32 ? (DevKernel)k_nbr_build<8> : e->T <= 64 ? (DevKernel)k_nbr_build<4>
-                                                                             : (DevKernel)k_nbr_build<2>;
-        const int lanes = e->T <= 32 ? 8 : e->T <= 64 ? 4 : 2;
-        if (e->T * lanes > 256) return IVP_ERR_BAD_ARG;
-        CKS(L.dev(IVP_K_NBR_BUILD, nb, e->n_tiles, e->T * lanes, D));
+        // cell-tiled build: one CTA per row segment, 8 lanes per particle
+        Dev copy = D;
+        void* args[] = {&copy};
+        CKS(L.kernel(IVP_K_NBR_BUILD, (const void*)k_nbr_build<8>, dim3(e->n_segs), dim3(256), args,
+                     sizeof(float4) * kStageCap));
     }
     CKS(L.dev(IVP_K_STATIC_OUT, k_static_outputs, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D));
     return IVP_OK;
@@ -384,9 +383,21 @@ int emit_advect(ivp_engine* e, Launcher& L) {
     return L.dev(IVP_K_ADVECT, k_advect, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, e->D);
 }
 
+int emit_visc_persistent(ivp_engine* e, Launcher& L) {
+    if (e->n_tiles == 0 || !e->any_visc) return IVP_OK;
+    KernelSet K;
+    kernel_set(e->G, e->BLOCK, &K);
+    CKS(L.memset0(e->D.bar_count, sizeof(unsigned)));
+    Dev copy = e->D;
+    void* args[] = {&copy};
+    return L.kernel(IVP_K_VISC, (const void*)K.v_persist, dim3(e->coop_grid_visc), dim3(e->BLOCK), args,
+                    e->coop_smem, true);
+}
+
 int emit_step(ivp_engine* e, Launcher& L) {
     CKS(L.dev(IVP_K_GRAVITY, k_gravity, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, e->D));
     if (!e->persistent) CKS(emit_visc(e, L));
+    else CKS(emit_visc_persistent(e, L));
     CKS(emit_solve(e, L, true));
     {
         Dev d = e->D;
@@ -463,6 +474,7 @@ int validate(const ivp_scene_desc* sc, int n, const ivp_options* o) {
 struct Plan {
     std::vector<SceneParams> hp;
     std::vector<int4> tiles;
+    std::vector<int4> segs;
     int n_total = 0, n_dyn = 0, n_keys = 0, scan_blocks = 0;
     size_t off[48];
     Layout lay;
@@ -530,6 +542,10 @@ void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
             P.tiles.push_back(make_int4(s, s_begin + b, s_begin + e, row_base + b));
         }
         q.tile_end = (int)P.tiles.size();
+        if (d.n_dynamic > 0)
+            for (int cz = 0; cz < q.dims[2]; ++cz)
+                for (int cy = 0; cy < q.dims[1]; ++cy)
+                    for (int x = 0; x < q.dims[0]; x += kSegW) P.segs.push_back(make_int4(s, cy, cz, x));
         s_begin += d.n_particles;
         row_base += d.n_dynamic;
         key_base += 2 * (int)ncell;
@@ -586,6 +602,7 @@ void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
     P.off[i++] = L.add(sizeof(float4) * N);                          // 42 vz
     P.off[i++] = L.add(sizeof(float4) * N);                          // 43 vap
     P.off[i++] = L.add(3 * sizeof(float4) * N);                      // 44 pinv
+    P.off[i++] = L.add(sizeof(int4) * std::max<size_t>(P.segs.size(), 1));  // 45 segs
 }
 
 cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
@@ -690,6 +707,9 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
     D.vz = reinterpret_cast<float4*>(w + P.off[i++]);
     D.vap = reinterpret_cast<float4*>(w + P.off[i++]);
     D.pinv = reinterpret_cast<float4*>(w + P.off[i++]);
+    D.segs = reinterpret_cast<int4*>(w + P.off[i++]);
+    D.n_segs = (int)P.segs.size();
+    e->n_segs = D.n_segs;
     {
         long long lim = 64;
         for (int sc = 0; sc < n_scenes; ++sc)
@@ -725,7 +745,9 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
         (e->n_tiles && cudaMemcpyAsync((void*)D.tiles, P.tiles.data(), sizeof(int4) * e->n_tiles,
                                        cudaMemcpyHostToDevice, s) != cudaSuccess) ||
         (e->n_total && cudaMemcpyAsync((void*)D.pscene, pscene.data(), sizeof(int) * e->n_total,
-                                       cudaMemcpyHostToDevice, s) != cudaSuccess))
+                                       cudaMemcpyHostToDevice, s) != cudaSuccess) ||
+        (e->n_segs && cudaMemcpyAsync((void*)D.segs, P.segs.data(), sizeof(int4) * e->n_segs,
+                                      cudaMemcpyHostToDevice, s) != cudaSuccess))
         return fail(IVP_ERR_CUDA);
     // the host vectors go out of scope: make the copies complete first
     if (cudaStreamSynchronize(s) != cudaSuccess) return fail(IVP_ERR_CUDA);
@@ -742,8 +764,14 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)K.persist, e->BLOCK, e->coop_smem) ==
                 cudaSuccess &&
             per_sm > 0) {
-            e->coop_grid = std::min(e->n_tiles, per_sm * nsm);
-            e->persistent = true;
+            int per_sm_v = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_v, (const void*)K.v_persist, e->BLOCK,
+                                                              e->coop_smem) == cudaSuccess &&
+                per_sm_v > 0) {
+                e->coop_grid = std::min(e->n_tiles, per_sm * nsm);
+                e->coop_grid_visc = std::min(e->n_tiles, per_sm_v * nsm);
+                e->persistent = true;
+            }
         }
     }
     *out = e;

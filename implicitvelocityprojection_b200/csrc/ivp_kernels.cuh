@@ -134,13 +134,28 @@ __device__ void scene_finalize(const Dev& D, int sc, int kind, double s) {
     scene_decide(D, D.scenes[sc], D.ctl[sc], kind, s, true);
 }
 
-// A scene's sum of its tile partials, one fixed association for every path:
-// lane l of one warp adds tiles tb+l, tb+l+32, ... in order, then an xor tree
-// (valid in every lane).
+// A scene's sum of its tile partials, one fixed association for every path
+// (it depends only on the scene's tile count): lane l of one warp keeps 8
+// accumulators, a[m] collecting tiles tb + l + 32 (8 r + m), loaded 8 at a
+// time so the loads are in flight together; then a fixed pairwise combine and
+// an xor tree (valid in every lane).
 __device__ __forceinline__ double scene_sum_warp(const double* partial, int tb, int te) {
     const int l = threadIdx.x & 31;
-    double s = 0.0;
-    for (int t = tb + l; t < te; t += 32) s += __ldcg(partial + t);
+    double a[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) a[m] = 0.0;
+    int t = tb + l;
+    for (; t + 7 * 32 < te; t += 8 * 32) {
+        double v[8];
+#pragma unroll
+        for (int m = 0; m < 8; ++m) v[m] = __ldcg(partial + t + 32 * m);
+#pragma unroll
+        for (int m = 0; m < 8; ++m) a[m] += v[m];
+    }
+#pragma unroll
+    for (int m = 0; m < 8; ++m)
+        if (t + 32 * m < te) a[m] += __ldcg(partial + t + 32 * m);
+    const double s = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
     return warp_sum_d(s);
 }
 
@@ -377,135 +392,182 @@ __global__ void k_order(const Dev D) {
 // diagonal k = 1/(Aii + 1e-3) (pressure_base.py:49-87) and the constraint
 // c = rho - rho0 (pressure_base.py:169-184).
 //
-// G lanes share one particle: the 3 x-adjacent cells of each (y, z) row are
-// one contiguous slot range, which the group walks G candidates at a time
-// (coalesced float4 loads).  A group ballot orders the hits of each round by
-// slot, so the list keeps the exact sequential candidate order (rows dz, dy
-// ascending; dynamic cells before static cells; slots ascending) and the
-// first-cache_size truncation of the sequential scan.
+// Cell-tiled: one CTA per segment of kSegW cells along x of one (y, z) cell
+// row.  The CTA stages the candidates of the 9 neighbouring rows x {dynamic,
+// static} -- 18 contiguous slot ranges covering x_lo-1 .. x_hi+1 -- into
+// shared memory with coalesced loads, together with their cell starts; then
+// G lanes per particle test the particle's own candidate ranges from shared
+// memory.  A group ballot orders the hits of each round by slot, so each list
+// keeps the sequential candidate order (rows dz, dy ascending; dynamic cells
+// before static cells; slots ascending) and the first-cache_size truncation
+// of the sequential scan.  Segments whose neighbourhood exceeds the staging
+// capacity read the candidates from global memory instead.
+constexpr int kSegW = 8;
+constexpr int kStageCap = 2048;  // staged candidates per CTA (32 KB of float4)
+
 template <int G>
 __global__ void __launch_bounds__(256, 4) k_nbr_build(const Dev D) {
-    constexpr int NG = 256 / G;  // groups (particles) per CTA at most
-    __shared__ int2 sh_rng[NG][18];
-    __shared__ int sh_pairs;
-    const int4 tile = D.tiles[blockIdx.x];
-    const int g = threadIdx.x / G, lane = threadIdx.x % G;
-    const int i = tile.y + g;
-    const bool valid = i < tile.z;
-    const int sc = tile.x;
+    constexpr int NG = 256 / G;
+    constexpr int NC = kSegW + 3;  // cell starts x_lo-1 .. x_hi+2
+    constexpr int HB = 64;         // hit buffer per particle (>= list stride is not required: capped at cap)
+    extern __shared__ float4 stage[];
+    __shared__ int sh_cs[18][NC];
+    __shared__ int sh_off[18], sh_base[18];
+    __shared__ int sh_total, sh_pairs;
+    __shared__ int hit_j[NG][HB];
+    __shared__ short hit_q[NG][HB];
+    const int4 seg = D.segs[blockIdx.x];  // (scene, cy, cz, x_lo)
+    const int sc = seg.x, cy = seg.y, cz = seg.z, x_lo = seg.w;
     const SceneParams& P = D.scenes[sc];
+    const int dimx = P.dims[0];
+    const int x_hi = min(x_lo + kSegW, dimx) - 1;
+    const int kd0 = P.key_base + (cz * P.dims[1] + cy) * dimx;
+    const int s0 = __ldg(D.cell_start + kd0 + x_lo), s1 = __ldg(D.cell_start + kd0 + x_hi + 1);
+    if (s0 == s1) return;  // no dynamic particle in this segment (block-uniform)
+    // cell starts of the 18 neighbour ranges (column c <-> x = x_lo - 1 + c)
+    for (int e = threadIdx.x; e < 18 * NC; e += blockDim.x) {
+        const int q = e / NC, c = e % NC;
+        const int rr = q >> 1, pass = q & 1;
+        const int z = cz + rr / 3 - 1, y = cy + rr % 3 - 1;
+        const int x = x_lo - 1 + c;
+        int v = -1;
+        if (z >= 0 && z < P.dims[2] && y >= 0 && y < P.dims[1] && x >= 0 && x <= dimx)
+            v = __ldg(D.cell_start + P.key_base + (pass ? P.ncell : 0) + (z * P.dims[1] + y) * dimx + x);
+        sh_cs[q][c] = v;
+    }
+    if (threadIdx.x == 0) sh_pairs = 0;
+    __syncthreads();
+    const int ca = (x_lo > 0 ? x_lo - 1 : 0) - (x_lo - 1);                    // first staged column
+    const int cb = (x_hi < dimx - 1 ? x_hi + 1 : dimx - 1) + 1 - (x_lo - 1);  // one past the last
+    if (threadIdx.x < 32) {
+        // prefix of the 18 range lengths (one warp)
+        const int q = threadIdx.x;
+        int len = 0, b = 0;
+        if (q < 18) {
+            b = sh_cs[q][ca];
+            const int e = sh_cs[q][cb];
+            len = (b >= 0 && e >= b) ? e - b : 0;
+        }
+        int incl = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (q >= o) incl += t;
+        }
+        if (q < 18) {
+            sh_off[q] = incl - len;
+            sh_base[q] = b;
+        }
+        if (q == 31) sh_total = incl;
+    }
+    __syncthreads();
+    const bool staged = sh_total <= kStageCap;
+    if (staged) {
+        // one flat pass over the staged candidates: every thread's loads are
+        // independent (issued together), not one range after another
+        const int total = sh_total;
+#pragma unroll 4
+        for (int k = threadIdx.x; k < total; k += blockDim.x) {
+            int q = 0;
+#pragma unroll
+            for (int t = 1; t < 18; ++t) q += (k >= sh_off[t]) ? 1 : 0;
+            stage[k] = __ldg(D.xm + sh_base[q] + (k - sh_off[q]));
+        }
+    }
+    __syncthreads();
+    const int g = threadIdx.x / G, lane = threadIdx.x % G;
     const int wl = threadIdx.x & 31;
     const int gshift = wl & ~(G - 1);
     const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << gshift;
     const unsigned below = (1u << lane) - 1u;
-    if (threadIdx.x == 0) sh_pairs = 0;
-    float3 xi = make_float3(0.f, 0.f, 0.f);
-    float mi = 1.0f;
-    int cx = 0, cy = 0, cz = 0;
-    if (valid) {
-        const float4 xi4 = D.xm[i];
-        xi = f3(xi4);
-        mi = xi4.w;
-        cx = cell_coord(xi.x, P.cell_inv, P.dims[0]);
-        cy = cell_coord(xi.y, P.cell_inv, P.dims[1]);
-        cz = cell_coord(xi.z, P.cell_inv, P.dims[2]);
-    }
-    // the 9 (dy, dz) rows x {dynamic, static} slot ranges, loaded together
-    {
-        const int x0 = cx > 0 ? cx - 1 : 0;
-        const int x1 = cx < P.dims[0] - 1 ? cx + 1 : P.dims[0] - 1;
-        for (int q = lane; q < 18; q += G) {
-            const int rr = q >> 1, pass = q & 1;
-            const int z = cz + rr / 3 - 1, yy = cy + rr % 3 - 1;
-            int2 rg = make_int2(0, 0);
-            if (valid && z >= 0 && z < P.dims[2] && yy >= 0 && yy < P.dims[1]) {
-                const int kb = P.key_base + (pass ? P.ncell : 0) + (z * P.dims[1] + yy) * P.dims[0];
-                rg = make_int2(__ldg(D.cell_start + kb + x0), __ldg(D.cell_start + kb + x1 + 1));
-            }
-            sh_rng[g][q] = rg;
-        }
-    }
-    __syncthreads();
     const float h = P.h, inv_h = P.inv_h, r2max = P.r2_max, spk = P.spiky_k, ck = P.cubic_k;
     const int dyn_end = P.s_dyn_end;
-    const int row = tile.w + g;
-    float4* out = D.nbr + (size_t)row * D.stride;
-    const int cap = P.cache < D.stride ? P.cache : D.stride;
-    float rho = 0.0f, aii = 0.0f;
-    float3 jii = make_float3(0.0f, 0.0f, 0.0f);
-    int cnt = 0, found = 0;
-    // candidate j: test, then (in slot order, via the group ballot) store
-    auto visit = [&](int j, int je) {
-        bool hit = false;
-        float4 xj4 = make_float4(0.f, 0.f, 0.f, 0.f);
-        float3 r = make_float3(0.f, 0.f, 0.f);
-        float d2 = 0.0f;
-        if (j < je && j != i) {
-            xj4 = __ldg(D.xm + j);
-            r = sub3(xi, f3(xj4));
-            d2 = norm2_rn(r);
-            hit = d2 <= r2max;
+    const int cap = min(min(P.cache, D.stride), HB);
+    int my_pairs = 0;
+    for (int i = s0 + g; i < s1; i += NG) {
+        const float4 xi4 = D.xm[i];
+        const float3 xi = f3(xi4);
+        const float mi = xi4.w;
+        const int cx = cell_coord(xi.x, P.cell_inv, dimx);
+        const int c0 = (cx > 0 ? cx - 1 : 0) - (x_lo - 1);
+        const int c1 = (cx < dimx - 1 ? cx + 1 : dimx - 1) + 1 - (x_lo - 1);
+        // phase 1: filter -- the ordered hit indices of the first `cap` neighbours
+        int cnt = 0, found = 0;
+#pragma unroll 1
+        for (int q = 0; q < 18; ++q) {
+            const int jb = sh_cs[q][c0], je = sh_cs[q][c1];
+            if (jb < 0) continue;
+            const int sb = sh_base[q], so = sh_off[q];
+            for (int base = jb; base < je; base += G) {
+                const int j = base + lane;
+                bool hit = false;
+                if (j < je && j != i) {
+                    const float4 xj4 = staged ? stage[so + (j - sb)] : __ldg(D.xm + j);
+                    hit = norm2_rn(sub3(xi, f3(xj4))) <= r2max;
+                }
+                const unsigned ball = (__ballot_sync(gmask, hit) >> gshift);
+                const int pos = cnt + __popc(ball & below);
+                if (hit && pos < cap) {
+                    hit_j[g][pos] = j;
+                    hit_q[g][pos] = (short)q;
+                }
+                const int nh = __popc(ball);
+                found += nh;
+                cnt = min(cnt + nh, cap);
+            }
         }
-        const unsigned ball = (__ballot_sync(gmask, hit) >> gshift);
-        const int pos = cnt + __popc(ball & below);
-        if (hit && pos < cap) {
+        __syncwarp(gmask);
+        // phase 2: dense over the hits -- J_ij = m_j grad W_ij, density, Aii
+        const int row = P.row_base + (i - P.s_begin);
+        float4* out = D.nbr + (size_t)row * D.stride;
+        float rho = 0.0f, aii = 0.0f;
+        float3 jii = make_float3(0.0f, 0.0f, 0.0f);
+        for (int k = lane; k < cnt; k += G) {
+            const int j = hit_j[g][k];
+            const int q = hit_q[g][k];
+            const float4 xj4 = staged ? stage[sh_off[q] + (j - sh_base[q])] : __ldg(D.xm + j);
+            const float3 r = sub3(xi, f3(xj4));
             // spiky gradient (sph_kernel.py:52-61): -k (h - |r|)^2 r / |r|
-            const float rn = sqrtf(d2);
+            const float rn = sqrtf(norm2_rn(r));
             const float rc = rn < 1e-6f ? 1e-6f : rn;
             const float t = h - rc;
             const float sg = -spk * (t * t);
             const float ir = __frcp_rn(rc);
             const float mj = xj4.w;
             const float3 J = make_float3(mj * (sg * (r.x * ir)), mj * (sg * (r.y * ir)), mj * (sg * (r.z * ir)));
-            out[pos] = make_float4(J.x, J.y, J.z, __int_as_float(j));
+            out[k] = make_float4(J.x, J.y, J.z, __int_as_float(j));
             rho += mj * cubic_Wq(rn * inv_h, ck);
             if (j < dyn_end) aii += dot3(J, J) * __frcp_rn(mj);
             jii = sub3(jii, J);
         }
-        const int nh = __popc(ball);
-        found += nh;
-        cnt = min(cnt + nh, cap);
-    };
-    if (valid) {
-#pragma unroll 1
-        for (int q = 0; q < 18; ++q) {
-            const int2 rg = sh_rng[g][q];
-            const int jb = rg.x, je = rg.y;
-            int base = jb;
-            // two candidate rounds per iteration keep two loads in flight
-            for (; base + G < je; base += 2 * G) {
-                visit(base + lane, je);
-                visit(base + G + lane, je);
-            }
-            if (base < je) visit(base + lane, je);
+        rho = group_sum_masked<G>(rho, gmask);
+        aii = group_sum_masked<G>(aii, gmask);
+        jii.x = group_sum_masked<G>(jii.x, gmask);
+        jii.y = group_sum_masked<G>(jii.y, gmask);
+        jii.z = group_sum_masked<G>(jii.z, gmask);
+        if (lane == 0) {
+            float dens = 0.0f;
+            dens = dens + mi * P.W0;
+            dens += rho;
+            aii += dot3(jii, jii) * __frcp_rn(mi);
+            const float kd = __frcp_rn(aii + 1e-3f);
+            D.nbr_cnt[row] = cnt;
+            D.dens[i] = dens;
+            D.kd[i] = kd;
+            D.c[i] = dens - D.rho0s[i];
+            const int p = D.pid[i];
+            D.rflu[i] = D.material[p] == 1 ? __frcp_rn(dens) : 0.0f;
+            D.density_out[p] = dens;
+            D.k_out[p] = kd;
+            if (found > cap) atomicAdd(&D.overflow[sc], 1);
+            my_pairs += cnt;
         }
+        __syncwarp(gmask);
     }
-    rho = group_sum<G>(rho);
-    aii = group_sum<G>(aii);
-    jii.x = group_sum<G>(jii.x);
-    jii.y = group_sum<G>(jii.y);
-    jii.z = group_sum<G>(jii.z);
-    if (valid && lane == 0) {
-        float dens = 0.0f;
-        dens = dens + mi * P.W0;
-        dens += rho;
-        aii += dot3(jii, jii) * __frcp_rn(mi);
-        const float kd = __frcp_rn(aii + 1e-3f);
-        D.nbr_cnt[row] = cnt;
-        D.dens[i] = dens;
-        D.kd[i] = kd;
-        D.c[i] = dens - D.rho0s[i];
-        const int p = D.pid[i];
-        D.rflu[i] = D.material[p] == 1 ? __frcp_rn(dens) : 0.0f;
-        D.density_out[p] = dens;
-        D.k_out[p] = kd;
-        if (found > cap) atomicAdd(&D.overflow[sc], 1);
-    }
-    // one pair-count atomic per CTA (every tile belongs to one scene)
-    int c = (valid && lane == 0) ? cnt : 0;
+    // one pair-count atomic per CTA
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-    if ((threadIdx.x & 31) == 0 && c) atomicAdd(&sh_pairs, c);
+    for (int o = 16; o > 0; o >>= 1) my_pairs += __shfl_xor_sync(0xffffffffu, my_pairs, o);
+    if (wl == 0 && my_pairs) atomicAdd(&sh_pairs, my_pairs);
     __syncthreads();
     if (threadIdx.x == 0 && sh_pairs) atomicAdd(&D.pairs[sc], (unsigned long long)sh_pairs);
 }
@@ -1384,49 +1446,68 @@ __device__ bool grid_reduce_barrier(const Dev& D, int kind, int* sh_flag, double
     return sh_flag[1] != 0;
 }
 
+// Phase driver shared by the persistent kernels: per-CTA tile range, local
+// copies of the control blocks, one grid barrier + reduction per phase.
 template <int G, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_ip_persistent(const Dev D) {
-    extern __shared__ double dyn_sh[];
-    double* sum_sh = dyn_sh;                                                 // [n_scenes]
-    double* sum_sh2 = dyn_sh + D.n_scenes;                                   // [n_scenes]
-    SceneCtl* sc_sh = reinterpret_cast<SceneCtl*>(dyn_sh + 2 * D.n_scenes);  // [n_scenes]
-    __shared__ double red_sh[32];
-    __shared__ int flag_sh[2], any_sh;
-    const int t0 = (int)(((long long)blockIdx.x * D.n_tiles) / gridDim.x);
-    const int t1 = (int)(((long long)(blockIdx.x + 1) * D.n_tiles) / gridDim.x);
-    // CTA 0 starts every scene's control block (reset_stats); the first
-    // barrier publishes it
-    if (blockIdx.x == 0 && threadIdx.x == 0)
-        for (int s = 0; s < D.n_scenes; ++s) {
-            const SceneParams& P = D.scenes[s];
-            ctl_begin(P, D.ctl[s]);
-            D.ctl[s].v_on = (D.visc_enabled && visc_on(P) && P.n_dyn > 0) ? 1 : 0;
-            D.ctl[s].v_active = 0;
-            D.ctl[s].v_total = 0;
-        }
-    if (!grid_reduce_barrier(D, -1, flag_sh, sum_sh, sum_sh2)) return;
-    // local copies of the control blocks, refreshed after every phase
-    auto refresh = [&]() {
+struct Phaser {
+    const Dev& D;
+    int t0, t1;
+    double* sum_sh;
+    double* sum_sh2;
+    SceneCtl* sc_sh;
+    double* red_sh;
+    int* flag_sh;
+    int* any_sh;
+    long long phases;
+
+    __device__ Phaser(const Dev& d, double* dyn, double* red, int* flag, int* anyp)
+        : D(d), red_sh(red), flag_sh(flag), any_sh(anyp), phases(0) {
+        t0 = (int)(((long long)blockIdx.x * D.n_tiles) / gridDim.x);
+        t1 = (int)(((long long)(blockIdx.x + 1) * D.n_tiles) / gridDim.x);
+        sum_sh = dyn;
+        sum_sh2 = dyn + D.n_scenes;
+        sc_sh = reinterpret_cast<SceneCtl*>(dyn + 2 * D.n_scenes);
+    }
+
+    __device__ bool barrier(int kind) { return grid_reduce_barrier(D, kind, flag_sh, sum_sh, sum_sh2); }
+
+    __device__ void refresh() {
         for (int s = threadIdx.x; s < D.n_scenes; s += BLOCK) sc_sh[s] = ctl_load(D.ctl + s);
         __syncthreads();
-    };
-    refresh();
-    long long phases = 0;
-    const long long limit = D.phase_limit;
-    auto run_phase = [&](int kind) -> bool {
+    }
+
+    __device__ bool any(int kind) {
+        if (threadIdx.x == 0) {
+            int a = 0;
+            for (int s = 0; s < D.n_scenes; ++s) a |= phase_active(sc_sh[s], kind) ? 1 : 0;
+            *any_sh = a;
+        }
+        __syncthreads();
+        const bool r = *any_sh != 0;
+        __syncthreads();
+        return r;
+    }
+
+    // VISC selects the phase family compiled into this kernel (each
+    // persistent kernel keeps its own register budget)
+    template <bool VISC>
+    __device__ bool run(int kind) {
         for (int t = t0; t < t1; ++t) {
             const TileCtx T = tile_ctx<G>(D, t);
             const SceneCtl& C = sc_sh[T.sc];
             if (!phase_active(C, kind)) continue;
             const SceneParams& P = D.scenes[T.sc];
             double part, part2 = 0.0;
-            if (kind == K_PACK) part = pack_tile<G>(D, P, T, C.outer_it);
-            else if (kind == K_RHS) part = rhs_tile<G>(D, P, T);
-            else if (kind == K_CG_A) part = cga_tile<G>(D, P, T, (float)C.beta, C.cg_it);
-            else if (kind == K_CG_B) part = cgb_tile<G>(D, P, T, (float)C.alpha, C.cg_it);
-            else if (kind == K_V_SETUP) part = visc_setup_tile<G>(D, P, T);
-            else if (kind == K_V_A) part = visc_a_tile<G>(D, P, T, (float)C.v_beta, C.v_it);
-            else visc_b_tile<G>(D, T, (float)C.v_alpha, C.v_it, &part, &part2);
+            if constexpr (VISC) {
+                if (kind == K_V_SETUP) part = visc_setup_tile<G>(D, P, T);
+                else if (kind == K_V_A) part = visc_a_tile<G>(D, P, T, (float)C.v_beta, C.v_it);
+                else visc_b_tile<G>(D, T, (float)C.v_alpha, C.v_it, &part, &part2);
+            } else {
+                if (kind == K_PACK) part = pack_tile<G>(D, P, T, C.outer_it);
+                else if (kind == K_RHS) part = rhs_tile<G>(D, P, T);
+                else if (kind == K_CG_A) part = cga_tile<G>(D, P, T, (float)C.beta, C.cg_it);
+                else part = cgb_tile<G>(D, P, T, (float)C.alpha, C.cg_it);
+            }
             const double tot = block_sum_d<BLOCK>(part, red_sh);
             const double tot2 = kind == K_V_B ? block_sum_d<BLOCK>(part2, red_sh) : 0.0;
             if (threadIdx.x == 0) {
@@ -1434,8 +1515,8 @@ __global__ void __launch_bounds__(BLOCK) k_ip_persistent(const Dev D) {
                 D.partial[D.n_tiles + t] = tot2;
             }
         }
-        if (!grid_reduce_barrier(D, kind, flag_sh, sum_sh, sum_sh2)) return false;
-        if (++phases > limit) {
+        if (!barrier(kind)) return false;
+        if (++phases > D.phase_limit) {
             // guard: every CTA reaches the same count; CTA 0 stops the scenes,
             // a barrier publishes it
             if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -1449,37 +1530,58 @@ __global__ void __launch_bounds__(BLOCK) k_ip_persistent(const Dev D) {
                 }
                 D.flags->timeout = 1;
             }
-            if (!grid_reduce_barrier(D, -1, flag_sh, sum_sh, sum_sh2)) return false;
+            if (!barrier(-1)) return false;
         }
         refresh();
         return true;
-    };
-    auto any = [&](int kind) -> bool {
-        if (threadIdx.x == 0) {
-            int a = 0;
-            for (int s = 0; s < D.n_scenes; ++s) a |= phase_active(sc_sh[s], kind) ? 1 : 0;
-            any_sh = a;
-        }
-        __syncthreads();
-        const bool r = any_sh != 0;
-        __syncthreads();
-        return r;
-    };
-    // implicit viscosity (framework.py:421), then v -> d (ip.py:343)
-    if (any(K_V_SETUP)) {
-        if (!run_phase(K_V_SETUP)) return;
-        while (any(K_V_A)) {
-            if (!run_phase(K_V_A)) return;
-            if (!any(K_V_B)) break;
-            if (!run_phase(K_V_B)) return;
-        }
-        for (int t = t0; t < t1; ++t) {
-            const TileCtx T = tile_ctx<G>(D, t);
-            if (sc_sh[T.sc].v_on) visc_end_tile(D, T);
-        }
-        __syncthreads();
     }
-    for (int t = t0; t < t1; ++t) {
+};
+
+// Weiler 2018 implicit viscosity of every scene that enables it, in one
+// persistent cooperative launch (weiler18.py:371-401).
+template <int G, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_visc_persistent(const Dev D) {
+    extern __shared__ double dyn_sh[];
+    __shared__ double red_sh[32];
+    __shared__ int flag_sh[2], any_sh;
+    Phaser<G, BLOCK> ph(D, dyn_sh, red_sh, flag_sh, &any_sh);
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        for (int s = 0; s < D.n_scenes; ++s) {
+            const SceneParams& P = D.scenes[s];
+            SceneCtl c = ctl_load(D.ctl + s);
+            c.v_on = (visc_on(P) && P.n_dyn > 0) ? 1 : 0;
+            c.v_active = 0;
+            c.v_total = 0;
+            D.ctl[s] = c;
+        }
+    if (!ph.barrier(-1)) return;
+    ph.refresh();
+    if (!ph.any(K_V_SETUP)) return;
+    if (!ph.template run<true>(K_V_SETUP)) return;
+    while (ph.any(K_V_A)) {
+        if (!ph.template run<true>(K_V_A)) return;
+        if (!ph.any(K_V_B)) break;
+        if (!ph.template run<true>(K_V_B)) return;
+    }
+    for (int t = ph.t0; t < ph.t1; ++t) {
+        const TileCtx T = tile_ctx<G>(D, t);
+        if (ph.sc_sh[T.sc].v_on) visc_end_tile(D, T);
+    }
+}
+
+// The whole IP.solve of every scene in one persistent cooperative launch.
+template <int G, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_ip_persistent(const Dev D) {
+    extern __shared__ double dyn_sh[];
+    __shared__ double red_sh[32];
+    __shared__ int flag_sh[2], any_sh;
+    Phaser<G, BLOCK> ph(D, dyn_sh, red_sh, flag_sh, &any_sh);
+    // CTA 0 starts every scene's control block (reset_stats); the first
+    // barrier publishes it
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        for (int s = 0; s < D.n_scenes; ++s) ctl_begin(D.scenes[s], D.ctl[s]);
+    // d = dt v (ip.py:343) for the owned particles
+    for (int t = ph.t0; t < ph.t1; ++t) {
         const int4 tile = __ldg(D.tiles + t);
         const SceneParams& P = D.scenes[tile.x];
         for (int i = tile.y + threadIdx.x; i < tile.z; i += BLOCK) {
@@ -1488,22 +1590,23 @@ __global__ void __launch_bounds__(BLOCK) k_ip_persistent(const Dev D) {
             D.d0[i] = make_float4(dt * D.v[3 * p], dt * D.v[3 * p + 1], dt * D.v[3 * p + 2], 0.0f);
         }
     }
-    if (!grid_reduce_barrier(D, -1, flag_sh, sum_sh, sum_sh2)) return;
-    while (any(K_PACK)) {
-        if (!run_phase(K_PACK)) return;
-        if (!any(K_RHS)) break;
-        if (!run_phase(K_RHS)) return;
-        while (any(K_CG_A)) {
-            if (!run_phase(K_CG_A)) return;
-            if (!any(K_CG_B)) break;
-            if (!run_phase(K_CG_B)) return;
+    if (!ph.barrier(-1)) return;
+    ph.refresh();
+    while (ph.any(K_PACK)) {
+        if (!ph.template run<false>(K_PACK)) return;
+        if (!ph.any(K_RHS)) break;
+        if (!ph.template run<false>(K_RHS)) return;
+        while (ph.any(K_CG_A)) {
+            if (!ph.template run<false>(K_CG_A)) return;
+            if (!ph.any(K_CG_B)) break;
+            if (!ph.template run<false>(K_CG_B)) return;
         }
     }
     // epilogue (ip.py:394-404): v = d/dt for scenes that did not raise,
     // divergence, statistics
-    for (int t = t0; t < t1; ++t) {
+    for (int t = ph.t0; t < ph.t1; ++t) {
         const TileCtx T = tile_ctx<G>(D, t);
-        const SceneCtl& C = sc_sh[T.sc];
+        const SceneCtl& C = ph.sc_sh[T.sc];
         const SceneParams& P = D.scenes[T.sc];
         if (C.status == IVP_OK_ && T.lane == 0 && T.valid) {
             const float4 d = (C.outer_it & 1) ? D.d1[T.i] : D.d0[T.i];
@@ -1521,7 +1624,7 @@ __global__ void __launch_bounds__(BLOCK) k_ip_persistent(const Dev D) {
             c.acc_solves += 1;
             c.acc_outer += c.outer_it;
             c.acc_cg += c.total_cg;
-            c.acc_visc += c.v_on ? c.v_total : 0;
+            c.acc_visc += (D.visc_enabled && c.v_on) ? c.v_total : 0;
             if (c.final_err > c.acc_max_final_err) c.acc_max_final_err = c.final_err;
             if (c.status != IVP_OK_) {
                 c.acc_failed += 1;
