@@ -219,7 +219,7 @@ def run_ours(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     sc = make_scene(args.workload)
     opts = EngineOptions(lanes_per_particle=args.lanes,
-                         particles_per_block=args.ppb or 128 // args.lanes, persistent=not args.per_phase)
+                         particles_per_block=args.ppb or 256 // args.lanes, persistent=not args.per_phase)
     eng = Engine([sc], device=str(dev), options=opts, divergence=True)
     eng.build()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
@@ -357,7 +357,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="tall_column")
     ap.add_argument("--lanes", type=int, default=4)
-    ap.add_argument("--ppb", type=int, default=0, help="particles per CTA (default 128 / lanes)")
+    ap.add_argument("--ppb", type=int, default=0, help="particles per CTA (default 256 / lanes)")
     ap.add_argument("--per-phase", action="store_true", help="one launch per solver phase instead of the "
                     "persistent cooperative solve")
     ap.add_argument("--e2e-steps", type=int, default=20)

@@ -616,7 +616,7 @@ extern "C" {
 void ivp_default_options(ivp_options* o) {
     memset(o, 0, sizeof(*o));
     o->lanes_per_particle = 4;
-    o->particles_per_block = 32;
+    o->particles_per_block = 64;
     o->list_stride = 64;
     o->max_hist = kMaxHistDefault;
     o->use_graphs = 1;

@@ -134,29 +134,70 @@ __device__ void scene_finalize(const Dev& D, int sc, int kind, double s) {
     scene_decide(D, D.scenes[sc], D.ctl[sc], kind, s, true);
 }
 
-// A scene's sum of its tile partials, one fixed association for every path
-// (it depends only on the scene's tile count): lane l of one warp keeps 8
-// accumulators, a[m] collecting tiles tb + l + 32 (8 r + m), loaded 8 at a
-// time so the loads are in flight together; then a fixed pairwise combine and
-// an xor tree (valid in every lane).
-__device__ __forceinline__ double scene_sum_warp(const double* partial, int tb, int te) {
-    const int l = threadIdx.x & 31;
-    double a[8];
+// A scene's sum of its tile partials, with one fixed association that depends
+// only on the scene's tile count: 128 logical lanes, lane L adding tiles
+// L, L+128, L+256, ... in order onto 0.0, then the tree v[L] += v[L + off] for
+// off = 64, 32, 16, ..., 1.  scene_sum_block runs the lanes on four warps of
+// a CTA, scene_sum_warp on one warp (logical lanes l, l+32, l+64, l+96 in lane
+// l); both execute the same floating-point operations, so every path and every
+// batch composition produce the same bits.  Out-of-range slots add +0.0, which
+// leaves a sum started at +0.0 unchanged.
+constexpr int kSumChunk = 16;
+
+__device__ __forceinline__ double lane_sum128(const double* __restrict__ p, int t, int te) {
+    double s = 0.0;
+    for (; t < te; t += kSumChunk * 128) {
+        double v[kSumChunk];
 #pragma unroll
-    for (int m = 0; m < 8; ++m) a[m] = 0.0;
-    int t = tb + l;
-    for (; t + 7 * 32 < te; t += 8 * 32) {
-        double v[8];
+        for (int m = 0; m < kSumChunk; ++m) v[m] = t + 128 * m < te ? __ldcg(p + t + 128 * m) : 0.0;
 #pragma unroll
-        for (int m = 0; m < 8; ++m) v[m] = __ldcg(partial + t + 32 * m);
-#pragma unroll
-        for (int m = 0; m < 8; ++m) a[m] += v[m];
+        for (int m = 0; m < kSumChunk; ++m) s += v[m];
     }
+    return s;
+}
+
+// Tail of the tree for lanes 0..31 holding v[L] + v[L + 32] (after off = 64
+// and 32): shuffle-down steps 16..1, result in lane 0, broadcast.
+__device__ __forceinline__ double tree32(double v) {
 #pragma unroll
-    for (int m = 0; m < 8; ++m)
-        if (t + 32 * m < te) a[m] += __ldcg(partial + t + 32 * m);
-    const double s = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
-    return warp_sum_d(s);
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return __shfl_sync(0xffffffffu, v, 0);
+}
+
+__device__ __forceinline__ double scene_sum_warp(const double* __restrict__ partial, int tb, int te) {
+    const int l = threadIdx.x & 31;
+    // a[k] is logical lane l + 32 k; its q-th tile is tb + l + 32 (k + 4 q)
+    double a[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int t = tb + l; t < te; t += kSumChunk * 32) {
+        double v[kSumChunk];
+#pragma unroll
+        for (int m = 0; m < kSumChunk; ++m) v[m] = t + 32 * m < te ? __ldcg(partial + t + 32 * m) : 0.0;
+#pragma unroll
+        for (int m = 0; m < kSumChunk; ++m) a[m & 3] += v[m];
+    }
+    return tree32((a[0] + a[2]) + (a[1] + a[3]));
+}
+
+// All threads of the CTA call it (BLOCK >= 128); `sh` holds 128 doubles.
+// Result valid in every thread.
+template <int BLOCK>
+__device__ __forceinline__ double scene_sum_block(const double* __restrict__ partial, int tb, int te, double* sh) {
+    static_assert(BLOCK >= 128, "scene_sum_block needs four warps");
+    const int t = threadIdx.x;
+    __syncthreads();
+    if (t < 128) sh[t] = lane_sum128(partial, tb + t, te);
+    __syncthreads();
+    if (t < 64) sh[t] = sh[t] + sh[t + 64];
+    __syncthreads();
+    double v = 0.0;
+    if (t < 32) {
+        v = tree32(sh[t] + sh[t + 32]);
+        if (t == 0) sh[0] = v;
+    }
+    __syncthreads();
+    v = sh[0];
+    __syncthreads();
+    return v;
 }
 
 // Budget of decision launches for one solve sequence (per-phase path): past
@@ -230,7 +271,7 @@ __device__ void launch_finalize(const Dev& D, int kind) {
 // sums the scene's partials in tile order) and to the launch.
 template <int BLOCK>
 __device__ void block_finish(const Dev& D, int sc, bool active, double part, int kind, double part2 = 0.0) {
-    __shared__ double sh[32];
+    __shared__ double sh[128];
     __shared__ int sh_last;
     const double total = block_sum_d<BLOCK>(part, sh);
     const double total2 = kind == K_V_B ? block_sum_d<BLOCK>(part2, sh) : 0.0;
@@ -246,10 +287,11 @@ __device__ void block_finish(const Dev& D, int sc, bool active, double part, int
         }
     }
     __syncthreads();
-    if (sh_last && threadIdx.x < 32) {
+    if (sh_last) {  // uniform over the CTA
         __threadfence();
-        const double s = scene_sum_warp(D.partial, P.tile_begin, P.tile_end);
-        const double s2 = kind == K_V_B ? scene_sum_warp(D.partial + D.n_tiles, P.tile_begin, P.tile_end) : 0.0;
+        const double s = scene_sum_block<BLOCK>(D.partial, P.tile_begin, P.tile_end, sh);
+        const double s2 =
+            kind == K_V_B ? scene_sum_block<BLOCK>(D.partial + D.n_tiles, P.tile_begin, P.tile_end, sh) : 0.0;
         if (threadIdx.x == 0) {
             D.scene_counter[sc] = 0;
             scene_decide(D, D.scenes[sc], D.ctl[sc], kind, s, true, s2);
@@ -759,7 +801,10 @@ __global__ void k_advect(const Dev D) {
 // independent gather chains are in flight.  Entries past the row end become
 // (self, w = 0), which contributes exactly 0; entries outside the scene are
 // redirected to self and reported once after the loop.
-constexpr int PU = 4;
+#ifndef IVP_PAIR_UNROLL
+#define IVP_PAIR_UNROLL 4
+#endif
+constexpr int PU = IVP_PAIR_UNROLL;
 
 struct PairBatch {
     int j[PU];
@@ -833,8 +878,8 @@ __device__ __forceinline__ double pack_tile(const Dev& D, const SceneParams& P, 
 #pragma unroll
         for (int u = 0; u < PU; ++u) {
             const int j = b.j[u];
-            float3 dj = f3(__ldcg(src + j));
-            if (upd) dj = sub3(dj, f3(__ldcg(D.sol + j)));
+            float3 dj = f3(src[j]);
+            if (upd) dj = sub3(dj, f3(D.sol[j]));
             acc += dot3(sub3(di, dj), b.J[u]);
         }
     }
@@ -879,7 +924,7 @@ __device__ __forceinline__ double rhs_tile(const Dev& D, const SceneParams& P, c
         bad |= load_pairs<G>(nb, k0, cnt, self, P.s_begin, P.s_end, b);
 #pragma unroll
         for (int u = 0; u < PU; ++u) {
-            const float wgt = fki + mi * __ldcg(D.q + b.j[u]);
+            const float wgt = fki + mi * D.q[b.j[u]];
             ax += wgt * b.J[u].x;
             ay += wgt * b.J[u].y;
             az += wgt * b.J[u].z;
@@ -931,7 +976,7 @@ __device__ __forceinline__ double cga_tile(const Dev& D, const SceneParams& P, c
 #pragma unroll
         for (int u = 0; u < PU; ++u) {
             const int j = b.j[u];
-            const float4 rj = __ldcg(D.r + j), qj = __ldcg(pp + j);
+            const float4 rj = D.r[j], qj = pp[j];
             const float3 pj = make_float3(rj.x + beta * qj.x, rj.y + beta * qj.y, rj.z + beta * qj.z);
             acc += dot3(sub3(pi, pj), b.J[u]);
         }
@@ -974,7 +1019,7 @@ __device__ __forceinline__ double cgb_tile(const Dev& D, const SceneParams& P, c
         bad |= load_pairs<G>(nb, k0, cnt, self, P.s_begin, P.s_end, b);
 #pragma unroll
         for (int u = 0; u < PU; ++u) {
-            const float wgt = yi + mi * __ldcg(D.z + b.j[u]);
+            const float wgt = yi + mi * D.z[b.j[u]];
             ax += wgt * b.J[u].x;
             ay += wgt * b.J[u].y;
             az += wgt * b.J[u].z;
@@ -1018,7 +1063,7 @@ __device__ __forceinline__ void div_tile(const Dev& D, const SceneParams& P, con
     float acc = 0.0f;
     for (int k = T.lane; k < cnt; k += G) {
         const float4 e = __ldg(nb + k);
-        const float3 vj = scale3(s, f3(__ldcg(dc + __float_as_int(e.w))));
+        const float3 vj = scale3(s, f3(dc[__float_as_int(e.w)]));
         acc += dot3(sub3(vi, vj), f3(e));
     }
     acc = group_sum<G>(acc);
@@ -1066,7 +1111,7 @@ __device__ __forceinline__ double visc_setup_tile(const Dev& D, const SceneParam
             const int j = b.j[u];
             const float3 xij = sub3(xi, f3(__ldg(D.xm + j)));
             const int pj = D.pid[j];
-            const float3 vij = sub3(vi, make_float3(__ldcg(D.v + 3 * pj), __ldcg(D.v + 3 * pj + 1), __ldcg(D.v + 3 * pj + 2)));
+            const float3 vij = sub3(vi, make_float3(D.v[3 * pj], D.v[3 * pj + 1], D.v[3 * pj + 2]));
             const float rsq = dot3(xij, xij);
             const float c = (10.0f * __ldg(D.rflu + j)) * __frcp_rn(rsq + eps2);
             const float3 J = b.J[u];
@@ -1147,7 +1192,7 @@ __device__ __forceinline__ double visc_a_tile(const Dev& D, const SceneParams& P
         for (int u = 0; u < PU; ++u) {
             const int j = b.j[u];
             const float3 xij = sub3(xi, f3(__ldg(D.xm + j)));
-            const float4 zj = __ldcg(D.vz + j), qj = __ldcg(pp + j);
+            const float4 zj = D.vz[j], qj = pp[j];
             const float3 pj = make_float3(zj.x + beta * qj.x, zj.y + beta * qj.y, zj.z + beta * qj.z);
             const float rsq = dot3(xij, xij);
             const float s = (10.0f * __ldg(D.rflu + j)) * __frcp_rn(rsq + eps2) * dot3(sub3(pi, pj), xij);
@@ -1360,12 +1405,14 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
 
 // Grid-wide barrier of a co-resident (cooperative) grid, fused with the
 // phase's reduction: the last CTA to arrive sums every active scene's tile
-// partials (scene_sum_warp, the same association as the per-phase path),
-// applies the scene decisions to the control blocks in global memory and only
-// then releases the others.  Control blocks are read past L1 (other CTAs
-// write them).  The wait is bounded: after kBarrierLimitNs a CTA sets the
-// timeout flag and reports failure, so a fault can never keep the kernel
-// spinning.
+// partials (the same association as the per-phase path), runs the scene
+// decisions (one thread per scene) on its own copies of the control blocks
+// (current: every CTA refreshes them after each barrier), writes them back and
+// only then releases the others.  Every CTA executes a gpu-scope fence after
+// the barrier, which orders its later plain loads (the L1-cached neighbour
+// gathers) after every write of the previous phase.  The wait is bounded: after kBarrierLimitNs a
+// CTA sets the timeout flag and reports failure, so a fault can never keep
+// the kernel spinning.
 constexpr unsigned long long kBarrierLimitNs = 2000000000ull;
 
 __device__ __forceinline__ bool phase_active(const SceneCtl& C, int kind) {
@@ -1388,7 +1435,13 @@ __device__ __forceinline__ SceneCtl ctl_load(const SceneCtl* p) {
     return c;
 }
 
-__device__ bool grid_reduce_barrier(const Dev& D, int kind, int* sh_flag, double* sum_sh, double* sum_sh2) {
+// Scenes up to this count are summed one after another by the whole CTA;
+// more are spread over the warps, one scene per warp.
+constexpr int kBlockSumScenes = 2;
+
+template <int BLOCK>
+__device__ bool grid_reduce_barrier(const Dev& D, int kind, int* sh_flag, double* sum_sh, double* sum_sh2,
+                                    SceneCtl* sc_sh, double* red_sh) {
     unsigned g = 0;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -1401,25 +1454,42 @@ __device__ bool grid_reduce_barrier(const Dev& D, int kind, int* sh_flag, double
     if (sh_flag[0]) {
         __threadfence();
         if (kind >= 0) {
-            const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-            for (int s = warp; s < D.n_scenes; s += nwarps) {
-                if (!phase_active(ctl_load(D.ctl + s), kind)) continue;
-                const SceneParams& P = D.scenes[s];
-                const double v = scene_sum_warp(D.partial, P.tile_begin, P.tile_end);
-                const double v2 = kind == K_V_B ? scene_sum_warp(D.partial + D.n_tiles, P.tile_begin, P.tile_end) : 0.0;
-                if ((threadIdx.x & 31) == 0) {
-                    sum_sh[s] = v;
-                    sum_sh2[s] = v2;
+            const int ns = D.n_scenes;
+            if (ns <= kBlockSumScenes) {
+                for (int s = 0; s < ns; ++s) {
+                    if (!phase_active(sc_sh[s], kind)) continue;
+                    const SceneParams& P = D.scenes[s];
+                    const double v = scene_sum_block<BLOCK>(D.partial, P.tile_begin, P.tile_end, red_sh);
+                    const double v2 =
+                        kind == K_V_B ? scene_sum_block<BLOCK>(D.partial + D.n_tiles, P.tile_begin, P.tile_end, red_sh)
+                                      : 0.0;
+                    if (threadIdx.x == 0) {
+                        sum_sh[s] = v;
+                        sum_sh2[s] = v2;
+                    }
+                }
+            } else {
+                const int warp = threadIdx.x >> 5;
+                for (int s = warp; s < ns; s += BLOCK / 32) {
+                    if (!phase_active(sc_sh[s], kind)) continue;
+                    const SceneParams& P = D.scenes[s];
+                    const double v = scene_sum_warp(D.partial, P.tile_begin, P.tile_end);
+                    const double v2 =
+                        kind == K_V_B ? scene_sum_warp(D.partial + D.n_tiles, P.tile_begin, P.tile_end) : 0.0;
+                    if ((threadIdx.x & 31) == 0) {
+                        sum_sh[s] = v;
+                        sum_sh2[s] = v2;
+                    }
                 }
             }
             __syncthreads();
-            if (threadIdx.x == 0)
-                for (int s = 0; s < D.n_scenes; ++s) {
-                    SceneCtl c = ctl_load(D.ctl + s);
-                    if (!phase_active(c, kind)) continue;
-                    scene_decide(D, D.scenes[s], c, kind, sum_sh[s], true, sum_sh2[s]);
-                    D.ctl[s] = c;
-                }
+            for (int s = threadIdx.x; s < ns; s += BLOCK) {
+                SceneCtl& c = sc_sh[s];
+                if (!phase_active(c, kind)) continue;
+                scene_decide(D, D.scenes[s], c, kind, sum_sh[s], true, sum_sh2[s]);
+                D.ctl[s] = c;
+                __threadfence();
+            }
         }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -1469,7 +1539,9 @@ struct Phaser {
         sc_sh = reinterpret_cast<SceneCtl*>(dyn + 2 * D.n_scenes);
     }
 
-    __device__ bool barrier(int kind) { return grid_reduce_barrier(D, kind, flag_sh, sum_sh, sum_sh2); }
+    __device__ bool barrier(int kind) {
+        return grid_reduce_barrier<BLOCK>(D, kind, flag_sh, sum_sh, sum_sh2, sc_sh, red_sh);
+    }
 
     __device__ void refresh() {
         for (int s = threadIdx.x; s < D.n_scenes; s += BLOCK) sc_sh[s] = ctl_load(D.ctl + s);
@@ -1537,12 +1609,21 @@ struct Phaser {
     }
 };
 
+// Register budget of the persistent kernels: room for IVP_PERSIST_THREADS
+// resident threads per SM (the occupancy sets how many tiles each CTA walks
+// through one after another in every phase).
+#ifndef IVP_PERSIST_THREADS
+#define IVP_PERSIST_THREADS 1024
+#endif
+template <int BLOCK>
+constexpr int persist_min_blocks() { return IVP_PERSIST_THREADS / BLOCK > 0 ? IVP_PERSIST_THREADS / BLOCK : 1; }
+
 // Weiler 2018 implicit viscosity of every scene that enables it, in one
 // persistent cooperative launch (weiler18.py:371-401).
 template <int G, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_visc_persistent(const Dev D) {
+__global__ void __launch_bounds__(BLOCK, persist_min_blocks<BLOCK>()) k_visc_persistent(const Dev D) {
     extern __shared__ double dyn_sh[];
-    __shared__ double red_sh[32];
+    __shared__ double red_sh[128];
     __shared__ int flag_sh[2], any_sh;
     Phaser<G, BLOCK> ph(D, dyn_sh, red_sh, flag_sh, &any_sh);
     if (blockIdx.x == 0 && threadIdx.x == 0)
@@ -1571,9 +1652,9 @@ __global__ void __launch_bounds__(BLOCK) k_visc_persistent(const Dev D) {
 
 // The whole IP.solve of every scene in one persistent cooperative launch.
 template <int G, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_ip_persistent(const Dev D) {
+__global__ void __launch_bounds__(BLOCK, persist_min_blocks<BLOCK>()) k_ip_persistent(const Dev D) {
     extern __shared__ double dyn_sh[];
-    __shared__ double red_sh[32];
+    __shared__ double red_sh[128];
     __shared__ int flag_sh[2], any_sh;
     Phaser<G, BLOCK> ph(D, dyn_sh, red_sh, flag_sh, &any_sh);
     // CTA 0 starts every scene's control block (reset_stats); the first

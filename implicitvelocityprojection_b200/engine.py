@@ -26,7 +26,7 @@ def _stream_ptr(stream: Optional[torch.cuda.Stream] = None) -> int:
 @dataclasses.dataclass
 class EngineOptions:
     lanes_per_particle: int = 4
-    particles_per_block: int = 32
+    particles_per_block: int = 64
     list_stride: int = 64
     max_hist: int = 128
     use_graphs: bool = True

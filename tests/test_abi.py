@@ -35,7 +35,7 @@ def test_status_strings_and_defaults():
     assert b"non-positive" in L.ivp_status_string(1)
     o = _lib.Options()
     L.ivp_default_options(o)
-    assert o.lanes_per_particle * o.particles_per_block == 128
+    assert o.lanes_per_particle * o.particles_per_block == 256
     assert o.list_stride >= 60 and o.use_graphs == 1
 
 
