@@ -26,6 +26,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -160,12 +161,21 @@ def load_peaks():
 
 
 def load_traffic(kernel: str, workload: str):
-    p = os.path.join(REPO, "profiles", "traffic.json")
-    if not os.path.exists(p):
+    """DRAM bytes per launch of `kernel` on `workload`, from the ncu summaries
+    under profiles/ (a line `traffic kernel=K workload=W dram_bytes_per_launch=B`)."""
+    d = os.path.join(REPO, "profiles")
+    if not os.path.isdir(d):
         return None
-    with open(p) as f:
-        d = json.load(f)
-    return d.get(workload, {}).get(kernel)
+    pat = re.compile(r"traffic kernel=(\S+) workload=(\S+) dram_bytes_per_launch=(\d+)")
+    for name in sorted(os.listdir(d)):
+        if not name.endswith(".md"):
+            continue
+        with open(os.path.join(d, name)) as f:
+            for line in f:
+                m = pat.search(line)
+                if m and m.group(1) == kernel and m.group(2) == workload:
+                    return float(m.group(3))
+    return None
 
 
 # ----------------------------------------------------------------- arms
