@@ -148,16 +148,20 @@ struct Dev {
     float4* d0;
     float4* d1;
     float4* sol;
-    float4* r;
-    float4* p0;
-    float4* p1;
+    float4* r;               // viscosity residual (own slot only)
+    // CG records, two float4 per slot (one 32-byte sector): [2i] the vector
+    // the next direction is formed from (IP residual r, or the viscosity
+    // preconditioned residual z with .w = 1/rho of fluid slots), [2i+1] the
+    // previous direction.  Iteration k reads cg[k & 1] and writes
+    // cg[(k + 1) & 1], so a neighbour gather takes one sector.
+    float4* cg0;
+    float4* cg1;
     float* y;
     float* s;
     float* fk;
     float* inv_m;            // 1/m of dynamic slots (0 for static)
     float* rflu;             // 1/rho of fluid slots (0 for non-fluid): viscosity neighbour weight
     float4* vs;              // viscosity: slot-ordered velocity
-    float4* vz;              // viscosity: preconditioned residual
     float4* vap;             // viscosity: A p
     float4* pinv;            // viscosity: 3x3 block-Jacobi inverse, 3 rows per slot
     float* q;                // fk / m
@@ -261,6 +265,22 @@ __device__ __forceinline__ float group_sum(float v) {
 #pragma unroll
     for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
+}
+
+// One 32-byte CG record (two float4, 32-byte aligned) in a single 256-bit
+// load: one L1 request per lane instead of two for a neighbour gather.
+__device__ __forceinline__ void ld_rec(const float4* p, float4& a, float4& b) {
+    asm volatile("ld.global.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+                 : "l"(p));
+}
+
+// Two consecutive neighbour-list entries (32-byte aligned, read-only for the
+// launch) in one 256-bit load through the non-coherent path.
+__device__ __forceinline__ void ld_rec_nc(const float4* p, float4& a, float4& b) {
+    asm volatile("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+                 : "l"(p));
 }
 
 __device__ __forceinline__ double warp_sum_d(double v) {

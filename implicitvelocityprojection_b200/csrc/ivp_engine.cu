@@ -453,7 +453,7 @@ int validate(const ivp_scene_desc* sc, int n, const ivp_options* o) {
         if (o->particles_per_block <= 0 || !kernel_set(o->lanes_per_particle, o->particles_per_block * o->lanes_per_particle, &K))
             return IVP_ERR_BAD_ARG;
     }
-    if (o->list_stride <= 0 || o->max_hist <= 0) return IVP_ERR_BAD_ARG;
+    if (o->list_stride <= 0 || (o->list_stride & 1) || o->max_hist <= 0) return IVP_ERR_BAD_ARG;
     long expect = 0;
     for (int s = 0; s < n; ++s) {
         const ivp_scene_desc& d = sc[s];
@@ -579,8 +579,8 @@ void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
     P.off[i++] = L.add(sizeof(float4) * N);                 // 19 d1
     P.off[i++] = L.add(sizeof(float4) * N);                 // 20 sol
     P.off[i++] = L.add(sizeof(float4) * N);                 // 21 r
-    P.off[i++] = L.add(sizeof(float4) * N);                 // 22 p0
-    P.off[i++] = L.add(sizeof(float4) * N);                 // 23 p1
+    P.off[i++] = L.add(2 * sizeof(float4) * N);             // 22 cg0
+    P.off[i++] = L.add(2 * sizeof(float4) * N);             // 23 cg1
     P.off[i++] = L.add(sizeof(float) * N);                  // 24 y
     P.off[i++] = L.add(sizeof(float) * N);                  // 25 s
     P.off[i++] = L.add(sizeof(float) * N);                  // 26 fk
@@ -599,10 +599,9 @@ void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
     P.off[i++] = L.add(sizeof(float) * N);                           // 39 z
     P.off[i++] = L.add(sizeof(float) * N);                           // 40 rflu
     P.off[i++] = L.add(sizeof(float4) * N);                          // 41 vs
-    P.off[i++] = L.add(sizeof(float4) * N);                          // 42 vz
-    P.off[i++] = L.add(sizeof(float4) * N);                          // 43 vap
-    P.off[i++] = L.add(3 * sizeof(float4) * N);                      // 44 pinv
-    P.off[i++] = L.add(sizeof(int4) * std::max<size_t>(P.segs.size(), 1));  // 45 segs
+    P.off[i++] = L.add(sizeof(float4) * N);                          // 42 vap
+    P.off[i++] = L.add(3 * sizeof(float4) * N);                      // 43 pinv
+    P.off[i++] = L.add(sizeof(int4) * std::max<size_t>(P.segs.size(), 1));  // 44 segs
 }
 
 cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
@@ -683,8 +682,8 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
     D.d1 = reinterpret_cast<float4*>(w + P.off[i++]);
     D.sol = reinterpret_cast<float4*>(w + P.off[i++]);
     D.r = reinterpret_cast<float4*>(w + P.off[i++]);
-    D.p0 = reinterpret_cast<float4*>(w + P.off[i++]);
-    D.p1 = reinterpret_cast<float4*>(w + P.off[i++]);
+    D.cg0 = reinterpret_cast<float4*>(w + P.off[i++]);
+    D.cg1 = reinterpret_cast<float4*>(w + P.off[i++]);
     D.y = reinterpret_cast<float*>(w + P.off[i++]);
     D.s = reinterpret_cast<float*>(w + P.off[i++]);
     D.fk = reinterpret_cast<float*>(w + P.off[i++]);
@@ -704,7 +703,6 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
     D.z = reinterpret_cast<float*>(w + P.off[i++]);
     D.rflu = reinterpret_cast<float*>(w + P.off[i++]);
     D.vs = reinterpret_cast<float4*>(w + P.off[i++]);
-    D.vz = reinterpret_cast<float4*>(w + P.off[i++]);
     D.vap = reinterpret_cast<float4*>(w + P.off[i++]);
     D.pinv = reinterpret_cast<float4*>(w + P.off[i++]);
     D.segs = reinterpret_cast<int4*>(w + P.off[i++]);

@@ -798,33 +798,46 @@ __global__ void k_advect(const Dev D) {
 // ------------------------------------------------------------- IP solve
 
 // Pair-loop unroll: each lane loads PU list entries before gathering, so PU
-// independent gather chains are in flight.  Entries past the row end become
-// (self, w = 0), which contributes exactly 0; entries outside the scene are
-// redirected to self and reported once after the loop.
+// independent gather chains are in flight.  The entries come in 32-byte
+// pairs: in a batch of G * PU entries starting at a multiple of G * PU, lane
+// l takes entries 2l + 2Gu and 2l + 2Gu + 1 (u < PU / 2), one 256-bit load
+// each.  Rows start on 1 KB boundaries and the list stride is even, so the
+// second entry of a pair is inside the row whenever the first is below the
+// count.  Entries past the row end become (self, w = 0), which contributes
+// exactly 0; entries outside the scene are redirected to self and reported
+// once after the loop.
 #ifndef IVP_PAIR_UNROLL
 #define IVP_PAIR_UNROLL 4
 #endif
 constexpr int PU = IVP_PAIR_UNROLL;
+static_assert(PU % 2 == 0, "entries are loaded in pairs");
 
 struct PairBatch {
     int j[PU];
     float3 J[PU];
 };
 
+__device__ __forceinline__ void pair_entry(const float4& e, bool in, int self, int lo, int hi, int& j, float3& J,
+                                           bool& bad) {
+    const int jj = __float_as_int(e.w);
+    const bool ok = jj >= lo && jj < hi;
+    bad |= in && !ok;
+    j = (in && ok) ? jj : self;
+    J = (in && ok) ? f3(e) : make_float3(0.f, 0.f, 0.f);
+}
+
+// k0 = 2 * lane + (batch start)
 template <int G>
 __device__ __forceinline__ bool load_pairs(const float4* __restrict__ nb, int k0, int cnt, int self, int lo, int hi,
                                            PairBatch& b) {
     bool bad = false;
 #pragma unroll
-    for (int u = 0; u < PU; ++u) {
-        const int k = k0 + u * G;
-        float4 e = make_float4(0.f, 0.f, 0.f, __int_as_float(self));
-        if (k < cnt) e = __ldg(nb + k);
-        const int j = __float_as_int(e.w);
-        const bool ok = j >= lo && j < hi;
-        bad |= !ok;
-        b.j[u] = ok ? j : self;
-        b.J[u] = ok ? f3(e) : make_float3(0.f, 0.f, 0.f);
+    for (int u = 0; u < PU / 2; ++u) {
+        const int k = k0 + u * 2 * G;
+        float4 e0 = make_float4(0.f, 0.f, 0.f, 0.f), e1 = e0;
+        if (k < cnt) ld_rec_nc(nb + k, e0, e1);
+        pair_entry(e0, k < cnt, self, lo, hi, b.j[2 * u], b.J[2 * u], bad);
+        pair_entry(e1, k + 1 < cnt, self, lo, hi, b.j[2 * u + 1], b.J[2 * u + 1], bad);
     }
     return bad;
 }
@@ -872,7 +885,7 @@ __device__ __forceinline__ double pack_tile(const Dev& D, const SceneParams& P, 
     float acc = 0.0f;
     bool bad = false;
     const int self = T.valid ? T.i : P.s_begin;
-    for (int k0 = T.lane; k0 < cnt; k0 += G * PU) {
+    for (int k0 = 2 * T.lane; k0 < cnt; k0 += G * PU) {
         PairBatch b;
         bad |= load_pairs<G>(nb, k0, cnt, self, P.s_begin, P.s_end, b);
 #pragma unroll
@@ -919,7 +932,7 @@ __device__ __forceinline__ double rhs_tile(const Dev& D, const SceneParams& P, c
     float ax = 0.0f, ay = 0.0f, az = 0.0f;
     bool bad = false;
     const int self = T.valid ? T.i : P.s_begin;
-    for (int k0 = T.lane; k0 < cnt; k0 += G * PU) {
+    for (int k0 = 2 * T.lane; k0 < cnt; k0 += G * PU) {
         PairBatch b;
         bad |= load_pairs<G>(nb, k0, cnt, self, P.s_begin, P.s_end, b);
 #pragma unroll
@@ -938,9 +951,9 @@ __device__ __forceinline__ double rhs_tile(const Dev& D, const SceneParams& P, c
     if (T.valid && T.lane == 0) {
         const float om = P.omega;
         const float4 rhs = make_float4(om * ax, om * ay, om * az, 0.0f);
-        D.r[T.i] = rhs;
+        D.cg0[2 * T.i] = rhs;
+        D.cg0[2 * T.i + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
         D.sol[T.i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        D.p0[T.i] = make_float4(0.f, 0.f, 0.f, 0.f);
         part = (double)dot3(f3(rhs), f3(rhs));
     }
     return part;
@@ -954,8 +967,8 @@ __device__ __forceinline__ double rhs_tile(const Dev& D, const SceneParams& P, c
 template <int G>
 __device__ __forceinline__ double cga_tile(const Dev& D, const SceneParams& P, const TileCtx& T, float beta,
                                            int cg_it) {
-    const float4* pp = (cg_it & 1) ? D.p1 : D.p0;
-    float4* pn = (cg_it & 1) ? D.p0 : D.p1;
+    const float4* cc = (cg_it & 1) ? D.cg1 : D.cg0;  // {r, p_prev}
+    float4* cn = (cg_it & 1) ? D.cg0 : D.cg1;
     const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
     const float4* nb = D.nbr + (size_t)T.row * D.stride;
     float3 xi = make_float3(0.f, 0.f, 0.f), pi = xi;
@@ -964,19 +977,20 @@ __device__ __forceinline__ double cga_tile(const Dev& D, const SceneParams& P, c
         const float4 a = D.xm[T.i];
         xi = f3(a);
         mi = a.w;
-        const float4 ri = D.r[T.i], qi = pp[T.i];
+        const float4 ri = cc[2 * T.i], qi = cc[2 * T.i + 1];
         pi = make_float3(ri.x + beta * qi.x, ri.y + beta * qi.y, ri.z + beta * qi.z);
     }
     float acc = 0.0f;
     bool bad = false;
     const int self = T.valid ? T.i : P.s_begin;
-    for (int k0 = T.lane; k0 < cnt; k0 += G * PU) {
+    for (int k0 = 2 * T.lane; k0 < cnt; k0 += G * PU) {
         PairBatch b;
         bad |= load_pairs<G>(nb, k0, cnt, self, P.s_begin, P.s_end, b);
 #pragma unroll
         for (int u = 0; u < PU; ++u) {
             const int j = b.j[u];
-            const float4 rj = D.r[j], qj = pp[j];
+            float4 rj, qj;
+            ld_rec(cc + 2 * j, rj, qj);
             const float3 pj = make_float3(rj.x + beta * qj.x, rj.y + beta * qj.y, rj.z + beta * qj.z);
             acc += dot3(sub3(pi, pj), b.J[u]);
         }
@@ -988,7 +1002,7 @@ __device__ __forceinline__ double cga_tile(const Dev& D, const SceneParams& P, c
         const float yi = acc * D.s[T.i];
         D.y[T.i] = yi;
         D.z[T.i] = yi * D.inv_m[T.i];
-        pn[T.i] = make_float4(pi.x, pi.y, pi.z, 0.0f);
+        cn[2 * T.i + 1] = make_float4(pi.x, pi.y, pi.z, 0.0f);
         part = (double)(mi * dot3(pi, pi)) + (double)P.omega * (double)yi * (double)acc;
     }
     return part;
@@ -1000,7 +1014,8 @@ __device__ __forceinline__ double cga_tile(const Dev& D, const SceneParams& P, c
 template <int G>
 __device__ __forceinline__ double cgb_tile(const Dev& D, const SceneParams& P, const TileCtx& T, float alpha,
                                            int cg_it) {
-    const float4* pc = (cg_it & 1) ? D.p0 : D.p1;
+    const float4* cc = (cg_it & 1) ? D.cg1 : D.cg0;  // own r
+    float4* cn = (cg_it & 1) ? D.cg0 : D.cg1;        // own p; receives the new r
     const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
     const float4* nb = D.nbr + (size_t)T.row * D.stride;
     float3 xi = make_float3(0.f, 0.f, 0.f);
@@ -1014,7 +1029,7 @@ __device__ __forceinline__ double cgb_tile(const Dev& D, const SceneParams& P, c
     float ax = 0.0f, ay = 0.0f, az = 0.0f;
     bool bad = false;
     const int self = T.valid ? T.i : P.s_begin;
-    for (int k0 = T.lane; k0 < cnt; k0 += G * PU) {
+    for (int k0 = 2 * T.lane; k0 < cnt; k0 += G * PU) {
         PairBatch b;
         bad |= load_pairs<G>(nb, k0, cnt, self, P.s_begin, P.s_end, b);
 #pragma unroll
@@ -1032,9 +1047,9 @@ __device__ __forceinline__ double cgb_tile(const Dev& D, const SceneParams& P, c
     double part = 0.0;
     if (T.valid && T.lane == 0) {
         const float om = P.omega;
-        const float4 p4 = pc[T.i];
+        const float4 p4 = cn[2 * T.i + 1];
         const float3 ap = make_float3(mi * p4.x + om * ax, mi * p4.y + om * ay, mi * p4.z + om * az);
-        float4 xs = D.sol[T.i], rs = D.r[T.i];
+        float4 xs = D.sol[T.i], rs = cc[2 * T.i];
         xs.x = xs.x + alpha * p4.x;
         xs.y = xs.y + alpha * p4.y;
         xs.z = xs.z + alpha * p4.z;
@@ -1042,7 +1057,7 @@ __device__ __forceinline__ double cgb_tile(const Dev& D, const SceneParams& P, c
         rs.y = rs.y - alpha * ap.y;
         rs.z = rs.z - alpha * ap.z;
         D.sol[T.i] = xs;
-        D.r[T.i] = rs;
+        cn[2 * T.i] = rs;
         part = (double)dot3(f3(rs), f3(rs));
     }
     return part;
@@ -1103,7 +1118,7 @@ __device__ __forceinline__ double visc_setup_tile(const Dev& D, const SceneParam
     float lx = 0.0f, ly = 0.0f, lz = 0.0f;
     bool bad = false;
     const int self = T.valid ? T.i : P.s_begin;
-    for (int k0 = T.lane; k0 < (fluid ? cnt : 0); k0 += G * PU) {
+    for (int k0 = 2 * T.lane; k0 < (fluid ? cnt : 0); k0 += G * PU) {
         PairBatch b;
         bad |= load_pairs<G>(nb, k0, cnt, self, P.s_begin, P.s_end, b);
 #pragma unroll
@@ -1157,9 +1172,9 @@ __device__ __forceinline__ double visc_setup_tile(const Dev& D, const SceneParam
         const float3 rh = make_float3(vi.x + (-1.0f) * av.x, vi.y + (-1.0f) * av.y, vi.z + (-1.0f) * av.z);
         const float3 z = make_float3(dot3(f3(r0), rh), dot3(f3(r1), rh), dot3(f3(r2), rh));
         D.r[T.i] = make_float4(rh.x, rh.y, rh.z, 0.f);
-        D.vz[T.i] = make_float4(z.x, z.y, z.z, 0.f);
+        D.cg0[2 * T.i] = make_float4(z.x, z.y, z.z, D.rflu[T.i]);
+        D.cg0[2 * T.i + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
         D.sol[T.i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        D.p0[T.i] = make_float4(0.f, 0.f, 0.f, 0.f);
         part = (double)dot3(rh, z);
     }
     return part;
@@ -1170,32 +1185,33 @@ __device__ __forceinline__ double visc_setup_tile(const Dev& D, const SceneParam
 template <int G>
 __device__ __forceinline__ double visc_a_tile(const Dev& D, const SceneParams& P, const TileCtx& T, float beta,
                                               int it) {
-    const float4* pp = (it & 1) ? D.p1 : D.p0;
-    float4* pn = (it & 1) ? D.p0 : D.p1;
+    const float4* cc = (it & 1) ? D.cg1 : D.cg0;  // {z | 1/rho, p_prev}
+    float4* cn = (it & 1) ? D.cg0 : D.cg1;
     const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
     const float4* nb = D.nbr + (size_t)T.row * D.stride;
     const bool fluid = T.valid && D.rflu[T.i] != 0.0f;
     float3 xi = make_float3(0.f, 0.f, 0.f), pi = xi;
     if (T.valid) {
         xi = f3(D.xm[T.i]);
-        const float4 zi = D.vz[T.i], qi = pp[T.i];
+        const float4 zi = cc[2 * T.i], qi = cc[2 * T.i + 1];
         pi = make_float3(zi.x + beta * qi.x, zi.y + beta * qi.y, zi.z + beta * qi.z);
     }
     const float eps2 = 0.01f * P.h * P.h;
     float lx = 0.0f, ly = 0.0f, lz = 0.0f;
     bool bad = false;
     const int self = T.valid ? T.i : P.s_begin;
-    for (int k0 = T.lane; k0 < (fluid ? cnt : 0); k0 += G * PU) {
+    for (int k0 = 2 * T.lane; k0 < (fluid ? cnt : 0); k0 += G * PU) {
         PairBatch b;
         bad |= load_pairs<G>(nb, k0, cnt, self, P.s_begin, P.s_end, b);
 #pragma unroll
         for (int u = 0; u < PU; ++u) {
             const int j = b.j[u];
             const float3 xij = sub3(xi, f3(__ldg(D.xm + j)));
-            const float4 zj = D.vz[j], qj = pp[j];
+            float4 zj, qj;
+            ld_rec(cc + 2 * j, zj, qj);
             const float3 pj = make_float3(zj.x + beta * qj.x, zj.y + beta * qj.y, zj.z + beta * qj.z);
             const float rsq = dot3(xij, xij);
-            const float s = (10.0f * __ldg(D.rflu + j)) * __frcp_rn(rsq + eps2) * dot3(sub3(pi, pj), xij);
+            const float s = (10.0f * zj.w) * __frcp_rn(rsq + eps2) * dot3(sub3(pi, pj), xij);
             lx += s * b.J[u].x;
             ly += s * b.J[u].y;
             lz += s * b.J[u].z;
@@ -1212,7 +1228,7 @@ __device__ __forceinline__ double visc_a_tile(const Dev& D, const SceneParams& P
             const float f = visc_factor(D, P, T.i);
             ap = make_float3(pi.x - f * lx, pi.y - f * ly, pi.z - f * lz);
         }
-        pn[T.i] = make_float4(pi.x, pi.y, pi.z, 0.f);
+        cn[2 * T.i + 1] = make_float4(pi.x, pi.y, pi.z, 0.f);
         D.vap[T.i] = make_float4(ap.x, ap.y, ap.z, 0.f);
         part = (double)dot3(pi, ap);
     }
@@ -1227,8 +1243,8 @@ __device__ __forceinline__ void visc_b_tile(const Dev& D, const TileCtx& T, floa
     *part = 0.0;
     *part2 = 0.0;
     if (!(T.valid && T.lane == 0)) return;
-    const float4* pc = (it & 1) ? D.p0 : D.p1;
-    const float4 p4 = pc[T.i], ap = D.vap[T.i];
+    float4* cn = (it & 1) ? D.cg0 : D.cg1;  // own p; receives the new z
+    const float4 p4 = cn[2 * T.i + 1], ap = D.vap[T.i];
     float4 x = D.sol[T.i], r = D.r[T.i];
     x.x = x.x + alpha * p4.x;
     x.y = x.y + alpha * p4.y;
@@ -1242,7 +1258,7 @@ __device__ __forceinline__ void visc_b_tile(const Dev& D, const TileCtx& T, floa
     const float3 rr = f3(r);
     const float3 z = make_float3(dot3(f3(D.pinv[3 * T.i]), rr), dot3(f3(D.pinv[3 * T.i + 1]), rr),
                                  dot3(f3(D.pinv[3 * T.i + 2]), rr));
-    D.vz[T.i] = make_float4(z.x, z.y, z.z, 0.f);
+    cn[2 * T.i] = make_float4(z.x, z.y, z.z, D.rflu[T.i]);
     *part = (double)dot3(rr, rr);
     *part2 = (double)dot3(rr, z);
 }

@@ -65,7 +65,7 @@ typedef struct {
 typedef struct {
     int32_t lanes_per_particle;   /* 1, 2, 4 or 8 lanes share one particle's neighbour sum */
     int32_t particles_per_block;  /* particles per CTA in the neighbour-sum kernels */
-    int32_t list_stride;          /* neighbour-list row stride (>= every scene's cache_size) */
+    int32_t list_stride;          /* neighbour-list row stride: even, >= every scene's cache_size */
     int32_t max_hist;             /* per-scene stats history length (outer iterations) */
     int32_t use_graphs;           /* 1: whole steps as CUDA graphs (device-side control, no host sync) */
     int32_t persistent;           /* 1: the IP solve as one persistent cooperative kernel with grid barriers;
