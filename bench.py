@@ -56,13 +56,34 @@ def make_scene(name: str):
     raise SystemExit(f"unknown workload {name}")
 
 
-def workload_config(sc, name: str) -> dict:
+def make_scenes(name: str):
+    """The workload as a list of independent scenes."""
+    from implicitvelocityprojection_b200 import scenes as S
+    if name.startswith("batch"):
+        n = int(name[5:] or 64)
+        return S.batch_mix(n_scenes=n)
+    return [make_scene(name)]
+
+
+def workload_config(scenes, name: str) -> dict:
+    if not isinstance(scenes, (list, tuple)):
+        scenes = [scenes]
+    common = {"surface_tension": "off", "reductions": "f64 (CG inner products, error averages)",
+              "l2": "flushed between timed steps (256 MiB device write, outside the timed events)"}
+    if len(scenes) > 1:
+        nd = [sc.n_dynamic for sc in scenes]
+        return {"workload": f"batch of {len(scenes)} column collapses (fluid log-uniform 4,096-65,536, "
+                            f"aspect U[1,4], seed 0)",
+                "scenes": len(scenes), "fluid_particles": int(sum(nd)), "fluid_min": int(min(nd)),
+                "fluid_max": int(max(nd)), "boundary_particles": int(sum(sc.n - sc.n_dynamic for sc in scenes)),
+                "spacing_m": scenes[0].particle_diameter, "dt_s": scenes[0].dt,
+                "densityErrorTol": scenes[0].density_error_tol, "viscosity": "off", **common}
+    sc = scenes[0]
     return {"workload": sc.name + ("_ip_only" if name == "tall_column_ip" else ""),
             "fluid_particles": sc.n_dynamic, "boundary_particles": sc.n - sc.n_dynamic,
             "spacing_m": sc.particle_diameter, "dt_s": sc.dt, "densityErrorTol": sc.density_error_tol,
             "viscosity": ("weiler18 nu=%g" % sc.viscosity_coeff) if sc.viscosity_method == 1 else "off",
-            "surface_tension": "off", "reductions": "f64 (CG inner products, error averages)",
-            "l2": "flushed between timed steps (256 MiB device write, outside the timed events)"}
+            **common}
 
 
 # ----------------------------------------------------------------- clocks
@@ -129,13 +150,14 @@ def algorithmic_bytes(kernel: str, n_dyn: int, n_all: int, pairs: int, it=None) 
     viscosity-CG iterations)."""
     P = float(pairs)
     if kernel == "ip_solve":
-        L, I, V = it["outer"], it["cg"], it["visc"]
+        L, I = it["outer"], it["cg"]
         b = (L + 1) * algorithmic_bytes("pack", n_dyn, n_all, pairs) + L * algorithmic_bytes("rhs", n_dyn, n_all, pairs)
         b += I * (algorithmic_bytes("cg_a", n_dyn, n_all, pairs) + algorithmic_bytes("cg_b", n_dyn, n_all, pairs))
         b += algorithmic_bytes("divergence", n_dyn, n_all, pairs) + 48 * n_dyn  # d = dt v, v = d / dt
-        if it.get("visc_on"):
-            b += 16 * P + 120 * n_dyn + V * ((16 * P + 64 * n_dyn) + 120 * n_dyn)
         return b
+    if kernel == "visc":  # Weiler 2018 solve: setup pass, then per iteration a list pass and a slot pass
+        V = it["visc"] if it.get("visc_on") else 0.0
+        return 16 * P + 120 * n_dyn + V * ((16 * P + 64 * n_dyn) + 120 * n_dyn)
     if kernel == "cg_a":
         return 16 * P + 48 * n_dyn
     if kernel == "cg_b":
@@ -180,43 +202,71 @@ def load_traffic(kernel: str, workload: str):
 
 # ----------------------------------------------------------------- arms
 
-def cpu_baseline(sc, budget_s: float, max_steps: int):
-    """The oracle (C restatement, OpenMP) stepping the same workload."""
+def cpu_baseline(scenes, budget_s: float, max_steps: int):
+    """The oracle (C restatement, OpenMP) stepping the same workload: one
+    scene for up to `budget_s`, or for a batch, two steps of each scene in
+    turn until the budget is spent."""
     from oracle import oracle as O
-    st = O.State.from_scene(sc)
-    st.rebuild()
-    t0 = time.perf_counter()
-    steps = 0
-    while steps < max_steps and (time.perf_counter() - t0) < budget_s:
-        st.step(fast=True)
-        steps += 1
-    dt = time.perf_counter() - t0
-    return {"value": sc.n_dynamic * steps / dt, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
-            "sample": f"{steps} full steps of {sc.name} ({sc.n_dynamic} fluid particles), {dt:.1f} s"}
+    if not isinstance(scenes, (list, tuple)):
+        scenes = [scenes]
+    per_scene = max_steps if len(scenes) == 1 else 2
+    t_all, ps, steps, used = 0.0, 0, 0, 0
+    for sc in scenes:
+        st = O.State.from_scene(sc)
+        st.rebuild()
+        t0 = time.perf_counter()
+        k = 0
+        while k < per_scene and t_all + (time.perf_counter() - t0) < budget_s:
+            st.step(fast=True)
+            k += 1
+        t_all += time.perf_counter() - t0
+        ps += sc.n_dynamic * k
+        steps += k
+        used += 1
+        if t_all >= budget_s:
+            break
+    if len(scenes) == 1:
+        sample = f"{steps} full steps of {scenes[0].name} ({scenes[0].n_dynamic} fluid particles), {t_all:.1f} s"
+    else:
+        sample = f"{steps} full steps over the first {used} of {len(scenes)} scenes ({ps} particle-steps), {t_all:.1f} s"
+    return {"value": ps / t_all, "unit": UNIT, "cores": O.num_threads(), "kind": "port", "sample": sample}
 
 
 def run_reference(args, rank, world):
+    """The CPU restatement of the reference's step (the oracle, OpenMP on the
+    host cores) on the same workload; for a batch, one step is one step of
+    every scene.  Timed steps stop early once `--ref-budget-s` is spent."""
     if rank != 0:
         return
-    sc = make_scene(args.workload)
+    scenes = make_scenes(args.workload)
     from oracle import oracle as O
-    st = O.State.from_scene(sc)
-    st.rebuild()
-    for _ in range(args.warmup):
-        st.step(fast=True)
+    states = []
+    for sc in scenes:
+        st = O.State.from_scene(sc)
+        st.rebuild()
+        states.append(st)
+    n_dyn = sum(sc.n_dynamic for sc in scenes)
+    for _ in range(min(args.warmup, 3)):
+        for st in states:
+            st.step(fast=True)
     times = []
+    t_start = time.perf_counter()
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        st.step(fast=True)
+        for st in states:
+            st.step(fast=True)
         times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_start > args.ref_budget_s:
+            break
     tot = sum(times)
-    value = sc.n_dynamic * len(times) / tot
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+    value = n_dyn * len(times) / tot
+    name = scenes[0].name if len(scenes) == 1 else f"{len(scenes)} scenes"
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": len(times),
             "warmup": args.warmup, "ms_per_step": 1000 * tot / len(times), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "impl": "reference", "config": workload_config(sc, args.workload),
+            "impl": "reference", "config": workload_config(scenes, args.workload),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
-                             "sample": f"{len(times)} full steps of {sc.name} on the CPU restatement"},
+                             "sample": f"{len(times)} full steps of {name} on the CPU restatement"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "p50_ms": 1000 * statistics.median(times), "p99_ms": 1000 * float(np.percentile(times, 99))}
     print(json.dumps(line), flush=True)
@@ -227,10 +277,11 @@ def run_ours(args, rank, world, local_rank):
     from implicitvelocityprojection_b200.engine import Engine, EngineOptions
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    sc = make_scene(args.workload)
+    scenes = make_scenes(args.workload)
+    n_dyn = sum(sc.n_dynamic for sc in scenes)
     opts = EngineOptions(lanes_per_particle=args.lanes,
                          particles_per_block=args.ppb or 256 // args.lanes, persistent=not args.per_phase)
-    eng = Engine([sc], device=str(dev), options=opts, divergence=True)
+    eng = Engine(scenes, device=str(dev), options=opts, divergence=True)
     eng.build()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream()
@@ -259,32 +310,34 @@ def run_ours(args, rank, world, local_rank):
     clk = clocks.stop()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     total_ms = float(sum(step_ms))
-    raw = eng.raw_stats(0)
+    raws = [eng.raw_stats(i) for i in range(len(scenes))]
     if world > 1:
         t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         total_ms = float(t.item())
-    valid = raw.failed_solves == 0 and raw.solves == args.steps and \
-        raw.max_final_density_error < sc.density_error_tol
-    value = world * sc.n_dynamic * args.steps / (total_ms / 1000.0)
+    valid = all(r.failed_solves == 0 and r.solves == args.steps and r.max_final_density_error < sc.density_error_tol
+                for r, sc in zip(raws, scenes))
+    value = world * n_dyn * args.steps / (total_ms / 1000.0)
 
     # per-kernel device time of the same workload (host-driven launches with
     # CUDA events around each kernel, after the timed region)
     prof = eng.profile_step(3)
-    pairs = int(eng.raw_stats(0).neighbour_pairs)
+    pairs = [int(r.neighbour_pairs) for r in eng_stats(eng, len(scenes))]
     if "ip_solve" in prof:
-        # gravity, persistent IP solve, advect, keys, 2 scan passes, place,
-        # order, neighbour build, static outputs
-        n_launch = 10 * args.steps
+        # gravity, viscosity (if on), persistent IP solve, advect, keys, 2
+        # scan passes, place, order, neighbour build, static outputs
+        n_launch = (10 + int("visc" in prof)) * args.steps
     else:
-        n_launch = 12 * args.steps + (raw.sum_outer_iters + args.steps) + raw.sum_outer_iters + \
-            2 * raw.sum_pcg_iters
+        so = sum(r.sum_outer_iters for r in raws)
+        n_launch = 12 * args.steps + (so + args.steps) + so + 2 * sum(r.sum_pcg_iters for r in raws)
     dom = max(prof.items(), key=lambda kv: kv[1][0])
     dom_name, (dom_ms, dom_n) = dom
     avg_s = dom_ms / dom_n / 1000.0
-    it = {"outer": raw.sum_outer_iters / args.steps, "cg": raw.sum_pcg_iters / args.steps,
-          "visc": raw.sum_visc_iters / args.steps, "visc_on": sc.viscosity_method == 1}
-    alg = algorithmic_bytes(dom_name, sc.n_dynamic, sc.n, pairs, it)
+    alg = 0.0
+    for sc, r, pr in zip(scenes, raws, pairs):
+        it = {"outer": r.sum_outer_iters / args.steps, "cg": r.sum_pcg_iters / args.steps,
+              "visc": r.sum_visc_iters / args.steps, "visc_on": sc.viscosity_method == 1}
+        alg += algorithmic_bytes(dom_name, sc.n_dynamic, sc.n, pr, it)
     peak, peak_kind = load_peaks()
     achieved = alg / avg_s / 1e9 if avg_s > 0 else 0.0
     roof = {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -292,28 +345,116 @@ def run_ours(args, rank, world, local_rank):
             "algorithmic_bytes_per_launch": alg, "avg_launch_us": avg_s * 1e6,
             "share_of_step": dom_ms / sum(v[0] for v in prof.values()),
             "kernels_ms_per_step": {k: round(v[0] / 3, 4) for k, v in prof.items()}}
+    del eng
+    torch.cuda.synchronize()
 
-    e2e = run_e2e(args, sc, dev) if (rank == 0 and not args.no_e2e) else None
+    e2e = None
+    if rank == 0 and not args.no_e2e:
+        e2e = run_e2e(args, scenes[0], dev) if len(scenes) == 1 else run_e2e_batch(args, scenes, dev, opts)
+    serial = None
+    if rank == 0 and len(scenes) > 1 and args.serial_steps > 0:
+        serial = run_serial(args, scenes, dev, opts, value / world)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(sc, args.cpu_budget_s, 200)
+        cpu = cpu_baseline(scenes, args.cpu_budget_s, 200)
     if rank == 0:
+        so = sum(r.sum_outer_iters for r in raws)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {**workload_config(sc, args.workload), "parallelism": f"replicas x{world}",
+                "config": {**workload_config(scenes, args.workload), "parallelism": f"replicas x{world}",
                            "lanes_per_particle": args.lanes,
                            "particles_per_block": opts.particles_per_block,
                            "solve": "per-phase launches" if args.per_phase else "persistent cooperative kernel"},
                 "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
-                "valid": bool(valid), "max_final_density_error": raw.max_final_density_error,
-                "outer_iters_per_step": raw.sum_outer_iters / args.steps,
-                "cg_iters_per_step": raw.sum_pcg_iters / args.steps,
-                "visc_cg_iters_per_step": raw.sum_visc_iters / args.steps,
-                "mean_neighbours": pairs / max(sc.n_dynamic, 1),
+                "valid": bool(valid), "max_final_density_error": max(r.max_final_density_error for r in raws),
+                "outer_iters_per_step": so / args.steps / len(scenes),
+                "cg_iters_per_step": sum(r.sum_pcg_iters for r in raws) / args.steps / len(scenes),
+                "visc_cg_iters_per_step": sum(r.sum_visc_iters for r in raws) / args.steps / len(scenes),
+                "mean_neighbours": sum(pairs) / max(n_dyn, 1),
                 "wall_s": wall, "gpu_launches": int(n_launch), "clocks": clk, "roofline": roof,
                 "cpu_baseline": cpu, "e2e": e2e}
+        if serial is not None:
+            line["serial"] = serial
         print(json.dumps(line), flush=True)
+
+
+def eng_stats(eng, n):
+    return [eng.raw_stats(i) for i in range(n)]
+
+
+def run_serial(args, scenes, dev, opts, batched_value):
+    """The same scenes one by one (one engine, one scene at a time), each
+    timed over a few steps after warm-up: the plain form the batched form
+    is compared with."""
+    import torch
+    from implicitvelocityprojection_b200.engine import Engine
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+    tot_s, tot_ps = 0.0, 0.0
+    for sc in scenes:
+        eng = Engine([sc], device=str(dev), options=opts)
+        eng.build()
+        for _ in range(3):
+            eng.step(1)
+        torch.cuda.synchronize()
+        ms = 0.0
+        for _ in range(args.serial_steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            eng.step(1)
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms += a.elapsed_time(b)
+        tot_s += ms / 1000.0
+        tot_ps += sc.n_dynamic * args.serial_steps
+        del eng
+    v = tot_ps / tot_s
+    return {"value": v, "unit": UNIT, "steps_per_scene": args.serial_steps,
+            "batched_over_serial": batched_value / v,
+            "form": "each scene alone in its own engine, device-timed steps summed"}
+
+
+def run_e2e_batch(args, scenes, dev, opts):
+    """Batched form end to end through Engine: every step copies all scenes'
+    x and v from pinned host memory into the bound arrays, steps, and copies
+    them back."""
+    import torch
+    from implicitvelocityprojection_b200.engine import Engine
+    eng = Engine(scenes, device=str(dev), options=opts)
+    eng.build()
+    x_d, v_d = eng.arrays["x"], eng.arrays["v"]
+    x_h = torch.empty(tuple(x_d.shape), dtype=torch.float32).pin_memory()
+    v_h = torch.empty(tuple(v_d.shape), dtype=torch.float32).pin_memory()
+    x_h.copy_(x_d)
+    v_h.copy_(v_d)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    steps = max(1, min(args.steps, args.e2e_steps))
+
+    def one():
+        x_d.copy_(x_h, non_blocking=True)
+        v_d.copy_(v_h, non_blocking=True)
+        eng.step(1)
+        x_h.copy_(x_d, non_blocking=True)
+        v_h.copy_(v_d, non_blocking=True)
+        torch.cuda.synchronize()
+
+    for _ in range(min(args.warmup, 3)):
+        one()
+    tot = 0.0
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        one()
+        tot += time.perf_counter() - t0
+    n = int(x_d.shape[0])
+    nd = sum(sc.n_dynamic for sc in scenes)
+    del eng
+    return {"value": nd * steps / tot, "unit": UNIT, "h2d_bytes_per_step": 2 * n * 12,
+            "d2h_bytes_per_step": 2 * n * 12, "steps": steps,
+            "api": "Engine(scenes).step(1) with every scene's x, v copied from/to pinned host memory every step"}
 
 
 def run_e2e(args, sc, dev):
@@ -374,6 +515,10 @@ def main():
     ap.add_argument("--cpu-budget-s", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--ref-budget-s", type=float, default=150.0,
+                    help="--impl reference: stop timing after this many seconds of CPU steps")
+    ap.add_argument("--serial-steps", type=int, default=5,
+                    help="batched workloads: steps per scene of the one-by-one comparison (0 skips it)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -51,7 +51,8 @@ class Options(ctypes.Structure):
         ("max_hist", ctypes.c_int32),
         ("use_graphs", ctypes.c_int32),
         ("persistent", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 2),
+        ("row_format", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 1),
     ]
 
 

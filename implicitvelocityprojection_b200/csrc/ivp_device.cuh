@@ -167,7 +167,8 @@ struct Dev {
     float* q;                // fk / m
     float* z;                // y / m
     // neighbour rows
-    float4* nbr;
+    float4* nbr;             // neighbour rows: float4 {J, j} entries, or float2 {j, w} when compact
+    int compact;
     int* nbr_cnt;
     int stride;
     // reductions
@@ -265,6 +266,26 @@ __device__ __forceinline__ float group_sum(float v) {
 #pragma unroll
     for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
+}
+
+// Entry k of a neighbour row in either layout: full rows hold {J_ij, j},
+// compact rows {j, w_ij} with J_ij = w_ij (x_i - x_j).
+__device__ __forceinline__ int row_j(const Dev& D, int row, int k) {
+    const size_t e = (size_t)row * D.stride + k;
+    return D.compact ? __float_as_int(reinterpret_cast<const float2*>(D.nbr)[e].x) : __float_as_int(D.nbr[e].w);
+}
+
+__device__ __forceinline__ float3 row_J(const Dev& D, int row, int k, float3 xi, int* j) {
+    const size_t e = (size_t)row * D.stride + k;
+    if (!D.compact) {
+        const float4 v = D.nbr[e];
+        *j = __float_as_int(v.w);
+        return f3(v);
+    }
+    const float2 v = reinterpret_cast<const float2*>(D.nbr)[e];
+    *j = __float_as_int(v.x);
+    const float3 r = sub3(xi, f3(D.xm[*j]));
+    return make_float3(__fmul_rn(v.y, r.x), __fmul_rn(v.y, r.y), __fmul_rn(v.y, r.z));
 }
 
 // One 32-byte CG record (two float4, 32-byte aligned) in a single 256-bit

@@ -454,6 +454,7 @@ int validate(const ivp_scene_desc* sc, int n, const ivp_options* o) {
             return IVP_ERR_BAD_ARG;
     }
     if (o->list_stride <= 0 || (o->list_stride & 1) || o->max_hist <= 0) return IVP_ERR_BAD_ARG;
+    if (o->row_format < 0 || o->row_format > 2) return IVP_ERR_BAD_ARG;
     long expect = 0;
     for (int s = 0; s < n; ++s) {
         const ivp_scene_desc& d = sc[s];
@@ -476,6 +477,7 @@ struct Plan {
     std::vector<int4> tiles;
     std::vector<int4> segs;
     int n_total = 0, n_dyn = 0, n_keys = 0, scan_blocks = 0;
+    bool compact = false;  // neighbour rows as {j, w} (8 B entries)
     size_t off[48];
     Layout lay;
 };
@@ -552,6 +554,10 @@ void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
     }
     P.n_total = s_begin;
     P.n_dyn = row_base;
+    // compact rows halve the list memory; they cost one more gather per
+    // pair, which outweighs the halved list stream on B200, so the default
+    // is full rows
+    P.compact = o->row_format == 2;
     P.n_keys = key_base;
     P.scan_blocks = std::max(1, (P.n_keys + SCAN_TILE - 1) / SCAN_TILE);
     const size_t N = (size_t)P.n_total, S = (size_t)n, NT = std::max<size_t>(P.tiles.size(), 1);
@@ -584,7 +590,7 @@ void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
     P.off[i++] = L.add(sizeof(float) * N);                  // 24 y
     P.off[i++] = L.add(sizeof(float) * N);                  // 25 s
     P.off[i++] = L.add(sizeof(float) * N);                  // 26 fk
-    P.off[i++] = L.add(sizeof(float4) * (size_t)P.n_dyn * (size_t)o->list_stride);  // 27 nbr
+    P.off[i++] = L.add((P.compact ? sizeof(float2) : sizeof(float4)) * (size_t)P.n_dyn * (size_t)o->list_stride);  // 27 nbr
     P.off[i++] = L.add(sizeof(int) * std::max<size_t>((size_t)P.n_dyn, 1));       // 28 nbr_cnt
     P.off[i++] = L.add(2 * sizeof(double) * NT);            // 29 partial (two per tile)
     P.off[i++] = L.add(sizeof(int) * S);                    // 30 scene_counter
@@ -719,6 +725,7 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
     D.n_tiles = e->n_tiles;
     D.n_keys = e->n_keys;
     D.stride = opt->list_stride;
+    D.compact = P.compact ? 1 : 0;
     D.hist_len = opt->max_hist;
     D.n_total = e->n_total;
 
@@ -755,7 +762,7 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
         int dev = 0, coop = 0, nsm = 0, per_sm = 0;
         KernelSet K;
         kernel_set(e->G, e->BLOCK, &K);
-        e->coop_smem = (size_t)n_scenes * (2 * sizeof(double) + sizeof(SceneCtl));
+        e->coop_smem = (size_t)n_scenes * (2 * sizeof(double) + sizeof(SceneCtl) + 3 * sizeof(int)) + sizeof(int);
         if (cudaGetDevice(&dev) == cudaSuccess &&
             cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) == cudaSuccess && coop &&
             cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess &&

@@ -562,6 +562,7 @@ __global__ void __launch_bounds__(256, 4) k_nbr_build(const Dev D) {
         // phase 2: dense over the hits -- J_ij = m_j grad W_ij, density, Aii
         const int row = P.row_base + (i - P.s_begin);
         float4* out = D.nbr + (size_t)row * D.stride;
+        float2* out2 = reinterpret_cast<float2*>(D.nbr) + (size_t)row * D.stride;
         float rho = 0.0f, aii = 0.0f;
         float3 jii = make_float3(0.0f, 0.0f, 0.0f);
         for (int k = lane; k < cnt; k += G) {
@@ -576,8 +577,12 @@ __global__ void __launch_bounds__(256, 4) k_nbr_build(const Dev D) {
             const float sg = -spk * (t * t);
             const float ir = __frcp_rn(rc);
             const float mj = xj4.w;
-            const float3 J = make_float3(mj * (sg * (r.x * ir)), mj * (sg * (r.y * ir)), mj * (sg * (r.z * ir)));
-            out[k] = make_float4(J.x, J.y, J.z, __int_as_float(j));
+            // J = w (x_i - x_j): the compact rows keep w and recompute J
+            // from the positions with the same three products
+            const float w = mj * (sg * ir);
+            const float3 J = make_float3(__fmul_rn(w, r.x), __fmul_rn(w, r.y), __fmul_rn(w, r.z));
+            if (D.compact) out2[k] = make_float2(__int_as_float(j), w);
+            else out[k] = make_float4(J.x, J.y, J.z, __int_as_float(j));
             rho += mj * cubic_Wq(rn * inv_h, ck);
             if (j < dyn_end) aii += dot3(J, J) * __frcp_rn(mj);
             jii = sub3(jii, J);
@@ -634,7 +639,6 @@ __global__ void __launch_bounds__(BLOCK) k_density(const Dev D) {
     const bool valid = i < tile.z;
     const int row = tile.w + g;
     const int cnt = valid ? D.nbr_cnt[row] : 0;
-    const float4* nb = D.nbr + (size_t)row * D.stride;
     float3 xi = make_float3(0.f, 0.f, 0.f);
     int pi = 0;
     if (valid) {
@@ -643,7 +647,7 @@ __global__ void __launch_bounds__(BLOCK) k_density(const Dev D) {
     }
     float acc = 0.0f;
     for (int k = lane; k < cnt; k += G) {
-        const int j = __float_as_int(nb[k].w);
+        const int j = row_j(D, row, k);
         const int pj = D.pid[j];
         const float3 r = sub3(xi, make_float3(D.x[3 * pj], D.x[3 * pj + 1], D.x[3 * pj + 2]));
         acc += D.m[pj] * cubic_W(sqrtf(dot3(r, r)), P.h, P.cubic_k);
@@ -670,13 +674,11 @@ __global__ void __launch_bounds__(BLOCK) k_aii(const Dev D) {
     const bool valid = i < tile.z;
     const int row = tile.w + g;
     const int cnt = valid ? D.nbr_cnt[row] : 0;
-    const float4* nb = D.nbr + (size_t)row * D.stride;
     const float4 xi4 = valid ? D.xm[i] : make_float4(0.f, 0.f, 0.f, 1.f);
     float aii = 0.0f, jx = 0.0f, jy = 0.0f, jz = 0.0f;
     for (int k = lane; k < cnt; k += G) {
-        const float4 e = nb[k];
-        const int j = __float_as_int(e.w);
-        const float3 J = f3(e);
+        int j;
+        const float3 J = row_J(D, row, k, f3(xi4), &j);
         if (j < P.s_dyn_end) aii += dot3(J, J) * __frcp_rn(D.xm[j].w);
         jx -= J.x;
         jy -= J.y;
@@ -826,18 +828,44 @@ __device__ __forceinline__ void pair_entry(const float4& e, bool in, int self, i
     J = (in && ok) ? f3(e) : make_float3(0.f, 0.f, 0.f);
 }
 
-// k0 = 2 * lane + (batch start)
+// k0 = 2 * lane + (batch start); xi is the row particle's position (the
+// compact rows recompute J_ij = w_ij (x_i - x_j) from it).
 template <int G>
-__device__ __forceinline__ bool load_pairs(const float4* __restrict__ nb, int k0, int cnt, int self, int lo, int hi,
-                                           PairBatch& b) {
+__device__ __forceinline__ bool load_pairs(const Dev& D, int row, float3 xi, int k0, int cnt, int self, int lo,
+                                           int hi, PairBatch& b) {
     bool bad = false;
+    if (!D.compact) {
+        const float4* __restrict__ nb = D.nbr + (size_t)row * D.stride;
 #pragma unroll
-    for (int u = 0; u < PU / 2; ++u) {
-        const int k = k0 + u * 2 * G;
-        float4 e0 = make_float4(0.f, 0.f, 0.f, 0.f), e1 = e0;
-        if (k < cnt) ld_rec_nc(nb + k, e0, e1);
-        pair_entry(e0, k < cnt, self, lo, hi, b.j[2 * u], b.J[2 * u], bad);
-        pair_entry(e1, k + 1 < cnt, self, lo, hi, b.j[2 * u + 1], b.J[2 * u + 1], bad);
+        for (int u = 0; u < PU / 2; ++u) {
+            const int k = k0 + u * 2 * G;
+            float4 e0 = make_float4(0.f, 0.f, 0.f, 0.f), e1 = e0;
+            if (k < cnt) ld_rec_nc(nb + k, e0, e1);
+            pair_entry(e0, k < cnt, self, lo, hi, b.j[2 * u], b.J[2 * u], bad);
+            pair_entry(e1, k + 1 < cnt, self, lo, hi, b.j[2 * u + 1], b.J[2 * u + 1], bad);
+        }
+    } else {
+        const float4* __restrict__ nb =
+            reinterpret_cast<const float4*>(reinterpret_cast<const float2*>(D.nbr) + (size_t)row * D.stride);
+#pragma unroll
+        for (int u = 0; u < PU / 2; ++u) {
+            const int k = k0 + u * 2 * G;
+            float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (k < cnt) e = __ldg(nb + (k >> 1));  // entries k, k+1: {j, w, j, w}
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int jj = __float_as_int(h ? e.z : e.x);
+                const float w = h ? e.w : e.y;
+                const bool in = k + h < cnt;
+                const bool ok = jj >= lo && jj < hi;
+                bad |= in && !ok;
+                const int j = (in && ok) ? jj : self;
+                const float3 r = sub3(xi, f3(__ldg(D.xm + j)));
+                b.j[2 * u + h] = j;
+                b.J[2 * u + h] = (in && ok) ? make_float3(__fmul_rn(w, r.x), __fmul_rn(w, r.y), __fmul_rn(w, r.z))
+                                            : make_float3(0.f, 0.f, 0.f);
+            }
+        }
     }
     return bad;
 }
@@ -875,7 +903,6 @@ __device__ __forceinline__ double pack_tile(const Dev& D, const SceneParams& P, 
     const float4* src = (upd && ((it - 1) & 1)) ? D.d1 : D.d0;
     float4* dst = (it & 1) ? D.d1 : D.d0;
     const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
-    const float4* nb = D.nbr + (size_t)T.row * D.stride;
     float3 xi = make_float3(0.f, 0.f, 0.f), di = xi;
     if (T.valid) {
         xi = f3(D.xm[T.i]);
@@ -887,7 +914,7 @@ __device__ __forceinline__ double pack_tile(const Dev& D, const SceneParams& P, 
     const int self = T.valid ? T.i : P.s_begin;
     for (int k0 = 2 * T.lane; k0 < cnt; k0 += G * PU) {
         PairBatch b;
-        bad |= load_pairs<G>(nb, k0, cnt, self, P.s_begin, P.s_end, b);
+        bad |= load_pairs<G>(D, T.row, xi, k0, cnt, self, P.s_begin, P.s_end, b);
 #pragma unroll
         for (int u = 0; u < PU; ++u) {
             const int j = b.j[u];
@@ -920,7 +947,6 @@ __device__ __forceinline__ double pack_tile(const Dev& D, const SceneParams& P, 
 template <int G>
 __device__ __forceinline__ double rhs_tile(const Dev& D, const SceneParams& P, const TileCtx& T) {
     const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
-    const float4* nb = D.nbr + (size_t)T.row * D.stride;
     float3 xi = make_float3(0.f, 0.f, 0.f);
     float fki = 0.0f, mi = 0.0f;
     if (T.valid) {
@@ -934,7 +960,7 @@ __device__ __forceinline__ double rhs_tile(const Dev& D, const SceneParams& P, c
     const int self = T.valid ? T.i : P.s_begin;
     for (int k0 = 2 * T.lane; k0 < cnt; k0 += G * PU) {
         PairBatch b;
-        bad |= load_pairs<G>(nb, k0, cnt, self, P.s_begin, P.s_end, b);
+        bad |= load_pairs<G>(D, T.row, xi, k0, cnt, self, P.s_begin, P.s_end, b);
 #pragma unroll
         for (int u = 0; u < PU; ++u) {
             const float wgt = fki + mi * D.q[b.j[u]];
@@ -970,7 +996,6 @@ __device__ __forceinline__ double cga_tile(const Dev& D, const SceneParams& P, c
     const float4* cc = (cg_it & 1) ? D.cg1 : D.cg0;  // {r, p_prev}
     float4* cn = (cg_it & 1) ? D.cg0 : D.cg1;
     const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
-    const float4* nb = D.nbr + (size_t)T.row * D.stride;
     float3 xi = make_float3(0.f, 0.f, 0.f), pi = xi;
     float mi = 0.0f;
     if (T.valid) {
@@ -985,7 +1010,7 @@ __device__ __forceinline__ double cga_tile(const Dev& D, const SceneParams& P, c
     const int self = T.valid ? T.i : P.s_begin;
     for (int k0 = 2 * T.lane; k0 < cnt; k0 += G * PU) {
         PairBatch b;
-        bad |= load_pairs<G>(nb, k0, cnt, self, P.s_begin, P.s_end, b);
+        bad |= load_pairs<G>(D, T.row, xi, k0, cnt, self, P.s_begin, P.s_end, b);
 #pragma unroll
         for (int u = 0; u < PU; ++u) {
             const int j = b.j[u];
@@ -1017,7 +1042,6 @@ __device__ __forceinline__ double cgb_tile(const Dev& D, const SceneParams& P, c
     const float4* cc = (cg_it & 1) ? D.cg1 : D.cg0;  // own r
     float4* cn = (cg_it & 1) ? D.cg0 : D.cg1;        // own p; receives the new r
     const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
-    const float4* nb = D.nbr + (size_t)T.row * D.stride;
     float3 xi = make_float3(0.f, 0.f, 0.f);
     float mi = 0.0f, yi = 0.0f;
     if (T.valid) {
@@ -1031,7 +1055,7 @@ __device__ __forceinline__ double cgb_tile(const Dev& D, const SceneParams& P, c
     const int self = T.valid ? T.i : P.s_begin;
     for (int k0 = 2 * T.lane; k0 < cnt; k0 += G * PU) {
         PairBatch b;
-        bad |= load_pairs<G>(nb, k0, cnt, self, P.s_begin, P.s_end, b);
+        bad |= load_pairs<G>(D, T.row, xi, k0, cnt, self, P.s_begin, P.s_end, b);
 #pragma unroll
         for (int u = 0; u < PU; ++u) {
             const float wgt = yi + mi * D.z[b.j[u]];
@@ -1068,7 +1092,6 @@ template <int G>
 __device__ __forceinline__ void div_tile(const Dev& D, const SceneParams& P, const TileCtx& T, int outer_it) {
     const float4* dc = (outer_it & 1) ? D.d1 : D.d0;
     const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
-    const float4* nb = D.nbr + (size_t)T.row * D.stride;
     const float s = P.inv_dt;
     float3 xi = make_float3(0.f, 0.f, 0.f), vi = xi;
     if (T.valid) {
@@ -1077,9 +1100,10 @@ __device__ __forceinline__ void div_tile(const Dev& D, const SceneParams& P, con
     }
     float acc = 0.0f;
     for (int k = T.lane; k < cnt; k += G) {
-        const float4 e = __ldg(nb + k);
-        const float3 vj = scale3(s, f3(dc[__float_as_int(e.w)]));
-        acc += dot3(sub3(vi, vj), f3(e));
+        int j;
+        const float3 J = row_J(D, T.row, k, xi, &j);
+        const float3 vj = scale3(s, f3(dc[j]));
+        acc += dot3(sub3(vi, vj), J);
     }
     acc = group_sum<G>(acc);
     if (T.valid && T.lane == 0 && D.div_out) D.div_out[D.pid[T.i]] = acc > 0.0f ? acc : 0.0f;
@@ -1102,7 +1126,6 @@ __device__ __forceinline__ float visc_factor(const Dev& D, const SceneParams& P,
 template <int G>
 __device__ __forceinline__ double visc_setup_tile(const Dev& D, const SceneParams& P, const TileCtx& T) {
     const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
-    const float4* nb = D.nbr + (size_t)T.row * D.stride;
     const bool fluid = T.valid && D.rflu[T.i] != 0.0f;
     float3 xi = make_float3(0.f, 0.f, 0.f), vi = xi;
     if (T.valid) {
@@ -1120,7 +1143,7 @@ __device__ __forceinline__ double visc_setup_tile(const Dev& D, const SceneParam
     const int self = T.valid ? T.i : P.s_begin;
     for (int k0 = 2 * T.lane; k0 < (fluid ? cnt : 0); k0 += G * PU) {
         PairBatch b;
-        bad |= load_pairs<G>(nb, k0, cnt, self, P.s_begin, P.s_end, b);
+        bad |= load_pairs<G>(D, T.row, xi, k0, cnt, self, P.s_begin, P.s_end, b);
 #pragma unroll
         for (int u = 0; u < PU; ++u) {
             const int j = b.j[u];
@@ -1188,7 +1211,6 @@ __device__ __forceinline__ double visc_a_tile(const Dev& D, const SceneParams& P
     const float4* cc = (it & 1) ? D.cg1 : D.cg0;  // {z | 1/rho, p_prev}
     float4* cn = (it & 1) ? D.cg0 : D.cg1;
     const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
-    const float4* nb = D.nbr + (size_t)T.row * D.stride;
     const bool fluid = T.valid && D.rflu[T.i] != 0.0f;
     float3 xi = make_float3(0.f, 0.f, 0.f), pi = xi;
     if (T.valid) {
@@ -1202,7 +1224,7 @@ __device__ __forceinline__ double visc_a_tile(const Dev& D, const SceneParams& P
     const int self = T.valid ? T.i : P.s_begin;
     for (int k0 = 2 * T.lane; k0 < (fluid ? cnt : 0); k0 += G * PU) {
         PairBatch b;
-        bad |= load_pairs<G>(nb, k0, cnt, self, P.s_begin, P.s_end, b);
+        bad |= load_pairs<G>(D, T.row, xi, k0, cnt, self, P.s_begin, P.s_end, b);
 #pragma unroll
         for (int u = 0; u < PU; ++u) {
             const int j = b.j[u];
@@ -1546,6 +1568,10 @@ struct Phaser {
     int* any_sh;
     long long phases;
 
+    int* act_sh;   // [n_scenes + 1] exclusive prefix of the phase's active tile counts
+    int* tb_sh;    // [n_scenes] first tile of each scene
+    int* tn_sh;    // [n_scenes] tile count of each scene
+
     __device__ Phaser(const Dev& d, double* dyn, double* red, int* flag, int* anyp)
         : D(d), red_sh(red), flag_sh(flag), any_sh(anyp), phases(0) {
         t0 = (int)(((long long)blockIdx.x * D.n_tiles) / gridDim.x);
@@ -1553,6 +1579,48 @@ struct Phaser {
         sum_sh = dyn;
         sum_sh2 = dyn + D.n_scenes;
         sc_sh = reinterpret_cast<SceneCtl*>(dyn + 2 * D.n_scenes);
+        act_sh = reinterpret_cast<int*>(sc_sh + D.n_scenes);
+        tb_sh = act_sh + D.n_scenes + 1;
+        tn_sh = tb_sh + D.n_scenes;
+        for (int s = threadIdx.x; s < D.n_scenes; s += BLOCK) {
+            tb_sh[s] = D.scenes[s].tile_begin;
+            tn_sh[s] = D.scenes[s].tile_end - D.scenes[s].tile_begin;
+        }
+        __syncthreads();
+    }
+
+    // Exclusive prefix of the tile counts of the scenes active in `kind`
+    // (warp 0, 32 scenes per pass).
+    __device__ void active_prefix(int kind) {
+        if (threadIdx.x < 32) {
+            const int lane = threadIdx.x;
+            int carry = 0;
+            for (int base = 0; base < D.n_scenes; base += 32) {
+                const int s = base + lane;
+                const int v = (s < D.n_scenes && phase_active(sc_sh[s], kind)) ? tn_sh[s] : 0;
+                int inc = v;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int u = __shfl_up_sync(0xffffffffu, inc, o);
+                    if (lane >= o) inc += u;
+                }
+                if (s < D.n_scenes) act_sh[s] = carry + inc - v;
+                carry += __shfl_sync(0xffffffffu, inc, 31);
+            }
+            if (lane == 0) act_sh[D.n_scenes] = carry;
+        }
+        __syncthreads();
+    }
+
+    // Last scene s with act_sh[s] <= a: the active scene holding active tile a.
+    __device__ int scene_of(int a) const {
+        int lo = 0, hi = D.n_scenes;  // act_sh[lo] <= a < act_sh[hi]
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (act_sh[mid] <= a) lo = mid;
+            else hi = mid;
+        }
+        return lo;
     }
 
     __device__ bool barrier(int kind) {
@@ -1578,12 +1646,21 @@ struct Phaser {
 
     // VISC selects the phase family compiled into this kernel (each
     // persistent kernel keeps its own register budget)
+    // The phase's active tiles (those of the scenes active in `kind`) are
+    // split evenly over the grid, so scenes that converged early leave no CTA
+    // idle while others work through a converging scene's tiles.
     template <bool VISC>
     __device__ bool run(int kind) {
-        for (int t = t0; t < t1; ++t) {
+        active_prefix(kind);
+        const int A = act_sh[D.n_scenes];
+        const int a0 = (int)(((long long)blockIdx.x * A) / gridDim.x);
+        const int a1 = (int)(((long long)(blockIdx.x + 1) * A) / gridDim.x);
+        int sc = a0 < a1 ? scene_of(a0) : 0;
+        for (int a = a0; a < a1; ++a) {
+            while (a >= act_sh[sc + 1]) ++sc;
+            const int t = tb_sh[sc] + (a - act_sh[sc]);
             const TileCtx T = tile_ctx<G>(D, t);
             const SceneCtl& C = sc_sh[T.sc];
-            if (!phase_active(C, kind)) continue;
             const SceneParams& P = D.scenes[T.sc];
             double part, part2 = 0.0;
             if constexpr (VISC) {
@@ -1750,7 +1827,7 @@ __global__ void k_export(const Dev D, int scene, int* count, int* ids, int cache
     const int p = D.pid[i] - P.p_begin;
     const int cnt = D.nbr_cnt[row];
     count[p] = cnt;
-    for (int k = 0; k < cnt && k < cache; ++k) ids[(size_t)p * cache + k] = D.pid[__float_as_int(D.nbr[(size_t)row * D.stride + k].w)] - P.p_begin;
+    for (int k = 0; k < cnt && k < cache; ++k) ids[(size_t)p * cache + k] = D.pid[row_j(D, row, k)] - P.p_begin;
 }
 
 }  // namespace ivp

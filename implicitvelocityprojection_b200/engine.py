@@ -31,6 +31,7 @@ class EngineOptions:
     max_hist: int = 128
     use_graphs: bool = True
     persistent: bool = True
+    row_format: int = 0  # 0 auto, 1 full {J, j}, 2 compact {j, w}
 
     def to_c(self) -> _lib.Options:
         o = _lib.Options()
@@ -40,6 +41,7 @@ class EngineOptions:
         o.max_hist = self.max_hist
         o.use_graphs = int(self.use_graphs)
         o.persistent = int(self.persistent)
+        o.row_format = int(self.row_format)
         return o
 
 

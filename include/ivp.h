@@ -70,7 +70,10 @@ typedef struct {
     int32_t use_graphs;           /* 1: whole steps as CUDA graphs (device-side control, no host sync) */
     int32_t persistent;           /* 1: the IP solve as one persistent cooperative kernel with grid barriers;
                                      0: one launch per phase, loops as conditional graph nodes */
-    int32_t reserved[2];
+    int32_t row_format;           /* neighbour-row entries: 0 default (= 1), 1 full {m_j gradW_ij, j}
+                                     (16 B), 2 compact {j, w_ij} (8 B, gradient rebuilt from the
+                                     positions: half the list memory, slower); bit-identical results */
+    int32_t reserved[1];
 } ivp_options;
 
 /* Device arrays in the reference's layout and particle order
