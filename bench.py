@@ -62,6 +62,8 @@ def make_scenes(name: str):
     if name.startswith("batch"):
         n = int(name[5:] or 64)
         return S.batch_mix(n_scenes=n)
+    if name == "served":  # a sample of the request stream's scenes
+        return [r.scene for r in S.request_stream(max_requests=8)]
     return [make_scene(name)]
 
 
@@ -379,6 +381,52 @@ def run_ours(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+def run_served(args, rank, world, local_rank):
+    """Served form: Poisson request stream (column collapses and dam breaks,
+    fluid counts log-uniform 2,048-262,144, steps U[100, 2000]) through the
+    continuous-batching server on virtual time (idle gaps skipped)."""
+    import torch
+    from implicitvelocityprojection_b200 import scenes as S
+    from implicitvelocityprojection_b200.engine import EngineOptions
+    from implicitvelocityprojection_b200.serve import Server
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    reqs = S.request_stream(rate=args.served_rate, duration_s=args.served_duration, seed=rank)
+    opts = EngineOptions(lanes_per_particle=args.lanes, particles_per_block=args.ppb or 256 // args.lanes)
+    # warm-up: one small request through the same path (library, graphs, allocator)
+    Server(device=str(dev), options=opts, chunk_steps=args.chunk_steps, keep_state=False).run(
+        [S.Request(arrival_s=0.0, scene=S.random_column(4096, 2.0, seed=99), steps=3)])
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    rep = Server(device=str(dev), options=opts, chunk_steps=args.chunk_steps, keep_state=False,
+                 hbm_budget_bytes=args.hbm_budget_gb * 1e9).run(reqs)
+    clk = clocks.stop()
+    sm = rep.summary()
+    tot = torch.tensor([sm["particle_steps"], rep.makespan_s], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(tot[:1])
+        mk = tot[1:].clone()
+        torch.distributed.all_reduce(mk, op=torch.distributed.ReduceOp.MAX)
+        tot[1] = mk[0]
+    value = float(tot[0].item()) / float(tot[1].item())
+    if rank == 0:
+        n_dyn = [r.scene.n_dynamic for r in reqs]
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": int(sm["particle_steps"]),
+                "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": f"served: Poisson {args.served_rate}/s for {args.served_duration} s, "
+                                       "column or dam break 50/50, fluid log-uniform 2,048-262,144, steps U[100,2000]",
+                           "requests": len(reqs), "fluid_mean": float(np.mean(n_dyn)),
+                           "chunk_steps": args.chunk_steps, "hbm_budget_gb": args.hbm_budget_gb,
+                           "clock": "virtual (busy time, idle gaps skipped)", "parallelism": f"replicas x{world}"},
+                "served": sm, "p50_ms": 1000 * sm["latency_p50_s"], "p99_ms": 1000 * sm["latency_p99_s"],
+                "valid": sm["failed"] == 0 and sm["rejected"] == 0, "clocks": clk,
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                        "api": "Server.run(requests): scenes uploaded on admission, results read back on completion"}}
+        print(json.dumps(line), flush=True)
+
+
 def eng_stats(eng, n):
     return [eng.raw_stats(i) for i in range(n)]
 
@@ -517,6 +565,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ref-budget-s", type=float, default=150.0,
                     help="--impl reference: stop timing after this many seconds of CPU steps")
+    ap.add_argument("--served-rate", type=float, default=4.0, help="served: requests per second")
+    ap.add_argument("--served-duration", type=float, default=30.0, help="served: seconds of arrivals")
+    ap.add_argument("--chunk-steps", type=int, default=50, help="served: steps between re-plans")
+    ap.add_argument("--hbm-budget-gb", type=float, default=150.0, help="served: admission budget")
     ap.add_argument("--serial-steps", type=int, default=5,
                     help="batched workloads: steps per scene of the one-by-one comparison (0 skips it)")
     args = ap.parse_args()
@@ -535,7 +587,10 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                              device_id=torch.device("cuda", local_rank))
     try:
-        run_ours(args, rank, world, local_rank)
+        if args.workload == "served":
+            run_served(args, rank, world, local_rank)
+        else:
+            run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch

@@ -68,6 +68,20 @@ def scene_desc(sc, offset: int) -> _lib.SceneDesc:
     return d
 
 
+def workspace_bytes(scenes: Sequence, options: Optional["EngineOptions"] = None) -> int:
+    """Device workspace an Engine over `scenes` allocates (ivp_workspace_bytes)."""
+    L = _lib.load()
+    descs = (_lib.SceneDesc * len(scenes))()
+    off = 0
+    for i, sc in enumerate(scenes):
+        descs[i] = scene_desc(sc, off)
+        off += sc.n
+    opt = (options or EngineOptions()).to_c()
+    nbytes = ctypes.c_size_t(0)
+    check(L.ivp_workspace_bytes(descs, len(scenes), ctypes.byref(opt), ctypes.byref(nbytes)), "ivp_workspace_bytes")
+    return int(nbytes.value)
+
+
 @dataclasses.dataclass
 class Stats:
     """Per-scene result of the last IP solve (names of pressure_base.py:331-339)."""

@@ -1,0 +1,105 @@
+"""Served form: the request loop's scheduling on CPU with a stand-in engine,
+and on the GPU bit-identity of a served request with the scene run alone."""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from implicitvelocityprojection_b200 import scenes as S
+from implicitvelocityprojection_b200.serve import Server
+
+
+class _Stats:
+    status = 0
+    failed_solves = 0
+    last_failure = 0
+
+
+class FakeEngine:
+    """Steps every scene by adding the step count to x (so a test can check
+    that state is carried exactly across rebuilds)."""
+    live = 0
+    peak = 0
+    built = []
+
+    def __init__(self, scenes):
+        self.scenes = [dataclasses.replace(s, x=s.x.copy(), v=s.v.copy()) for s in scenes]
+        FakeEngine.built.append([s.name for s in scenes])
+
+    def build(self):
+        pass
+
+    def step(self, n):
+        for s in self.scenes:
+            s.x = s.x + np.float32(n)
+
+    def raw_stats(self, i):
+        return _Stats()
+
+    def get(self, name, i):
+        return getattr(self.scenes[i], name).copy()
+
+    def reset_counters(self):
+        pass
+
+
+def _req(t, n, steps, name):
+    sc = S.Scene(x=np.zeros((n, 3), np.float32), v=np.zeros((n, 3), np.float32),
+                 is_dynamic=np.ones(n, np.int32), material=np.ones(n, np.int32),
+                 density0=np.full(n, 1000.0, np.float32), particle_radius=0.01,
+                 domain_size=np.array([1.0, 1.0, 1.0], np.float32), name=name)
+    return S.Request(arrival_s=t, scene=sc, steps=steps)
+
+
+def test_fcfs_admission_budget_and_state_carry():
+    reqs = [_req(0.0, 10, 7, "a"), _req(0.0, 20, 12, "b"), _req(0.0, 15, 5, "c"), _req(0.5, 5, 9, "d")]
+    budget = 35  # footprint = particle count: a + b fit, c waits
+    FakeEngine.built = []
+    srv = Server(engine_factory=FakeEngine, footprint=lambda sc: sc.n, hbm_budget_bytes=budget, chunk_steps=4)
+    rep = srv.run(reqs)
+    assert [r.rid for r in rep.results] == [0, 1, 2, 3]
+    for r, q in zip(rep.results, reqs):
+        assert r.status == 0 and r.steps == q.steps
+        assert np.all(r.x == np.float32(q.steps)), (r.rid, r.x[0])  # exact across rebuilds
+    # never more than the budget resident, and c (first in line) is admitted before d
+    for names in FakeEngine.built:
+        assert sum({"a": 10, "b": 20, "c": 15, "d": 5}[n] for n in names) <= budget
+    first = {n: i for i, names in reversed(list(enumerate(FakeEngine.built))) for n in names}
+    assert first["c"] <= first["d"]
+    s = rep.summary()
+    assert s["completed"] == 4 and s["rejected"] == 0 and s["particle_steps"] == 10 * 7 + 20 * 12 + 15 * 5 + 5 * 9
+
+
+def test_oversized_request_rejected_and_idle_gaps_skipped():
+    reqs = [_req(0.0, 50, 3, "big"), _req(100.0, 5, 3, "late")]
+    srv = Server(engine_factory=FakeEngine, footprint=lambda sc: sc.n, hbm_budget_bytes=10, chunk_steps=2)
+    rep = srv.run(reqs)
+    assert rep.rejected == 1
+    assert len(rep.results) == 1 and rep.results[0].rid == 1
+    assert rep.results[0].admit_s >= 100.0  # virtual clock jumped to the arrival
+
+
+def test_workspace_footprint_grows_with_particles():
+    from implicitvelocityprojection_b200.engine import workspace_bytes
+    small = workspace_bytes([S.random_column(3000, 2.0, seed=1)])
+    big = workspace_bytes([S.random_column(30000, 2.0, seed=1)])
+    assert 0 < small < big
+
+
+@pytest.mark.gpu
+def test_served_request_equals_scene_alone():
+    """Requests joining and leaving at chunk boundaries (engine rebuilt each
+    time) end bit-identical to each scene stepped alone."""
+    from implicitvelocityprojection_b200.engine import Engine
+    scs = [S.random_column(2500, 1.5, seed=41), S.small_dam_break(3000, seed=42), S.random_column(4000, 3.0, seed=43)]
+    steps = [9, 6, 8]
+    reqs = [S.Request(arrival_s=t, scene=sc, steps=n) for t, sc, n in zip((0.0, 0.0, 1e-4), scs, steps)]
+    rep = Server(chunk_steps=3).run(reqs)
+    assert rep.rebuilds >= 2
+    for r, sc, n in zip(rep.results, scs, steps):
+        assert r.status == 0
+        alone = Engine([sc])
+        alone.build()
+        alone.step(n)
+        assert np.array_equal(r.x, alone.get("x")), r.rid
+        assert np.array_equal(r.v, alone.get("v")), r.rid
