@@ -709,17 +709,288 @@ int orc_weiler18_solve(int n, const orc_visc_params* V, const float* x, float* v
     return it;
 }
 
+/* ----------------------------------------- Jeske 2023 surface tension */
+
+typedef struct {
+    float sigma;       /* surfaceTensionCoeff */
+    float dt;
+    float d;           /* particle diameter */
+    float h_st;        /* jeske23.py:455: 2 d */
+    int cache;
+    int max_iter;      /* jeske23.py:470 */
+    double tol;        /* jeske23.py:471, absolute on r.r */
+    int fast;
+} orc_st_params;
+
+/* compute_Wst (jeske23.py:26-44): theta W_cubic(max(r, d); h_st), theta = 10/7 */
+static float st_W(float r, float d, float h) {
+    float theta = 10.0f / 7.0f;
+    float rc = r > d ? r : d;
+    float q = rc / h;
+    float norm = 8.0f / (3.14159265358979f * h * h * h);
+    float fq = 0.0f;
+    if (q <= 0.5f) {
+        fq = 1.0f - 6.0f * q * q + 6.0f * q * q * q;
+    } else if (q <= 1.0f) {
+        float t = 1.0f - q;
+        fq = 2.0f * t * t * t;
+    }
+    return theta * norm * fq;
+}
+
+/* compute_grad_Wst (jeske23.py:47-67): zero for r <= d, else theta grad W_cubic */
+static void st_gradW(const float* xij, float r, float d, float h, float* o) {
+    o[0] = o[1] = o[2] = 0.0f;
+    if (r <= d || r < 1.0e-12f) return;
+    float q = r / h;
+    if (q > 1.0f) return;
+    float theta = 10.0f / 7.0f;
+    float norm = 8.0f / (3.14159265358979f * h * h * h);
+    float fpq;
+    if (q <= 0.5f) {
+        fpq = -12.0f * q + 18.0f * q * q;
+    } else {
+        float t = 1.0f - q;
+        fpq = -6.0f * t * t;
+    }
+    float s = theta * norm * (1.0f / h) * fpq;
+    for (int c = 0; c < 3; ++c) o[c] = s * (xij[c] / r);
+}
+
+/* compute_divergence_jeske23 (jeske23.py:74-115): m_j v_ij . gradW_ij over fluid j */
+static void st_divergence(int n, const orc_st_params* S, const float* v, const float* m, const int* material,
+                          const int* dyn, const int* count, const int* ids, const float* gradW, float* div) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) {
+        if (!dyn[i] || material[i] != 1) {
+            div[i] = 0.0f;
+            continue;
+        }
+        float acc = 0.0f;
+        int cnt = clamp_cnt(count[i], S->cache);
+        for (int k = 0; k < cnt; ++k) {
+            long b = (long)i * S->cache + k;
+            int j = ids[b];
+            if (material[j] != 1) continue;
+            float vij[3] = {v[3 * i] - v[3 * j], v[3 * i + 1] - v[3 * j + 1], v[3 * i + 2] - v[3 * j + 2]};
+            acc = acc + m[j] * dot3(vij, gradW + 3 * b);
+        }
+        div[i] = acc;
+    }
+}
+
+/* compute_g_tilde_jeske23 (jeske23.py:118-188): per fluid pair
+ * g~ = W / rho_bar + dt (gradW . v_ij / rho_bar - W / (2 rho_bar^2) (div_i + div_j)) */
+static void st_g_tilde(int n, const orc_st_params* S, const float* x, const float* v, const float* density,
+                       const int* material, const int* dyn, const int* count, const int* ids, const float* div,
+                       float* gt) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) {
+        int cnt = clamp_cnt(count[i], S->cache);
+        float* g = gt + (size_t)i * S->cache;
+        if (!dyn[i] || material[i] != 1) {
+            for (int k = 0; k < cnt; ++k) g[k] = 0.0f;
+            continue;
+        }
+        for (int k = 0; k < cnt; ++k) {
+            int j = ids[(size_t)i * S->cache + k];
+            if (material[j] != 1) {
+                g[k] = 0.0f;
+                continue;
+            }
+            float xij[3] = {x[3 * i] - x[3 * j], x[3 * i + 1] - x[3 * j + 1], x[3 * i + 2] - x[3 * j + 2]};
+            float r = len3(xij);
+            if (r >= S->h_st) {
+                g[k] = 0.0f;
+                continue;
+            }
+            float vij[3] = {v[3 * i] - v[3 * j], v[3 * i + 1] - v[3 * j + 1], v[3 * i + 2] - v[3 * j + 2]};
+            float rho_bar = 0.5f * (density[i] + density[j]);
+            float W = st_W(r, S->d, S->h_st);
+            float gw[3];
+            st_gradW(xij, r, S->d, S->h_st, gw);
+            float gij = W / rho_bar;
+            float term_kernel = dot3(gw, vij) / rho_bar;
+            float term_density = W / (2.0f * rho_bar * rho_bar) * (div[i] + div[j]);
+            g[k] = gij + S->dt * (term_kernel - term_density);
+        }
+    }
+}
+
+/* compute_rhs_jeske23 (jeske23.py:190-237): b_i = -dt sigma / m_i sum m_bar x_ij g~ */
+static void st_rhs(int n, const orc_st_params* S, const float* x, const float* m, const int* material, const int* dyn,
+                   const int* count, const int* ids, const float* gt, float* b) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) {
+        float* o = b + 3 * (size_t)i;
+        if (!dyn[i] || material[i] != 1) {
+            o[0] = o[1] = o[2] = 0.0f;
+            continue;
+        }
+        float factor = -S->dt * S->sigma / m[i];
+        float acc[3] = {0.0f, 0.0f, 0.0f};
+        int cnt = clamp_cnt(count[i], S->cache);
+        for (int k = 0; k < cnt; ++k) {
+            long bb = (long)i * S->cache + k;
+            int j = ids[bb];
+            if (material[j] != 1) continue;
+            float g = gt[bb];
+            if (g == 0.0f) continue;
+            float mbar = 0.5f * (m[i] + m[j]);
+            for (int c = 0; c < 3; ++c) acc[c] = acc[c] + (mbar * (x[3 * i + c] - x[3 * j + c])) * g;
+        }
+        for (int c = 0; c < 3; ++c) o[c] = factor * acc[c];
+    }
+}
+
+/* compute_Av_jeske23 (jeske23.py:240-292): (M v)_i = v_i + dt^2 sigma / m_i sum m_bar g~ v_ij */
+static void st_Av(int n, const orc_st_params* S, const float* vin, const float* m, const int* material,
+                  const int* dyn, const int* count, const int* ids, const float* gt, float* av) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) {
+        const float* vi = vin + 3 * (size_t)i;
+        if (!dyn[i] || material[i] != 1) {
+            for (int c = 0; c < 3; ++c) av[3 * i + c] = vi[c];
+            continue;
+        }
+        float dt2 = S->dt * S->dt;
+        float factor = dt2 * S->sigma / m[i];
+        float sum[3] = {0.0f, 0.0f, 0.0f};
+        int cnt = clamp_cnt(count[i], S->cache);
+        for (int k = 0; k < cnt; ++k) {
+            long bb = (long)i * S->cache + k;
+            int j = ids[bb];
+            if (material[j] != 1) continue;
+            float g = gt[bb];
+            if (g == 0.0f) continue;
+            float mbar = 0.5f * (m[i] + m[j]);
+            float w = mbar * g;
+            for (int c = 0; c < 3; ++c) sum[c] = sum[c] + w * (vi[c] - vin[3 * j + c]);
+        }
+        for (int c = 0; c < 3; ++c) av[3 * i + c] = vi[c] + factor * sum[c];
+    }
+}
+
+/* compute_precond_jeske23 (jeske23.py:295-350): 1 / max(1 + dt^2 sigma / m_i sum m_bar g~, 1e-12) */
+static void st_precond(int n, const orc_st_params* S, const float* m, const int* material, const int* dyn,
+                       const int* count, const int* ids, const float* gt, float* inv) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) {
+        if (!dyn[i] || material[i] != 1) {
+            inv[i] = 1.0f;
+            continue;
+        }
+        float dt2 = S->dt * S->dt;
+        float factor = dt2 * S->sigma / m[i];
+        float ds = 0.0f;
+        int cnt = clamp_cnt(count[i], S->cache);
+        for (int k = 0; k < cnt; ++k) {
+            long bb = (long)i * S->cache + k;
+            int j = ids[bb];
+            if (material[j] != 1) continue;
+            float mbar = 0.5f * (m[i] + m[j]);
+            ds = ds + mbar * gt[bb];
+        }
+        float dv = 1.0f + factor * ds;
+        if (dv < 1.0e-12f) dv = 1.0e-12f;
+        inv[i] = 1.0f / dv;
+    }
+}
+
+/* Jeske23.solve (jeske23.py:585-655) with its PCG (jeske23.py:520-579):
+ * v += dv, M dv = v - M v + b, dv_0 = 0, preconditioner diag(inv).  Returns
+ * the CG iterations. */
+int orc_jeske23_solve(int n, const orc_st_params* S, const float* x, float* v, const float* m, const float* density,
+                      const int* material, const int* dyn, const int* count, const int* ids, const float* gradW,
+                      float* div_out, float* b_out) {
+    size_t n3 = 3 * (size_t)n;
+    float* div = (float*)calloc((size_t)n, sizeof(float));
+    float* gt = (float*)calloc((size_t)n * S->cache, sizeof(float));
+    float* b = (float*)calloc(n3, sizeof(float));
+    float* inv = (float*)calloc((size_t)n, sizeof(float));
+    float* dv = (float*)calloc(n3, sizeof(float));
+    float* r = (float*)calloc(n3, sizeof(float));
+    float* z = (float*)calloc(n3, sizeof(float));
+    float* p = (float*)calloc(n3, sizeof(float));
+    float* ap = (float*)calloc(n3, sizeof(float));
+    float* rhs = (float*)calloc(n3, sizeof(float));
+    st_divergence(n, S, v, m, material, dyn, count, ids, gradW, div);
+    st_g_tilde(n, S, x, v, density, material, dyn, count, ids, div, gt);
+    st_rhs(n, S, x, m, material, dyn, count, ids, gt, b);
+    st_precond(n, S, m, material, dyn, count, ids, gt, inv);
+    st_Av(n, S, v, m, material, dyn, count, ids, gt, ap);
+    for (int i = 0; i < n; ++i)
+        if (dyn[i])
+            for (int c = 0; c < 3; ++c) {
+                rhs[3 * i + c] = v[3 * i + c] + (-1.0f) * ap[3 * i + c];
+                rhs[3 * i + c] = rhs[3 * i + c] + 1.0f * b[3 * i + c];
+            }
+    memcpy(r, rhs, sizeof(float) * n3);
+    /* z = (inv I3) r, as wp.mat33 * vec3 */
+#define ST_PRECOND()                                                                   \
+    for (int i = 0; i < n; ++i)                                                        \
+        if (dyn[i]) {                                                                  \
+            float M[9] = {inv[i], 0.0f, 0.0f, 0.0f, inv[i], 0.0f, 0.0f, 0.0f, inv[i]}; \
+            mat33_vec(M, r + 3 * i, z + 3 * i);                                        \
+        }
+    ST_PRECOND();
+    memcpy(p, z, sizeof(float) * n3);
+    double rz_old = dot_dyn(n, r, z, dyn, S->fast);
+    int it = 0;
+    if (rz_old > 1e-12) {
+        for (;;) {
+            st_Av(n, S, p, m, material, dyn, count, ids, gt, ap);
+            double pap = dot_dyn(n, p, ap, dyn, S->fast);
+            if (pap <= 0.0) break;
+            double alpha = rz_old / (pap > 1e-12 ? pap : 1e-12);
+            float af = (float)alpha, naf = (float)(-alpha);
+            for (int i = 0; i < n; ++i)
+                if (dyn[i])
+                    for (int c = 0; c < 3; ++c) dv[3 * i + c] = dv[3 * i + c] + af * p[3 * i + c];
+            for (int i = 0; i < n; ++i)
+                if (dyn[i])
+                    for (int c = 0; c < 3; ++c) r[3 * i + c] = r[3 * i + c] + naf * ap[3 * i + c];
+            double rr = dot_dyn(n, r, r, dyn, S->fast);
+            ++it;
+            if ((rr < S->tol && it >= 2) || it >= S->max_iter) break;
+            ST_PRECOND();
+            double rz_new = dot_dyn(n, r, z, dyn, S->fast);
+            double beta = rz_new / (rz_old > 1e-12 ? rz_old : 1e-12);
+            float bf = (float)beta;
+            for (int i = 0; i < n; ++i)
+                if (dyn[i])
+                    for (int c = 0; c < 3; ++c) p[3 * i + c] = z[3 * i + c] + bf * p[3 * i + c];
+            rz_old = rz_new;
+        }
+    }
+#undef ST_PRECOND
+    for (int i = 0; i < n; ++i)
+        if (dyn[i])
+            for (int c = 0; c < 3; ++c) v[3 * i + c] = v[3 * i + c] + 1.0f * dv[3 * i + c];
+    if (div_out) memcpy(div_out, div, sizeof(float) * (size_t)n);
+    if (b_out) memcpy(b_out, b, sizeof(float) * n3);
+    free(div); free(gt); free(b); free(inv); free(dv); free(r); free(z); free(p); free(ap); free(rhs);
+    return it;
+}
+
 /*
  * One Framework.forward() step with IP (framework.py:423-544): gravity,
- * Weiler18 implicit viscosity when `visc` > 0 (no surface tension), IP.solve,
+ * Jeske23 implicit surface tension when `sigma` > 0, Weiler18 implicit
+ * viscosity when `visc` > 0 (framework.py:400-421), IP.solve,
  * advect + clamp, neighbour rebuild, density, Aii.  `count/ids/gradW/density/kd` must hold the state of
  * the previous rebuild (Framework.initialize, framework.py:282-290).
  */
 int orc_step(int n, const orc_params* P, float dt, const float* g, const float* domain, float* x, float* v,
              const float* rho0, const float* m, const float* m_inv, const int* dyn, int* count, int* ids,
              float* gradW, float* density, float* kd, double* err_hist, int* pcg_hist, orc_stats* st,
-             long* overflow, const int* material, float visc, int* visc_iters) {
+             long* overflow, const int* material, float visc, int* visc_iters, float sigma, int* st_iters) {
     orc_apply_gravity(n, v, dyn, g, dt);
+    if (material && sigma > 0.0f) {
+        /* Jeske23 implicit surface tension (framework.py:417-418) */
+        orc_st_params S = {sigma, dt, 0.5f * P->h, P->h, P->cache_size, 100, 1e-5, P->fast};
+        int it = orc_jeske23_solve(n, &S, x, v, m, density, material, dyn, count, ids, gradW, NULL, NULL);
+        if (st_iters) *st_iters = it;
+    }
     if (material && visc > 0.0f) {
         /* Weiler18 implicit viscosity (framework.py:400-421) */
         orc_visc_params V = {visc, dt, P->h, P->cache_size, 1000, 1e-5, P->fast};

@@ -48,6 +48,19 @@ class ViscParams(ctypes.Structure):
     ]
 
 
+class StParams(ctypes.Structure):
+    _fields_ = [
+        ("sigma", ctypes.c_float),
+        ("dt", ctypes.c_float),
+        ("d", ctypes.c_float),
+        ("h_st", ctypes.c_float),
+        ("cache", ctypes.c_int),
+        ("max_iter", ctypes.c_int),
+        ("tol", ctypes.c_double),
+        ("fast", ctypes.c_int),
+    ]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [
         ("outer_iters", ctypes.c_int),
@@ -85,9 +98,11 @@ def lib():
         L.orc_apply_gravity.argtypes = [i, P, P, P, f]
         L.orc_advect_and_clamp.argtypes = [i, P, P, P, f, P, f]
         L.orc_step.argtypes = [i, ctypes.POINTER(Params), f, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P,
-                               ctypes.POINTER(Stats), ctypes.POINTER(l), P, f, P]
+                               ctypes.POINTER(Stats), ctypes.POINTER(l), P, f, P, f, P]
         L.orc_weiler18_solve.argtypes = [i, ctypes.POINTER(ViscParams), P, P, P, P, P, P, P, P, P, P]
         L.orc_weiler18_solve.restype = i
+        L.orc_jeske23_solve.argtypes = [i, ctypes.POINTER(StParams), P, P, P, P, P, P, P, P, P, P, P]
+        L.orc_jeske23_solve.restype = i
         L.orc_step.restype = i
         L.orc_cg_f64.argtypes = [i, f, i, P, P, P, P, P, P, P, P, d, i, P]
         L.orc_cg_f64.restype = i
@@ -157,6 +172,8 @@ class State:
     material: Optional[np.ndarray] = None
     viscosity: float = 0.0        # Weiler18 kinematic viscosity (0 = off)
     visc_iters: int = 0
+    surface_tension: float = 0.0  # Jeske23 sigma (0 = off)
+    st_iters: int = 0
     count: Optional[np.ndarray] = None
     ids: Optional[np.ndarray] = None
     gradW: Optional[np.ndarray] = None
@@ -180,7 +197,8 @@ class State:
                   tol_opt=sc.density_error_tol, max_outer=sc.max_outer_iters,
                   max_pcg=sc.max_iteration_pcg, fixed_iters=sc.fixed_outer_iters,
                   material=_i32(sc.material),
-                  viscosity=float(sc.viscosity_coeff) if int(sc.viscosity_method) == 1 else 0.0)
+                  viscosity=float(sc.viscosity_coeff) if int(sc.viscosity_method) == 1 else 0.0,
+                  surface_tension=float(sc.surface_tension_coeff) if int(sc.surface_tension_method) == 1 else 0.0)
         kw.update(over)
         return cls(**kw)
 
@@ -247,12 +265,15 @@ class State:
         st = Stats()
         ov = ctypes.c_long(0)
         vit = ctypes.c_int(0)
+        sit = ctypes.c_int(0)
         status = lib().orc_step(n, ctypes.byref(P), float(self.dt), _p(self.gravity), _p(self.domain_size),
                                 _p(self.x), _p(self.v), _p(self.density0), _p(self.m), _p(self.m_inv),
                                 _p(self.is_dynamic), _p(self.count), _p(self.ids), _p(self.gradW),
                                 _p(self.density), _p(self.k), _p(err), _p(pcg), ctypes.byref(st), ctypes.byref(ov),
-                                _p(self.material), float(self.viscosity), ctypes.byref(vit))
+                                _p(self.material), float(self.viscosity), ctypes.byref(vit),
+                                float(self.surface_tension), ctypes.byref(sit))
         self.visc_iters = int(vit.value)
+        self.st_iters = int(sit.value)
         self._record(st, err, pcg)
         self.overflow = int(ov.value)
         self.status = int(status)
@@ -265,6 +286,19 @@ class State:
         return int(lib().orc_weiler18_solve(self.n, ctypes.byref(V), _p(self.x), _p(self.v), _p(self.m),
                                             _p(self.density), _p(self.density0), _p(self.material),
                                             _p(self.is_dynamic), _p(self.count), _p(self.ids), _p(self.gradW)))
+
+    # --- Jeske23.solve (jeske23.py:585-655) on the current lists
+    def surface_tension_solve(self, sigma: float, fast: bool = True, particle_radius: Optional[float] = None):
+        """Returns (CG iterations, div, b) of one Jeske23 solve (v updated)."""
+        d = np.float32(2.0 * particle_radius) if particle_radius is not None else np.float32(0.5 * self.h)
+        S = StParams(sigma=float(sigma), dt=float(self.dt), d=float(d), h_st=float(np.float32(2.0) * d),
+                     cache=self.cache_size, max_iter=100, tol=1e-5, fast=int(fast))
+        div = np.zeros(self.n, np.float32)
+        b = np.zeros((self.n, 3), np.float32)
+        it = lib().orc_jeske23_solve(self.n, ctypes.byref(S), _p(self.x), _p(self.v), _p(self.m), _p(self.density),
+                                     _p(self.material), _p(self.is_dynamic), _p(self.count), _p(self.ids),
+                                     _p(self.gradW), _p(div), _p(b))
+        return int(it), div, b
 
     # --- one outer-iteration linear system and its FP64 solution
     def system(self, d: np.ndarray):

@@ -15,6 +15,11 @@ kernels.npz       cubic_kernel / spiky_kernel_derivative at sampled radii;
 visc_solve.npz    one Weiler18 implicit-viscosity solve (weiler18.py:371-401) on
                   the moving block;
 column_visc_steps.npz  Framework.forward() steps with Weiler18 viscosity on;
+st_solve.npz      one Jeske23 implicit surface-tension solve (jeske23.py:585-655)
+                  on the moving block;
+column_st_steps.npz  Framework.forward() steps with Jeske23 surface tension and
+                  Weiler18 viscosity on (surface tension runs first,
+                  framework.py:417-421);
 block_solve.npz   one IP solve (ip.py:331-404) from a compressed, moving block
                   inside a static box, after the reference's neighbour build,
                   density and Aii;
@@ -70,7 +75,7 @@ class _Cfg:
     """Stand-in for config_builder.SimConfig with the keys the hot path reads."""
 
 
-def _make_objects(sc, viscosity_method=0, viscosity_coeff=0.0):
+def _make_objects(sc, viscosity_method=0, viscosity_coeff=0.0, st_method=0, st_coeff=0.0):
     from scripts.io.config_builder import SimConfig
     from scripts.sim.simulation_data import SimulationData
     from scripts.sim.neighbour_search import NeighbourSearch
@@ -78,8 +83,8 @@ def _make_objects(sc, viscosity_method=0, viscosity_coeff=0.0):
     conf = sc.config()
     cfg = SimConfig(domain_size=tuple(float(s) for s in sc.domain_size), domain_start=(0.0, 0.0, 0.0),
                     particle_radius=sc.particle_radius, dt=sc.dt, density0=1000.0,
-                    gravity=tuple(sc.gravity), viscosity_method=viscosity_method, surface_tension_method=0,
-                    viscosity_coeff=viscosity_coeff, surface_tension_coeff=0.0,
+                    gravity=tuple(sc.gravity), viscosity_method=viscosity_method, surface_tension_method=st_method,
+                    viscosity_coeff=viscosity_coeff, surface_tension_coeff=st_coeff,
                     scene_data={"Configuration": conf})
     ps = SimulationData(cfg)
     ps.allocate(sc.n)
@@ -176,14 +181,38 @@ def make_visc_solve(out, coeff=0.05):
         dv=visc.dv.numpy().copy())
 
 
-def make_column_steps(out, steps, viscosity=0.0):
+def make_st_solve(out, sigma=0.05):
+    """One Jeske23.solve (jeske23.py:585-655) on the moving block."""
+    from scripts.sim.forces.pressure.ip import IP
+    from scripts.sim.forces.non_pressure.surface_tension.jeske23 import Jeske23
+    sc = _scene_block()
+    cfg, ps, ns = _make_objects(sc, 0, 0.0, 1, sigma)
+    solver = IP(ps, ns, cfg)
+    ns.build(ps.x, ps.particle_num)
+    ns.build_cache(ps.x, ps.particle_num, int(ps.cache_size), ps.neighbor_count, ps.neighbor_ids,
+                   ps.neighbor_gradW)
+    solver.compute_density()
+    st = Jeske23(ps, ns, cfg)
+    v_before = ps.v.numpy().copy()
+    t0 = time.time()
+    st.solve(sigma, sigma, sc.dt)
+    print(f"st_solve: {time.time() - t0:.1f}s")
+    np.savez_compressed(
+        out, x=sc.x, v0=v_before, is_dynamic=sc.is_dynamic, material=sc.material, density0=sc.density0,
+        particle_radius=np.float64(sc.particle_radius), domain_size=sc.domain_size, dt=np.float64(sc.dt),
+        sigma=np.float64(sigma), density=ps.density.numpy().copy(), v=ps.v.numpy().copy(),
+        dv=st.dv.numpy().copy(), div=st.div_arr.numpy().copy(), b=st.b_st.numpy().copy())
+
+
+def make_column_steps(out, steps, viscosity=0.0, sigma=0.0):
     from scripts.framework import Framework
     sc = _scene_column()
-    cfg, ps, ns = _make_objects(sc, 1 if viscosity > 0 else 0, viscosity)
+    cfg, ps, ns = _make_objects(sc, 1 if viscosity > 0 else 0, viscosity, 1 if sigma > 0 else 0, sigma)
     fw = Framework(ps, ns, cfg)
     if viscosity <= 0:
         fw.viscosity = _NoForce()
-    fw.surface_tension = _NoForce()
+    if sigma <= 0:
+        fw.surface_tension = _NoForce()
     fw.initialize()
     nd = sc.n_dynamic
     rec = {k: [] for k in ("x", "v", "density", "k", "err", "pcg", "outer", "final_err", "cnt", "off", "ids")}
@@ -217,7 +246,7 @@ def make_column_steps(out, steps, viscosity=0.0):
     np.savez_compressed(
         out, x0=sc.x, v0=sc.v, is_dynamic=sc.is_dynamic, material=sc.material, density0=sc.density0,
         particle_radius=np.float64(sc.particle_radius), domain_size=sc.domain_size, dt=np.float64(sc.dt),
-        gravity=np.asarray(sc.gravity, np.float32), viscosity=np.float64(viscosity),
+        gravity=np.asarray(sc.gravity, np.float32), viscosity=np.float64(viscosity), sigma=np.float64(sigma),
         x=np.stack(rec["x"]), v=np.stack(rec["v"]), density=np.stack(rec["density"]), k=np.stack(rec["k"]),
         err=err, err_off=err_off, pcg=pcg, pcg_off=pcg_off, outer=np.array(rec["outer"], np.int32),
         final_err=np.array(rec["final_err"], np.float64), nbr_count=np.stack(rec["cnt"]),
@@ -238,7 +267,10 @@ def main():
             "column_steps": lambda: make_column_steps(os.path.join(HERE, "column_steps.npz"), a.steps),
             "visc_solve": lambda: make_visc_solve(os.path.join(HERE, "visc_solve.npz")),
             "column_visc_steps": lambda: make_column_steps(os.path.join(HERE, "column_visc_steps.npz"), 10,
-                                                           viscosity=0.01)}
+                                                           viscosity=0.01),
+            "st_solve": lambda: make_st_solve(os.path.join(HERE, "st_solve.npz")),
+            "column_st_steps": lambda: make_column_steps(os.path.join(HERE, "column_st_steps.npz"), 8,
+                                                         viscosity=0.01, sigma=0.05)}
     for name, job in jobs.items():
         if a.only and name != a.only:
             continue

@@ -225,3 +225,48 @@ def test_column_visc_steps_one_step_parity(golden_dir):
             continue
         assert _rel(st.v[dyn], g["v"][s][dyn]) < RTOL, s
         assert np.abs(st.x[dyn] - g["x"][s][dyn]).max() < 1e-6, s
+
+
+# ---------------------------------------------------- Jeske23 surface tension
+
+def _st_state(g, x, v, sigma, visc=0.0):
+    sc = S.Scene(x=np.array(x, np.float32), v=np.array(v, np.float32), is_dynamic=g["is_dynamic"],
+                 material=g["material"], density0=g["density0"], particle_radius=float(g["particle_radius"]),
+                 domain_size=g["domain_size"], dt=float(g["dt"]), viscosity_method=1 if visc > 0 else 0,
+                 viscosity_coeff=visc, surface_tension_method=1, surface_tension_coeff=sigma)
+    return O.State.from_scene(sc)
+
+
+@pytest.mark.parametrize("fast", [False, True])
+def test_surface_tension_solve_golden(golden_dir, fast):
+    g = _load(golden_dir, "st_solve.npz")
+    st = _st_state(g, g["x"], g["v0"], float(g["sigma"]))
+    st.rebuild()
+    dyn = st.is_dynamic == 1
+    it, div, b = st.surface_tension_solve(float(g["sigma"]), fast=fast, particle_radius=float(g["particle_radius"]))
+    assert it >= 1
+    assert _rel(div[dyn], g["div"][dyn]) < 1e-5
+    assert _rel(b[dyn], g["b"][dyn]) < 1e-4
+    assert _rel(st.v[dyn], g["v"][dyn]) < RTOL
+    assert _rel(st.v[dyn] - g["v0"][dyn], g["dv"][dyn]) < 2e-3  # the correction, relative to its own size
+
+
+def test_column_st_steps_one_step_parity(golden_dir):
+    """Steps with surface tension then viscosity then IP (framework.py:417-421)."""
+    g = _load(golden_dir, "column_st_steps.npz")
+    dyn = g["is_dynamic"] == 1
+    sigma, visc = float(g["sigma"]), float(g["viscosity"])
+    compared = 0
+    for s in range(g["x"].shape[0]):
+        x_prev = g["x0"] if s == 0 else g["x"][s - 1]
+        v_prev = g["v0"] if s == 0 else g["v"][s - 1]
+        st = _st_state(g, x_prev, v_prev, sigma, visc)
+        st.rebuild()
+        st.step(fast=True)
+        assert st.status == O.OK
+        if st.stats_outer_iters != int(g["outer"][s]):
+            continue
+        compared += 1
+        assert _rel(st.v[dyn], g["v"][s][dyn]) < RTOL, s
+        assert np.abs(st.x[dyn] - g["x"][s][dyn]).max() < 1e-6, s
+    assert compared >= g["x"].shape[0] - 1
