@@ -50,7 +50,9 @@ def make_scene(name: str):
         return S.tall_column(viscosity=False)
     if name == "small_column":
         return S.small_column()
-    if name == "dam_break":
+    if name == "dam_break":  # Weiler18 nu = 1e-3 and Jeske23 sigma = 0.05 on
+        return S.dam_break()
+    if name == "dam_break_ip":
         return S.dam_break(viscosity_method=0, viscosity_coeff=0.0, surface_tension_method=0,
                            surface_tension_coeff=0.0)
     raise SystemExit(f"unknown workload {name}")
@@ -70,7 +72,7 @@ def make_scenes(name: str):
 def workload_config(scenes, name: str) -> dict:
     if not isinstance(scenes, (list, tuple)):
         scenes = [scenes]
-    common = {"surface_tension": "off", "reductions": "f64 (CG inner products, error averages)",
+    common = {"reductions": "f64 (CG inner products, error averages)",
               "l2": "flushed between timed steps (256 MiB device write, outside the timed events)"}
     if len(scenes) > 1:
         nd = [sc.n_dynamic for sc in scenes]
@@ -79,12 +81,15 @@ def workload_config(scenes, name: str) -> dict:
                 "scenes": len(scenes), "fluid_particles": int(sum(nd)), "fluid_min": int(min(nd)),
                 "fluid_max": int(max(nd)), "boundary_particles": int(sum(sc.n - sc.n_dynamic for sc in scenes)),
                 "spacing_m": scenes[0].particle_diameter, "dt_s": scenes[0].dt,
-                "densityErrorTol": scenes[0].density_error_tol, "viscosity": "off", **common}
+                "densityErrorTol": scenes[0].density_error_tol, "viscosity": "off", "surface_tension": "off",
+                **common}
     sc = scenes[0]
-    return {"workload": sc.name + ("_ip_only" if name == "tall_column_ip" else ""),
+    return {"workload": sc.name + ("_ip_only" if name in ("tall_column_ip", "dam_break_ip") else ""),
             "fluid_particles": sc.n_dynamic, "boundary_particles": sc.n - sc.n_dynamic,
             "spacing_m": sc.particle_diameter, "dt_s": sc.dt, "densityErrorTol": sc.density_error_tol,
             "viscosity": ("weiler18 nu=%g" % sc.viscosity_coeff) if sc.viscosity_method == 1 else "off",
+            "surface_tension": ("jeske23 sigma=%g" % sc.surface_tension_coeff)
+            if sc.surface_tension_method == 1 and sc.surface_tension_coeff > 0 else "off",
             **common}
 
 
@@ -157,6 +162,10 @@ def algorithmic_bytes(kernel: str, n_dyn: int, n_all: int, pairs: int, it=None) 
         b += I * (algorithmic_bytes("cg_a", n_dyn, n_all, pairs) + algorithmic_bytes("cg_b", n_dyn, n_all, pairs))
         b += algorithmic_bytes("divergence", n_dyn, n_all, pairs) + 48 * n_dyn  # d = dt v, v = d / dt
         return b
+    if kernel == "surface_tension":  # Jeske 2023: divergence + setup passes, per iteration a list pass (J rows
+        # and the stored w_ij) and a slot pass
+        V = it.get("st", 0.0)
+        return 2 * 16 * P + 4 * P + 150 * n_dyn + V * ((16 * P + 4 * P + 64 * n_dyn) + 96 * n_dyn)
     if kernel == "visc":  # Weiler 2018 solve: setup pass, then per iteration a list pass and a slot pass
         V = it["visc"] if it.get("visc_on") else 0.0
         return 16 * P + 120 * n_dyn + V * ((16 * P + 64 * n_dyn) + 120 * n_dyn)
@@ -328,7 +337,7 @@ def run_ours(args, rank, world, local_rank):
     if "ip_solve" in prof:
         # gravity, viscosity (if on), persistent IP solve, advect, keys, 2
         # scan passes, place, order, neighbour build, static outputs
-        n_launch = (10 + int("visc" in prof)) * args.steps
+        n_launch = (10 + int("visc" in prof) + int("surface_tension" in prof)) * args.steps
     else:
         so = sum(r.sum_outer_iters for r in raws)
         n_launch = 12 * args.steps + (so + args.steps) + so + 2 * sum(r.sum_pcg_iters for r in raws)
@@ -338,7 +347,8 @@ def run_ours(args, rank, world, local_rank):
     alg = 0.0
     for sc, r, pr in zip(scenes, raws, pairs):
         it = {"outer": r.sum_outer_iters / args.steps, "cg": r.sum_pcg_iters / args.steps,
-              "visc": r.sum_visc_iters / args.steps, "visc_on": sc.viscosity_method == 1}
+              "visc": r.sum_visc_iters / args.steps, "visc_on": sc.viscosity_method == 1,
+              "st": r.sum_st_iters / args.steps}
         alg += algorithmic_bytes(dom_name, sc.n_dynamic, sc.n, pr, it)
     peak, peak_kind = load_peaks()
     achieved = alg / avg_s / 1e9 if avg_s > 0 else 0.0
@@ -373,6 +383,7 @@ def run_ours(args, rank, world, local_rank):
                 "outer_iters_per_step": so / args.steps / len(scenes),
                 "cg_iters_per_step": sum(r.sum_pcg_iters for r in raws) / args.steps / len(scenes),
                 "visc_cg_iters_per_step": sum(r.sum_visc_iters for r in raws) / args.steps / len(scenes),
+                "st_cg_iters_per_step": sum(r.sum_st_iters for r in raws) / args.steps / len(scenes),
                 "mean_neighbours": sum(pairs) / max(n_dyn, 1),
                 "wall_s": wall, "gpu_launches": int(n_launch), "clocks": clk, "roofline": roof,
                 "cpu_baseline": cpu, "e2e": e2e}

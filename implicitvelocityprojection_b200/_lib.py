@@ -39,7 +39,9 @@ class SceneDesc(ctypes.Structure):
         ("cache_size", ctypes.c_int32),
         ("viscosity_coeff", ctypes.c_float),
         ("viscosity_method", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 4),
+        ("surface_tension_method", ctypes.c_int32),
+        ("surface_tension_coeff", ctypes.c_float),
+        ("reserved", ctypes.c_int32 * 2),
     ]
 
 
@@ -88,12 +90,14 @@ class SolveStats(ctypes.Structure):
         ("max_final_density_error", ctypes.c_double),
         ("neighbour_pairs", ctypes.c_int64),
         ("sum_visc_iters", ctypes.c_int64),
+        ("sum_st_iters", ctypes.c_int64),
     ]
 
 
 # kernel ids of ivp_profile_step (include/ivp.h)
 KERNEL_NAMES = ["gravity", "solve_begin", "pack", "rhs", "cg_a", "cg_b", "solve_end", "divergence", "advect",
-                "keys", "scan_local", "scan_add", "place", "order", "nbr_build", "static_out", "visc", "ip_solve"]
+                "keys", "scan_local", "scan_add", "place", "order", "nbr_build", "static_out", "visc", "ip_solve",
+                "surface_tension"]
 K_COUNT = 24
 NOALLOC_MAX_PARTICLES = 65536
 NOALLOC_MAX_CELLS = 262144
@@ -115,6 +119,7 @@ SIGNATURES = {
     "ivp_compute_aii": (_I, [_P, _P]),
     "ivp_ip_solve": (_I, [_P, _P]),
     "ivp_viscosity_solve": (_I, [_P, _P]),
+    "ivp_surface_tension_solve": (_I, [_P, _P]),
     "ivp_apply_gravity": (_I, [_P, _P]),
     "ivp_advect": (_I, [_P, _P]),
     "ivp_step": (_I, [_P, _I, _P]),

@@ -50,6 +50,10 @@ struct SceneParams {
     float spiky_k;             // 45 / (pi h^6) (sph_kernel.py:55)
     float visc_coeff;
     int visc_method;
+    float st_coeff;            // Jeske 2023 surface tension sigma
+    int st_method;
+    float st_d;                // particle diameter d (W^st clamps r at d)
+    float st_h;                // surface-tension support h_st = 2 d (jeske23.py:455)
     int max_outer, max_pcg, fixed_iters, cache;
     int tile_begin, tile_end;
     int hist_base;
@@ -74,7 +78,9 @@ struct SceneCtl {
     int status;
     int n_err;
     int total_cg;
-    // Weiler 2018 implicit viscosity CG (weiler18.py:298-365)
+    // implicit non-pressure CG, shared by the surface tension (Jeske 2023,
+    // jeske23.py:520-579) and viscosity (Weiler 2018, weiler18.py:298-365)
+    // solves, which run one after the other
     double v_rz;         // r.z of the current iterate
     double v_alpha;
     double v_beta;
@@ -82,7 +88,9 @@ struct SceneCtl {
     int v_active;        // CG running
     int v_it;            // CG iterations of this solve
     int v_total;         // CG iterations of the last step (stats)
-    int v_on;            // viscosity enabled for this scene (set at the start of a step)
+    int v_on;            // the force being solved is enabled for this scene (set at its start)
+    int v_max;           // CG iteration cap of that force (100 surface tension, 1000 viscosity)
+    int v_pad;
     // sticky counters since the last reset (ivp_reset_counters)
     double acc_max_final_err;
     int acc_solves;
@@ -91,6 +99,7 @@ struct SceneCtl {
     int acc_failed;
     int acc_last_failure;
     int acc_visc;        // viscosity CG iterations
+    int acc_st;          // surface-tension CG iterations
 };
 
 static_assert(sizeof(SceneCtl) % sizeof(double) == 0, "SceneCtl is read as doubles");
@@ -164,6 +173,9 @@ struct Dev {
     float4* vs;              // viscosity: slot-ordered velocity
     float4* vap;             // viscosity: A p
     float4* pinv;            // viscosity: 3x3 block-Jacobi inverse, 3 rows per slot
+    float2* st_w;            // surface tension: {j, m_bar_ij g~_ij} per neighbour-row entry (same indexing)
+    float4* st_rec;          // surface tension, two float4 per slot: {v, div} {rho, 1/rho if fluid, 0, 0}
+    float* st_inv;           // surface tension: Jacobi inverse per slot (jeske23.py:295-350)
     float* q;                // fk / m
     float* z;                // y / m
     // neighbour rows
@@ -186,6 +198,7 @@ struct Dev {
     int advect_skip_failed;
     // the persistent solve runs the viscosity phases (set on step launches)
     int visc_enabled;
+    int force;               // implicit non-pressure solve of this launch: 0 viscosity, 1 surface tension
     // persistent solve: grid-barrier words and the phase budget
     unsigned* bar_count;
     unsigned* bar_gen;

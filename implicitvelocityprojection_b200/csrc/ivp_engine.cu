@@ -63,6 +63,7 @@ struct ivp_engine {
     bool bound = false;
     bool want_divergence = false;
     bool any_visc = false;
+    bool any_st = false;
     // persistent solve
     bool persistent = false;
     int coop_grid = 0, coop_grid_visc = 0;
@@ -185,14 +186,15 @@ struct Kern {
 };
 
 struct KernelSet {
-    DevKernel pack, rhs, cg_a, cg_b, dens, aii, div, persist, v_setup, v_a, v_b, v_end, v_persist;
+    DevKernel pack, rhs, cg_a, cg_b, dens, aii, div, persist, v_setup, v_a, v_b, v_end, v_persist, st_div;
 };
 
 template <int G, int B>
 KernelSet make_set() {
     return {Kern<G, B>::pack(), Kern<G, B>::rhs(), Kern<G, B>::cg_a(), Kern<G, B>::cg_b(),
             Kern<G, B>::dens(), Kern<G, B>::aii(), Kern<G, B>::div(), k_ip_persistent<G, B>,
-            k_visc_setup<G, B>, k_visc_a<G, B>, k_visc_b<G, B>, k_visc_end<G, B>, k_visc_persistent<G, B>};
+            k_visc_setup<G, B>, k_visc_a<G, B>, k_visc_b<G, B>, k_visc_end<G, B>, k_visc_persistent<G, B>,
+            k_st_div<G, B>};
 }
 
 // Instantiated launch shapes: G lanes per particle x {128, 256} threads.
@@ -322,38 +324,46 @@ int emit_solve_loop(ivp_engine* e, Launcher& L) {
     return IVP_OK;
 }
 
-// Weiler 2018 viscosity, one launch per phase (the persistent solve runs the
-// same phases itself).
-int emit_visc(ivp_engine* e, Launcher& L) {
-    if (e->n_tiles == 0 || !e->any_visc) return IVP_OK;
+bool force_any(const ivp_engine* e, int force) { return force == FORCE_ST ? e->any_st : e->any_visc; }
+
+// An implicit non-pressure solve, one launch per phase: Jeske 2023 surface
+// tension (force 1, with its divergence pass) or Weiler 2018 viscosity
+// (force 0).  The persistent kernel runs the same phases itself.
+int emit_force(ivp_engine* e, Launcher& L, int force) {
+    if (e->n_tiles == 0 || !force_any(e, force)) return IVP_OK;
     KernelSet K;
     if (!kernel_set(e->G, e->BLOCK, &K)) return IVP_ERR_BAD_ARG;
     const int nt = e->n_tiles, B = e->BLOCK;
-    CKS(L.dev(IVP_K_VISC, k_visc_begin, nt, e->T, e->D));
+    const int kid = force == FORCE_ST ? IVP_K_SURFACE_TENSION : IVP_K_VISC;
+    Dev D0 = e->D;
+    D0.force = force;
+    if (force == FORCE_ST) CKS(L.dev(kid, k_slot_velocity, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D0));
+    CKS(L.dev(kid, k_visc_begin, nt, e->T, D0));
+    if (force == FORCE_ST) CKS(L.dev(kid, K.st_div, nt, B, D0));
     if (!L.graph) {
-        CKS(L.dev(IVP_K_VISC, K.v_setup, nt, B, e->D));
+        CKS(L.dev(kid, K.v_setup, nt, B, D0));
         CK(cudaMemcpyAsync(e->h_flags, e->D.flags, sizeof(Flags), cudaMemcpyDeviceToHost, L.stream));
         CK(cudaStreamSynchronize(L.stream));
         for (int guard = 0; e->h_flags->any_visc && guard < 1000000; ++guard) {
-            CKS(L.dev(IVP_K_VISC, K.v_a, nt, B, e->D));
-            CKS(L.dev(IVP_K_VISC, K.v_b, nt, B, e->D));
+            CKS(L.dev(kid, K.v_a, nt, B, D0));
+            CKS(L.dev(kid, K.v_b, nt, B, D0));
             CK(cudaMemcpyAsync(e->h_flags, e->D.flags, sizeof(Flags), cudaMemcpyDeviceToHost, L.stream));
             CK(cudaStreamSynchronize(L.stream));
         }
     } else {
         cudaGraphConditionalHandle h;
         CK(cudaGraphConditionalHandleCreate(&h, L.graph, 0, 0));
-        Dev d = e->D;
+        Dev d = D0;
         d.h_visc = (unsigned long long)h;
-        CKS(L.dev(IVP_K_VISC, K.v_setup, nt, B, d));
+        CKS(L.dev(kid, K.v_setup, nt, B, d));
         cudaGraph_t body;
         CKS(add_conditional(L.graph, L, h, cudaGraphCondTypeWhile, &body));
         Launcher Lb;
         Lb.graph = body;
-        CKS(Lb.dev(IVP_K_VISC, K.v_a, nt, B, d));
-        CKS(Lb.dev(IVP_K_VISC, K.v_b, nt, B, d));
+        CKS(Lb.dev(kid, K.v_a, nt, B, d));
+        CKS(Lb.dev(kid, K.v_b, nt, B, d));
     }
-    return L.dev(IVP_K_VISC, K.v_end, nt, B, e->D);
+    return L.dev(kid, K.v_end, nt, B, D0);
 }
 
 int emit_solve(ivp_engine* e, Launcher& L, bool with_visc = false) {
@@ -383,21 +393,33 @@ int emit_advect(ivp_engine* e, Launcher& L) {
     return L.dev(IVP_K_ADVECT, k_advect, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, e->D);
 }
 
-int emit_visc_persistent(ivp_engine* e, Launcher& L) {
-    if (e->n_tiles == 0 || !e->any_visc) return IVP_OK;
+int emit_force_persistent(ivp_engine* e, Launcher& L, int force) {
+    if (e->n_tiles == 0 || !force_any(e, force)) return IVP_OK;
     KernelSet K;
     kernel_set(e->G, e->BLOCK, &K);
     CKS(L.memset0(e->D.bar_count, sizeof(unsigned)));
     Dev copy = e->D;
+    copy.force = force;
+    if (force == FORCE_ST)
+        CKS(L.dev(IVP_K_SURFACE_TENSION, k_slot_velocity, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, copy));
     void* args[] = {&copy};
-    return L.kernel(IVP_K_VISC, (const void*)K.v_persist, dim3(e->coop_grid_visc), dim3(e->BLOCK), args,
-                    e->coop_smem, true);
+    return L.kernel(force == FORCE_ST ? IVP_K_SURFACE_TENSION : IVP_K_VISC, (const void*)K.v_persist,
+                    dim3(e->coop_grid_visc), dim3(e->BLOCK), args, e->coop_smem, true);
+}
+
+// Non-pressure forces in the reference's order (framework.py:400-421):
+// surface tension, then viscosity.
+int emit_forces(ivp_engine* e, Launcher& L) {
+    for (int force : {FORCE_ST, FORCE_VISC}) {
+        if (e->persistent) CKS(emit_force_persistent(e, L, force));
+        else CKS(emit_force(e, L, force));
+    }
+    return IVP_OK;
 }
 
 int emit_step(ivp_engine* e, Launcher& L) {
     CKS(L.dev(IVP_K_GRAVITY, k_gravity, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, e->D));
-    if (!e->persistent) CKS(emit_visc(e, L));
-    else CKS(emit_visc_persistent(e, L));
+    CKS(emit_forces(e, L));
     CKS(emit_solve(e, L, true));
     {
         Dev d = e->D;
@@ -472,13 +494,18 @@ int validate(const ivp_scene_desc* sc, int n, const ivp_options* o) {
     return IVP_OK;
 }
 
+bool scene_st(const ivp_scene_desc& d) {
+    return d.surface_tension_method == 1 && d.surface_tension_coeff > 0.0f && d.n_dynamic > 0;
+}
+
 struct Plan {
     std::vector<SceneParams> hp;
     std::vector<int4> tiles;
     std::vector<int4> segs;
     int n_total = 0, n_dyn = 0, n_keys = 0, scan_blocks = 0;
     bool compact = false;  // neighbour rows as {j, w} (8 B entries)
-    size_t off[48];
+    bool any_st = false;   // some scene runs the implicit surface tension
+    size_t off[56];
     Layout lay;
 };
 
@@ -531,6 +558,10 @@ void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
         q.spiky_k = 45.0f / (3.14159265359f * h * h * h * h * h * h);
         q.visc_coeff = d.viscosity_coeff;
         q.visc_method = d.viscosity_method;
+        q.st_coeff = d.surface_tension_coeff;
+        q.st_method = d.surface_tension_method;
+        q.st_d = 2.0f * d.particle_radius;  // jeske23.py:454-455
+        q.st_h = 2.0f * q.st_d;
         q.max_outer = d.max_outer_iters;
         q.max_pcg = d.max_iteration_pcg;
         q.fixed_iters = d.fixed_outer_iters;
@@ -558,6 +589,8 @@ void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
     // pair, which outweighs the halved list stream on B200, so the default
     // is full rows
     P.compact = o->row_format == 2;
+    for (int s = 0; s < n; ++s)
+        if (scene_st(sc[s])) P.any_st = true;
     P.n_keys = key_base;
     P.scan_blocks = std::max(1, (P.n_keys + SCAN_TILE - 1) / SCAN_TILE);
     const size_t N = (size_t)P.n_total, S = (size_t)n, NT = std::max<size_t>(P.tiles.size(), 1);
@@ -608,6 +641,9 @@ void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
     P.off[i++] = L.add(sizeof(float4) * N);                          // 42 vap
     P.off[i++] = L.add(3 * sizeof(float4) * N);                      // 43 pinv
     P.off[i++] = L.add(sizeof(int4) * std::max<size_t>(P.segs.size(), 1));  // 44 segs
+    P.off[i++] = L.add(P.any_st ? sizeof(float2) * (size_t)P.n_dyn * (size_t)o->list_stride : 0);  // 45 st_w
+    P.off[i++] = L.add(P.any_st ? 2 * sizeof(float4) * N : 0);       // 46 st_rec
+    P.off[i++] = L.add(P.any_st ? sizeof(float) * N : 0);            // 47 st_inv
 }
 
 cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
@@ -661,8 +697,11 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
     e->scan_blocks = P.scan_blocks;
     e->n_scenes = n_scenes;
     for (int sc = 0; sc < n_scenes; ++sc)
+    {
         if (scenes[sc].viscosity_method == 1 && scenes[sc].viscosity_coeff > 0.0f && scenes[sc].n_dynamic > 0)
             e->any_visc = true;
+        if (scene_st(scenes[sc])) e->any_st = true;
+    }
     char* w = static_cast<char*>(workspace);
     Dev& D = e->D;
     int i = 0;
@@ -712,6 +751,9 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
     D.vap = reinterpret_cast<float4*>(w + P.off[i++]);
     D.pinv = reinterpret_cast<float4*>(w + P.off[i++]);
     D.segs = reinterpret_cast<int4*>(w + P.off[i++]);
+    D.st_w = reinterpret_cast<float2*>(w + P.off[i++]);
+    D.st_rec = reinterpret_cast<float4*>(w + P.off[i++]);
+    D.st_inv = reinterpret_cast<float*>(w + P.off[i++]);
     D.n_segs = (int)P.segs.size();
     e->n_segs = D.n_segs;
     {
@@ -836,6 +878,13 @@ int ivp_update_scene(ivp_engine* e, int32_t scene, const ivp_scene_desc* d, void
     q.tol_pcg = d->tol_pcg;
     q.visc_coeff = d->viscosity_coeff;
     q.visc_method = d->viscosity_method;
+    // a force may be switched off, not on: its buffers and launches were
+    // planned at creation
+    const bool st = d->surface_tension_method == 1 && d->surface_tension_coeff > 0.0f;
+    const bool vi = d->viscosity_method == 1 && d->viscosity_coeff > 0.0f;
+    if ((st && !e->any_st) || (vi && !e->any_visc)) return IVP_ERR_BAD_ARG;
+    q.st_coeff = d->surface_tension_coeff;
+    q.st_method = d->surface_tension_method;
     cudaStream_t s = as_stream(stream);
     CK(cudaMemcpyAsync((void*)(e->D.scenes + scene), &q, sizeof(SceneParams), cudaMemcpyHostToDevice, s));
     CK(cudaStreamSynchronize(s));
@@ -880,7 +929,15 @@ int ivp_viscosity_solve(ivp_engine* e, void* stream) {
     if (!e->bound) return IVP_ERR_NOT_BOUND;
     Launcher L;
     L.stream = as_stream(stream);
-    return emit_visc(e, L);
+    return emit_force(e, L, FORCE_VISC);
+}
+
+int ivp_surface_tension_solve(ivp_engine* e, void* stream) {
+    if (!e) return IVP_ERR_BAD_ARG;
+    if (!e->bound) return IVP_ERR_NOT_BOUND;
+    Launcher L;
+    L.stream = as_stream(stream);
+    return emit_force(e, L, FORCE_ST);
 }
 
 int ivp_apply_gravity(ivp_engine* e, void* stream) {
@@ -930,6 +987,7 @@ int ivp_read_stats(ivp_engine* e, int32_t scene, void* stream, ivp_solve_stats* 
     out->max_final_density_error = C.acc_max_final_err;
     out->neighbour_pairs = (int64_t)e->h_pairs[scene];
     out->sum_visc_iters = C.acc_visc;
+    out->sum_st_iters = C.acc_st;
     if (e->h_flags->timeout) {
         g_err = "a solve exceeded its iteration budget or a grid barrier timed out";
         out->status = IVP_ERR_TIMEOUT;

@@ -14,7 +14,11 @@
 
 namespace ivp {
 
-enum Kind { K_PACK = 0, K_RHS = 1, K_CG_A = 2, K_CG_B = 3, K_V_SETUP = 4, K_V_A = 5, K_V_B = 6 };
+// K_V_*: the implicit non-pressure CG (surface tension or viscosity, the
+// launch's Dev::force); K_ST_DIV: the surface-tension divergence pass before
+// its setup (no reduction)
+enum Kind { K_PACK = 0, K_RHS = 1, K_CG_A = 2, K_CG_B = 3, K_V_SETUP = 4, K_V_A = 5, K_V_B = 6, K_ST_DIV = 7 };
+constexpr int FORCE_VISC = 0, FORCE_ST = 1;
 
 constexpr int IVP_OK_ = 0, IVP_NOT_SPD_ = 1, IVP_NOT_CONVERGED_ = 2, IVP_TIMEOUT_ = 6;
 
@@ -40,6 +44,22 @@ constexpr int kViscMaxIter = 1000;
 constexpr double kViscTol = 1e-5;
 
 __device__ __forceinline__ bool visc_on(const SceneParams& P) { return P.visc_method == 1 && P.visc_coeff > 0.0f; }
+__device__ __forceinline__ bool st_enabled(const SceneParams& P) { return P.st_method == 1 && P.st_coeff > 0.0f; }
+
+// Start of an implicit non-pressure solve of force D.force for one scene.
+__device__ __forceinline__ void force_begin(const Dev& D, const SceneParams& P, SceneCtl& C) {
+    const bool on = D.force == FORCE_ST ? st_enabled(P) : visc_on(P);
+    C.v_on = (on && P.n_dyn > 0) ? 1 : 0;
+    C.v_max = D.force == FORCE_ST ? 100 : kViscMaxIter;  // jeske23.py:470, weiler18.py:208
+    C.v_active = 0;
+    C.v_total = 0;
+}
+
+// End of that solve: its CG iterations into the sticky counters.
+__device__ __forceinline__ void force_account(const Dev& D, SceneCtl& C) {
+    if (D.force == FORCE_ST) C.acc_st += C.v_total;
+    else C.acc_visc += C.v_total;
+}
 
 __device__ void scene_decide(const Dev& D, const SceneParams& P, SceneCtl& C, int kind, double s, bool hist,
                              double s2 = 0.0) {
@@ -60,10 +80,11 @@ __device__ void scene_decide(const Dev& D, const SceneParams& P, SceneCtl& C, in
         return;
     }
     if (kind == K_V_B) {
-        // weiler18.py:349-365: s = r.r (stop test), s2 = r.z (beta)
+        // weiler18.py:349-365 and jeske23.py:553-567: s = r.r (stop test),
+        // s2 = r.z (beta); both use tol 1e-5, caps 1000 and 100 (v_max)
         C.v_it += 1;
         C.v_total = C.v_it;
-        if ((s < kViscTol && C.v_it >= 2) || C.v_it >= kViscMaxIter) {
+        if ((s < kViscTol && C.v_it >= 2) || C.v_it >= C.v_max) {
             C.v_active = 0;
         } else {
             C.v_beta = s2 / (C.v_rz > 1e-12 ? C.v_rz : 1e-12);
@@ -736,7 +757,6 @@ __global__ void k_solve_end(const Dev D) {
         W.acc_solves += 1;
         W.acc_outer += C.outer_it;
         W.acc_cg += C.total_cg;
-        W.acc_visc += C.v_total;
         if (C.final_err > W.acc_max_final_err) W.acc_max_final_err = C.final_err;
         if (C.status != IVP_OK_) {
             W.acc_failed += 1;
@@ -817,15 +837,17 @@ static_assert(PU % 2 == 0, "entries are loaded in pairs");
 struct PairBatch {
     int j[PU];
     float3 J[PU];
+    unsigned live;  // bit u: entry u is a neighbour (not a masked slot past the row end)
 };
 
 __device__ __forceinline__ void pair_entry(const float4& e, bool in, int self, int lo, int hi, int& j, float3& J,
-                                           bool& bad) {
+                                           bool& bad, unsigned& live, int u) {
     const int jj = __float_as_int(e.w);
     const bool ok = jj >= lo && jj < hi;
     bad |= in && !ok;
     j = (in && ok) ? jj : self;
     J = (in && ok) ? f3(e) : make_float3(0.f, 0.f, 0.f);
+    live |= (in && ok) ? (1u << u) : 0u;
 }
 
 // k0 = 2 * lane + (batch start); xi is the row particle's position (the
@@ -834,6 +856,7 @@ template <int G>
 __device__ __forceinline__ bool load_pairs(const Dev& D, int row, float3 xi, int k0, int cnt, int self, int lo,
                                            int hi, PairBatch& b) {
     bool bad = false;
+    b.live = 0u;
     if (!D.compact) {
         const float4* __restrict__ nb = D.nbr + (size_t)row * D.stride;
 #pragma unroll
@@ -841,8 +864,8 @@ __device__ __forceinline__ bool load_pairs(const Dev& D, int row, float3 xi, int
             const int k = k0 + u * 2 * G;
             float4 e0 = make_float4(0.f, 0.f, 0.f, 0.f), e1 = e0;
             if (k < cnt) ld_rec_nc(nb + k, e0, e1);
-            pair_entry(e0, k < cnt, self, lo, hi, b.j[2 * u], b.J[2 * u], bad);
-            pair_entry(e1, k + 1 < cnt, self, lo, hi, b.j[2 * u + 1], b.J[2 * u + 1], bad);
+            pair_entry(e0, k < cnt, self, lo, hi, b.j[2 * u], b.J[2 * u], bad, b.live, 2 * u);
+            pair_entry(e1, k + 1 < cnt, self, lo, hi, b.j[2 * u + 1], b.J[2 * u + 1], bad, b.live, 2 * u + 1);
         }
     } else {
         const float4* __restrict__ nb =
@@ -862,6 +885,7 @@ __device__ __forceinline__ bool load_pairs(const Dev& D, int row, float3 xi, int
                 const int j = (in && ok) ? jj : self;
                 const float3 r = sub3(xi, f3(__ldg(D.xm + j)));
                 b.j[2 * u + h] = j;
+                b.live |= (in && ok) ? (1u << (2 * u + h)) : 0u;
                 b.J[2 * u + h] = (in && ok) ? make_float3(__fmul_rn(w, r.x), __fmul_rn(w, r.y), __fmul_rn(w, r.z))
                                             : make_float3(0.f, 0.f, 0.f);
             }
@@ -1295,6 +1319,286 @@ __device__ __forceinline__ void visc_end_tile(const Dev& D, const TileCtx& T) {
     D.v[3 * p + 2] = D.v[3 * p + 2] + 1.0f * dv.z;
 }
 
+
+// ---- Jeske 2023 implicit surface tension (jeske23.py), over fluid pairs
+
+// compute_Wst (jeske23.py:26-44): theta W_cubic(max(r, d); h_st), theta = 10/7
+__device__ __forceinline__ float st_W(float r, float d, float h) {
+    const float theta = 10.0f / 7.0f;
+    const float rc = r > d ? r : d;
+    const float q = rc / h;
+    const float norm = 8.0f / (3.14159265358979f * h * h * h);
+    float fq = 0.0f;
+    if (q <= 0.5f) {
+        fq = 1.0f - 6.0f * q * q + 6.0f * q * q * q;
+    } else if (q <= 1.0f) {
+        const float t = 1.0f - q;
+        fq = 2.0f * t * t * t;
+    }
+    return theta * norm * fq;
+}
+
+// compute_grad_Wst (jeske23.py:47-67): zero for r <= d, else theta grad W_cubic
+__device__ __forceinline__ float3 st_gradW(float3 xij, float r, float d, float h) {
+    if (r <= d || r < 1.0e-12f) return make_float3(0.f, 0.f, 0.f);
+    const float q = r / h;
+    if (q > 1.0f) return make_float3(0.f, 0.f, 0.f);
+    const float theta = 10.0f / 7.0f;
+    const float norm = 8.0f / (3.14159265358979f * h * h * h);
+    float fpq;
+    if (q <= 0.5f) {
+        fpq = -12.0f * q + 18.0f * q * q;
+    } else {
+        const float t = 1.0f - q;
+        fpq = -6.0f * t * t;
+    }
+    const float s = theta * norm * (1.0f / h) * fpq;
+    return make_float3(s * (xij.x / r), s * (xij.y / r), s * (xij.z / r));
+}
+
+// Slot-ordered velocity for the surface-tension passes: vs = {v, 1/rho of
+// fluid slots (0 otherwise)}, one 16-byte gather per neighbour.
+__global__ void k_slot_velocity(const Dev D) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= D.n_total) return;
+    const int s = D.inv[p];
+    D.vs[s] = make_float4(D.v[3 * p], D.v[3 * p + 1], D.v[3 * p + 2], D.dyn[p] ? D.rflu[s] : 0.0f);
+}
+
+// compute_divergence_jeske23 (jeske23.py:74-115): div_i = sum over fluid j of
+// m_j v_ij . grad W_ij = J_ij . v_ij.  Stores the slot's record for the
+// setup's neighbour gathers: {v, div} {rho, 1/rho if fluid}.
+template <int G>
+__device__ __forceinline__ void st_div_tile(const Dev& D, const SceneParams& P, const TileCtx& T) {
+    const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
+    float3 xi = make_float3(0.f, 0.f, 0.f), vi = xi;
+    float rfi = 0.0f;
+    if (T.valid) {
+        xi = f3(D.xm[T.i]);
+        const float4 v4 = D.vs[T.i];
+        vi = f3(v4);
+        rfi = v4.w;
+    }
+    const bool fluid = T.valid && rfi != 0.0f;
+    float acc = 0.0f;
+    bool bad = false;
+    const int self = T.valid ? T.i : P.s_begin;
+    for (int k0 = 2 * T.lane; k0 < (fluid ? cnt : 0); k0 += G * PU) {
+        PairBatch b;
+        bad |= load_pairs<G>(D, T.row, xi, k0, cnt, self, P.s_begin, P.s_end, b);
+#pragma unroll
+        for (int u = 0; u < PU; ++u) {
+            const float4 vj = D.vs[b.j[u]];
+            const bool use = ((b.live >> u) & 1u) && vj.w != 0.0f;
+            acc += use ? dot3(sub3(vi, f3(vj)), b.J[u]) : 0.0f;
+        }
+    }
+    if (bad) flag_bad(D, T.i, 7);
+    acc = group_sum<G>(acc);
+    if (T.valid && T.lane == 0) {
+        D.st_rec[2 * T.i] = make_float4(vi.x, vi.y, vi.z, fluid ? acc : 0.0f);
+        D.st_rec[2 * T.i + 1] = make_float4(D.dens[T.i], rfi, 0.f, 0.f);
+    }
+}
+
+// Setup (jeske23.py:612-649): g~_ij (compute_g_tilde_jeske23,
+// jeske23.py:118-188) kept as the list {j, w_ij = m_bar_ij g~_ij} per row
+// entry (the CG operator streams only that), the extra right-hand side b
+// (jeske23.py:190-237), the Jacobi inverse (jeske23.py:295-350),
+// rhs = v - M v + b, then r = rhs, z = M^-1 r, dv = 0, p_prev = 0; partial r.z.
+template <int G>
+__device__ __forceinline__ double st_setup_tile(const Dev& D, const SceneParams& P, const TileCtx& T) {
+    const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
+    float3 xi = make_float3(0.f, 0.f, 0.f), vi = xi;
+    float mi = 1.0f, rhoi = 1.0f, divi = 0.0f, rfi = 0.0f;
+    if (T.valid) {
+        const float4 a = D.xm[T.i];
+        xi = f3(a);
+        mi = a.w;
+        float4 r0, r1;
+        ld_rec(D.st_rec + 2 * T.i, r0, r1);
+        vi = f3(r0);
+        divi = r0.w;
+        rhoi = r1.x;
+        rfi = r1.y;
+    }
+    const bool fluid = T.valid && rfi != 0.0f;
+    const float d = P.st_d, hs = P.st_h, dt = P.dt;
+    float bx = 0.f, by = 0.f, bz = 0.f, sx = 0.f, sy = 0.f, sz = 0.f, ds = 0.f;
+    bool bad = false;
+    const int self = T.valid ? T.i : P.s_begin;
+    float2* wrow = D.st_w + (size_t)T.row * D.stride;
+    for (int k0 = 2 * T.lane; k0 < (fluid ? cnt : 0); k0 += G * PU) {
+        PairBatch b;
+        bad |= load_pairs<G>(D, T.row, xi, k0, cnt, self, P.s_begin, P.s_end, b);
+#pragma unroll
+        for (int u = 0; u < PU; ++u) {
+            const int k = k0 + (u >> 1) * 2 * G + (u & 1);
+            const int j = b.j[u];
+            const float4 xj4 = __ldg(D.xm + j);
+            float4 q0, q1;
+            ld_rec(D.st_rec + 2 * j, q0, q1);
+            const bool use = ((b.live >> u) & 1u) && q1.y != 0.0f;
+            const float3 xij = sub3(xi, f3(xj4));
+            const float r = sqrtf(norm2_rn(xij));
+            float gt = 0.0f;
+            float3 vij = make_float3(0.f, 0.f, 0.f);
+            if (use && r < hs) {
+                vij = sub3(vi, f3(q0));
+                const float rbar = 0.5f * (rhoi + q1.x);
+                const float W = st_W(r, d, hs);
+                const float3 gw = st_gradW(xij, r, d, hs);
+                const float gij = W / rbar;
+                const float tk = dot3(gw, vij) / rbar;
+                const float td = W / (2.0f * rbar * rbar) * (divi + q0.w);
+                gt = gij + dt * (tk - td);
+            }
+            const float mbar = 0.5f * (mi + xj4.w);
+            const float w = mbar * gt;
+            if (k < cnt) wrow[k] = make_float2(__int_as_float(j), use ? w : 0.0f);
+            if (use) {
+                ds += w;
+                if (gt != 0.0f) {
+                    bx += (mbar * xij.x) * gt;
+                    by += (mbar * xij.y) * gt;
+                    bz += (mbar * xij.z) * gt;
+                    sx += w * vij.x;
+                    sy += w * vij.y;
+                    sz += w * vij.z;
+                }
+            }
+        }
+    }
+    if (bad) flag_bad(D, T.i, 8);
+    bx = group_sum<G>(bx);
+    by = group_sum<G>(by);
+    bz = group_sum<G>(bz);
+    sx = group_sum<G>(sx);
+    sy = group_sum<G>(sy);
+    sz = group_sum<G>(sz);
+    ds = group_sum<G>(ds);
+    double part = 0.0;
+    if (T.valid && T.lane == 0) {
+        float3 bb = make_float3(0.f, 0.f, 0.f), mv = vi;
+        float inv = 1.0f;
+        if (fluid) {
+            const float sig = P.st_coeff;
+            const float fb = -dt * sig / mi;
+            bb = make_float3(fb * bx, fb * by, fb * bz);
+            const float f = dt * dt * sig / mi;
+            float dg = 1.0f + f * ds;
+            if (dg < 1.0e-12f) dg = 1.0e-12f;
+            inv = 1.0f / dg;
+            mv = make_float3(vi.x + f * sx, vi.y + f * sy, vi.z + f * sz);
+        }
+        float3 rh = make_float3(vi.x + (-1.0f) * mv.x, vi.y + (-1.0f) * mv.y, vi.z + (-1.0f) * mv.z);
+        rh = make_float3(rh.x + 1.0f * bb.x, rh.y + 1.0f * bb.y, rh.z + 1.0f * bb.z);
+        const float3 z = make_float3(inv * rh.x, inv * rh.y, inv * rh.z);
+        D.st_inv[T.i] = inv;
+        D.r[T.i] = make_float4(rh.x, rh.y, rh.z, 0.f);
+        D.cg0[2 * T.i] = make_float4(z.x, z.y, z.z, 0.f);
+        D.cg0[2 * T.i + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+        D.sol[T.i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        part = (double)dot3(rh, z);
+    }
+    return part;
+}
+
+// CG phase A (jeske23.py:540-545, 570-577): p = z + beta p_prev (formed on
+// the fly for the neighbours), (M p)_i = p_i + dt^2 sigma / m_i sum w_ij p_ij
+// (compute_Av_jeske23, jeske23.py:240-292); partial p.Mp.
+template <int G>
+__device__ __forceinline__ double st_a_tile(const Dev& D, const SceneParams& P, const TileCtx& T, float beta,
+                                            int it) {
+    const float4* cc = (it & 1) ? D.cg1 : D.cg0;  // {z, p_prev}
+    float4* cn = (it & 1) ? D.cg0 : D.cg1;
+    const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
+    const bool fluid = T.valid && D.rflu[T.i] != 0.0f;
+    float3 pi = make_float3(0.f, 0.f, 0.f);
+    float mi = 1.0f;
+    if (T.valid) {
+        mi = D.xm[T.i].w;
+        const float4 zi = cc[2 * T.i], qi = cc[2 * T.i + 1];
+        pi = make_float3(zi.x + beta * qi.x, zi.y + beta * qi.y, zi.z + beta * qi.z);
+    }
+    float sx = 0.f, sy = 0.f, sz = 0.f;
+    const int self = T.valid ? T.i : P.s_begin;
+    // list entries k, k+1 as one 16-byte load {j, w, j, w} (rows start on
+    // 512-byte boundaries and k is even)
+    const float4* wrow = reinterpret_cast<const float4*>(D.st_w + (size_t)T.row * D.stride);
+    for (int k0 = 2 * T.lane; k0 < (fluid ? cnt : 0); k0 += G * PU) {
+        int jj[PU];
+        float ww[PU];
+#pragma unroll
+        for (int u = 0; u < PU / 2; ++u) {
+            const int k = k0 + u * 2 * G;
+            float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (k < cnt) e = wrow[k >> 1];
+            const bool in0 = k < cnt, in1 = k + 1 < cnt;
+            jj[2 * u] = in0 ? __float_as_int(e.x) : self;
+            ww[2 * u] = in0 ? e.y : 0.0f;
+            jj[2 * u + 1] = in1 ? __float_as_int(e.z) : self;
+            ww[2 * u + 1] = in1 ? e.w : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < PU; ++u) {
+            const int j = (jj[u] >= P.s_begin && jj[u] < P.s_end) ? jj[u] : self;
+            float4 zj, qj;
+            ld_rec(cc + 2 * j, zj, qj);
+            const float3 pj = make_float3(zj.x + beta * qj.x, zj.y + beta * qj.y, zj.z + beta * qj.z);
+            const float w = ww[u];
+            if (w != 0.0f) {
+                sx += w * (pi.x - pj.x);
+                sy += w * (pi.y - pj.y);
+                sz += w * (pi.z - pj.z);
+            }
+        }
+    }
+    sx = group_sum<G>(sx);
+    sy = group_sum<G>(sy);
+    sz = group_sum<G>(sz);
+    double part = 0.0;
+    if (T.valid && T.lane == 0) {
+        float3 ap = pi;
+        if (fluid) {
+            const float f = P.dt * P.dt * P.st_coeff / mi;
+            ap = make_float3(pi.x + f * sx, pi.y + f * sy, pi.z + f * sz);
+        }
+        cn[2 * T.i + 1] = make_float4(pi.x, pi.y, pi.z, 0.f);
+        D.vap[T.i] = make_float4(ap.x, ap.y, ap.z, 0.f);
+        part = (double)dot3(pi, ap);
+    }
+    return part;
+}
+
+// CG phase B (jeske23.py:547-567), no neighbours: dv += alpha p,
+// r -= alpha M p, z = M^-1 r; partials r.r and r.z.
+template <int G>
+__device__ __forceinline__ void st_b_tile(const Dev& D, const TileCtx& T, float alpha, int it, double* part,
+                                          double* part2) {
+    *part = 0.0;
+    *part2 = 0.0;
+    if (!(T.valid && T.lane == 0)) return;
+    float4* cn = (it & 1) ? D.cg0 : D.cg1;  // own p; receives the new z
+    const float4 p4 = cn[2 * T.i + 1], ap = D.vap[T.i];
+    float4 x = D.sol[T.i], r = D.r[T.i];
+    x.x = x.x + alpha * p4.x;
+    x.y = x.y + alpha * p4.y;
+    x.z = x.z + alpha * p4.z;
+    const float na = -alpha;
+    r.x = r.x + na * ap.x;
+    r.y = r.y + na * ap.y;
+    r.z = r.z + na * ap.z;
+    D.sol[T.i] = x;
+    D.r[T.i] = r;
+    const float inv = D.st_inv[T.i];
+    const float3 rr = f3(r);
+    const float3 z = make_float3(inv * rr.x, inv * rr.y, inv * rr.z);
+    cn[2 * T.i] = make_float4(z.x, z.y, z.z, 0.f);
+    *part = (double)dot3(rr, rr);
+    *part2 = (double)dot3(rr, z);
+}
+
 // ---- one launch per phase (device-side control through graph conditionals)
 
 template <int G, int BLOCK>
@@ -1373,10 +1677,15 @@ __global__ void k_visc_begin(const Dev D) {
     if (blockIdx.x == 0 && threadIdx.x == 0) guard_begin(D);
     if (blockIdx.x == P.tile_begin && threadIdx.x == 0) {
         SceneCtl& C = D.ctl[tile.x];
-        C.v_on = (visc_on(P) && P.n_dyn > 0) ? 1 : 0;
-        C.v_active = 0;
-        C.v_total = 0;
+        force_begin(D, P, C);
     }
+}
+
+// Surface-tension divergence pass (one launch, no reduction).
+template <int G, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_st_div(const Dev D) {
+    const TileCtx T = tile_ctx<G>(D, blockIdx.x);
+    if (D.ctl[T.sc].v_on) st_div_tile<G>(D, D.scenes[T.sc], T);
 }
 
 template <int G, int BLOCK>
@@ -1387,7 +1696,8 @@ __global__ void __launch_bounds__(BLOCK) k_visc_setup(const Dev D) {
     __syncthreads();
     const bool active = sh_active != 0;
     double part = 0.0;
-    if (active) part = visc_setup_tile<G>(D, D.scenes[T.sc], T);
+    if (active)
+        part = D.force == FORCE_ST ? st_setup_tile<G>(D, D.scenes[T.sc], T) : visc_setup_tile<G>(D, D.scenes[T.sc], T);
     block_finish<BLOCK>(D, T.sc, active, part, K_V_SETUP);
 }
 
@@ -1405,7 +1715,9 @@ __global__ void __launch_bounds__(BLOCK) k_visc_a(const Dev D) {
     __syncthreads();
     const bool active = sh_active != 0;
     double part = 0.0;
-    if (active) part = visc_a_tile<G>(D, D.scenes[T.sc], T, sh_beta, sh_it);
+    if (active)
+        part = D.force == FORCE_ST ? st_a_tile<G>(D, D.scenes[T.sc], T, sh_beta, sh_it)
+                                   : visc_a_tile<G>(D, D.scenes[T.sc], T, sh_beta, sh_it);
     block_finish<BLOCK>(D, T.sc, active, part, K_V_A);
 }
 
@@ -1423,14 +1735,20 @@ __global__ void __launch_bounds__(BLOCK) k_visc_b(const Dev D) {
     __syncthreads();
     const bool active = sh_active != 0;
     double part = 0.0, part2 = 0.0;
-    if (active) visc_b_tile<G>(D, T, sh_alpha, sh_it, &part, &part2);
+    if (active) {
+        if (D.force == FORCE_ST) st_b_tile<G>(D, T, sh_alpha, sh_it, &part, &part2);
+        else visc_b_tile<G>(D, T, sh_alpha, sh_it, &part, &part2);
+    }
     block_finish<BLOCK>(D, T.sc, active, part, K_V_B, part2);
 }
 
 template <int G, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_visc_end(const Dev D) {
     const TileCtx T = tile_ctx<G>(D, blockIdx.x);
-    if (D.ctl[T.sc].v_on) visc_end_tile(D, T);
+    SceneCtl& C = D.ctl[T.sc];
+    if (!C.v_on) return;
+    visc_end_tile(D, T);
+    if (blockIdx.x == D.scenes[T.sc].tile_begin && threadIdx.x == 0) force_account(D, C);
 }
 
 // ---- the whole IP.solve in one persistent cooperative launch
@@ -1459,7 +1777,8 @@ __device__ __forceinline__ bool phase_active(const SceneCtl& C, int kind) {
         case K_RHS: return C.solve_pending != 0;
         case K_CG_A:
         case K_CG_B: return C.cg_active != 0;
-        case K_V_SETUP: return C.v_on != 0;
+        case K_V_SETUP:
+        case K_ST_DIV: return C.v_on != 0;
         default: return C.v_active != 0;
     }
 }
@@ -1662,10 +1981,18 @@ struct Phaser {
             const TileCtx T = tile_ctx<G>(D, t);
             const SceneCtl& C = sc_sh[T.sc];
             const SceneParams& P = D.scenes[T.sc];
-            double part, part2 = 0.0;
+            double part = 0.0, part2 = 0.0;
             if constexpr (VISC) {
-                if (kind == K_V_SETUP) part = visc_setup_tile<G>(D, P, T);
-                else if (kind == K_V_A) part = visc_a_tile<G>(D, P, T, (float)C.v_beta, C.v_it);
+                const bool st = D.force == FORCE_ST;
+                if (kind == K_ST_DIV) {
+                    st_div_tile<G>(D, P, T);
+                    continue;  // no reduction
+                }
+                if (kind == K_V_SETUP) part = st ? st_setup_tile<G>(D, P, T) : visc_setup_tile<G>(D, P, T);
+                else if (kind == K_V_A)
+                    part = st ? st_a_tile<G>(D, P, T, (float)C.v_beta, C.v_it)
+                              : visc_a_tile<G>(D, P, T, (float)C.v_beta, C.v_it);
+                else if (st) st_b_tile<G>(D, T, (float)C.v_alpha, C.v_it, &part, &part2);
                 else visc_b_tile<G>(D, T, (float)C.v_alpha, C.v_it, &part, &part2);
             } else {
                 if (kind == K_PACK) part = pack_tile<G>(D, P, T, C.outer_it);
@@ -1680,7 +2007,7 @@ struct Phaser {
                 D.partial[D.n_tiles + t] = tot2;
             }
         }
-        if (!barrier(kind)) return false;
+        if (!barrier(kind == K_ST_DIV ? -1 : kind)) return false;
         if (++phases > D.phase_limit) {
             // guard: every CTA reaches the same count; CTA 0 stops the scenes,
             // a barrier publishes it
@@ -1721,16 +2048,14 @@ __global__ void __launch_bounds__(BLOCK, persist_min_blocks<BLOCK>()) k_visc_per
     Phaser<G, BLOCK> ph(D, dyn_sh, red_sh, flag_sh, &any_sh);
     if (blockIdx.x == 0 && threadIdx.x == 0)
         for (int s = 0; s < D.n_scenes; ++s) {
-            const SceneParams& P = D.scenes[s];
             SceneCtl c = ctl_load(D.ctl + s);
-            c.v_on = (visc_on(P) && P.n_dyn > 0) ? 1 : 0;
-            c.v_active = 0;
-            c.v_total = 0;
+            force_begin(D, D.scenes[s], c);
             D.ctl[s] = c;
         }
     if (!ph.barrier(-1)) return;
     ph.refresh();
     if (!ph.any(K_V_SETUP)) return;
+    if (D.force == FORCE_ST && !ph.template run<true>(K_ST_DIV)) return;
     if (!ph.template run<true>(K_V_SETUP)) return;
     while (ph.any(K_V_A)) {
         if (!ph.template run<true>(K_V_A)) return;
@@ -1741,6 +2066,14 @@ __global__ void __launch_bounds__(BLOCK, persist_min_blocks<BLOCK>()) k_visc_per
         const TileCtx T = tile_ctx<G>(D, t);
         if (ph.sc_sh[T.sc].v_on) visc_end_tile(D, T);
     }
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        for (int s = 0; s < D.n_scenes; ++s) {
+            SceneCtl& c = D.ctl[s];
+            if (ph.sc_sh[s].v_on) {
+                c.v_total = ph.sc_sh[s].v_total;
+                force_account(D, c);
+            }
+        }
 }
 
 // The whole IP.solve of every scene in one persistent cooperative launch.
@@ -1798,7 +2131,6 @@ __global__ void __launch_bounds__(BLOCK, persist_min_blocks<BLOCK>()) k_ip_persi
             c.acc_solves += 1;
             c.acc_outer += c.outer_it;
             c.acc_cg += c.total_cg;
-            c.acc_visc += (D.visc_enabled && c.v_on) ? c.v_total : 0;
             if (c.final_err > c.acc_max_final_err) c.acc_max_final_err = c.final_err;
             if (c.status != IVP_OK_) {
                 c.acc_failed += 1;
@@ -1814,7 +2146,7 @@ __global__ void k_reset_counters(const Dev D) {
     if (s >= D.n_scenes) return;
     SceneCtl& C = D.ctl[s];
     C.acc_max_final_err = 0.0;
-    C.acc_solves = C.acc_outer = C.acc_cg = C.acc_failed = C.acc_last_failure = C.acc_visc = 0;
+    C.acc_solves = C.acc_outer = C.acc_cg = C.acc_failed = C.acc_last_failure = C.acc_visc = C.acc_st = 0;
     if (s == 0) D.flags->timeout = 0;
 }
 

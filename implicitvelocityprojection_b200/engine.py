@@ -65,6 +65,8 @@ def scene_desc(sc, offset: int) -> _lib.SceneDesc:
     d.cache_size = sc.cache_size
     d.viscosity_coeff = sc.viscosity_coeff
     d.viscosity_method = sc.viscosity_method
+    d.surface_tension_method = int(getattr(sc, "surface_tension_method", 0))
+    d.surface_tension_coeff = float(getattr(sc, "surface_tension_coeff", 0.0))
     return d
 
 
@@ -215,6 +217,11 @@ class Engine:
     def viscosity_solve(self, stream=None):
         """Weiler18.solve(coeff, dt) of every scene with implicit viscosity."""
         check(self.L.ivp_viscosity_solve(self._handle, ctypes.c_void_p(_stream_ptr(stream))), "ivp_viscosity_solve")
+
+    def surface_tension_solve(self, stream=None):
+        """Jeske23.solve(sigma, sigma, dt) of every scene with implicit surface tension."""
+        check(self.L.ivp_surface_tension_solve(self._handle, ctypes.c_void_p(_stream_ptr(stream))),
+              "ivp_surface_tension_solve")
 
     def apply_gravity(self, stream=None):
         check(self.L.ivp_apply_gravity(self._handle, ctypes.c_void_p(_stream_ptr(stream))), "ivp_apply_gravity")

@@ -1,8 +1,8 @@
 """Framework: the time-step orchestrator with the reference's interface
 (`scripts/framework.py:143-544`) for the IP pressure method.
 
-`forward()` runs one whole step -- gravity, implicit viscosity where
-enabled, the IP solve, advect + boundary clamp, neighbour rebuild, density
+`forward()` runs one whole step -- gravity, implicit surface tension and
+implicit viscosity where enabled, the IP solve, advect + boundary clamp, neighbour rebuild, density
 and Aii (framework.py:423-544) -- as one CUDA graph launch of the engine, then
 reads the solve statistics once (the reference synchronises many times per
 step).  `forward_many(n)` queues n steps and checks them once at the end.
@@ -38,14 +38,16 @@ class Framework:
         if pressure_method != 1:
             raise NotImplementedError(f"pressureMethod {pressure_method}: only IP (1) is implemented on this engine")
         self.pressure = IP(simulation_data, neighbour_search, config)
-        # non-pressure forces (framework.py:176-187): Weiler 2018 implicit
-        # viscosity runs inside the engine's step; the explicit forms and the
-        # surface-tension solvers are not built, so they must be disabled
+        # non-pressure forces (framework.py:176-187): Jeske 2023 implicit
+        # surface tension and Weiler 2018 implicit viscosity run inside the
+        # engine's step; the explicit forms (Akinci 2013 surface tension,
+        # XSPH-style viscosity) are not built, so they must be disabled
         if int(config.viscosity_method) != 1 and float(config.viscosity_coeff) != 0.0:
             raise NotImplementedError("explicit viscosity (viscosityMethod 0) is not implemented; set "
                                       "viscosityCoeff 0 or viscosityMethod 1")
-        if float(config.surface_tension_coeff) != 0.0:
-            raise NotImplementedError("surface tension is not implemented on this engine; set surfaceTensionCoeff 0")
+        if int(config.surface_tension_method) != 1 and float(config.surface_tension_coeff) != 0.0:
+            raise NotImplementedError("explicit surface tension (surfaceTensionMethod 0) is not implemented; set "
+                                      "surfaceTensionCoeff 0 or surfaceTensionMethod 1")
         self.elasticity = None
         self.pressure_enabled = bool(config.get_cfg("pressureEnabled", True))
         self._events = None

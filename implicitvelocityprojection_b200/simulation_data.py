@@ -36,6 +36,8 @@ class SceneSpec:
     cache_size: int = 60
     viscosity_coeff: float = 0.0
     viscosity_method: int = 0
+    surface_tension_coeff: float = 0.0
+    surface_tension_method: int = 0
 
 
 class SimulationData:
@@ -165,7 +167,11 @@ class SimulationData:
                        dt=float(cfg.dt if dt is None else dt), gravity=tuple(float(a) for a in g),
                        cache_size=self.cache_size,
                        viscosity_coeff=float(cfg.viscosity_coeff) if int(cfg.viscosity_method) == 1 else 0.0,
-                       viscosity_method=int(cfg.viscosity_method) if float(cfg.viscosity_coeff) > 0 else 0)
+                       viscosity_method=int(cfg.viscosity_method) if float(cfg.viscosity_coeff) > 0 else 0,
+                       surface_tension_coeff=float(cfg.surface_tension_coeff)
+                       if int(cfg.surface_tension_method) == 1 else 0.0,
+                       surface_tension_method=int(cfg.surface_tension_method)
+                       if float(cfg.surface_tension_coeff) > 0 else 0)
         if solver is not None:
             sp.omega = float(solver.omega)
             sp.tol_pcg = float(getattr(solver, "tol_pcg", 1e-6))

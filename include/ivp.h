@@ -59,7 +59,9 @@ typedef struct {
     int32_t cache_size;         /* neighborCacheSize (default 60) */
     float viscosity_coeff;      /* kinematic viscosity for Weiler18 (viscosityMethod 1) */
     int32_t viscosity_method;   /* 0 off, 1 Weiler 2018 implicit */
-    int32_t reserved[4];
+    int32_t surface_tension_method;  /* 0 off, 1 Jeske 2023 implicit (surfaceTensionMethod) */
+    float surface_tension_coeff;     /* sigma (surfaceTensionCoeff) */
+    int32_t reserved[2];
 } ivp_scene_desc;
 
 typedef struct {
@@ -109,13 +111,14 @@ typedef struct {
     double max_final_density_error;
     int64_t neighbour_pairs;      /* pairs in the scene's current neighbour lists */
     int64_t sum_visc_iters;       /* implicit-viscosity CG iterations */
+    int64_t sum_st_iters;         /* implicit surface-tension CG iterations */
 } ivp_solve_stats;
 
 /* Kernel ids reported by ivp_profile_step. */
 enum {
     IVP_K_GRAVITY = 0, IVP_K_SOLVE_BEGIN, IVP_K_PACK, IVP_K_RHS, IVP_K_CG_A, IVP_K_CG_B, IVP_K_SOLVE_END,
     IVP_K_DIVERGENCE, IVP_K_ADVECT, IVP_K_KEYS, IVP_K_SCAN_LOCAL, IVP_K_SCAN_ADD, IVP_K_PLACE, IVP_K_ORDER,
-    IVP_K_NBR_BUILD, IVP_K_STATIC_OUT, IVP_K_VISC, IVP_K_PERSISTENT, IVP_K_COUNT = 24
+    IVP_K_NBR_BUILD, IVP_K_STATIC_OUT, IVP_K_VISC, IVP_K_PERSISTENT, IVP_K_SURFACE_TENSION, IVP_K_COUNT = 24
 };
 
 typedef struct ivp_engine ivp_engine;
@@ -166,6 +169,14 @@ int ivp_ip_solve(ivp_engine* e, void* stream);
  * scene whose viscosity_method is 1 and viscosity_coeff > 0; updates the bound
  * velocities.  Uses the current neighbour lists and densities. */
 int ivp_viscosity_solve(ivp_engine* e, void* stream);
+
+/* Jeske23.solve(sigma, sigma, dt) (scripts/sim/forces/non_pressure/
+ * surface_tension/jeske23.py:585-655): implicit surface tension with Jacobi
+ * PCG for every scene whose surface_tension_method is 1 and
+ * surface_tension_coeff > 0; updates the bound velocities.  Uses the current
+ * neighbour lists and densities.  ivp_step runs it after gravity and before
+ * the viscosity (framework.py:400-421). */
+int ivp_surface_tension_solve(ivp_engine* e, void* stream);
 
 /* apply_gravity (framework.py:26-41). */
 int ivp_apply_gravity(ivp_engine* e, void* stream);

@@ -366,3 +366,93 @@ def test_row_formats_bitwise_equal(persistent):
         ca, ia = full.neighbours(i)
         cb, ib = comp.neighbours(i)
         assert np.array_equal(ca, cb) and np.array_equal(ia, ib)
+
+
+# ---------------------------------------------------- Jeske23 surface tension
+
+def _st_scene(g, x, v, sigma, visc=0.0):
+    sc = _scene_from_golden(g, x, v)
+    sc.surface_tension_method = 1
+    sc.surface_tension_coeff = float(sigma)
+    if visc > 0:
+        sc.viscosity_method = 1
+        sc.viscosity_coeff = float(visc)
+    return sc
+
+
+@pytest.mark.parametrize("persistent", [True, False])
+def test_surface_tension_solve_vs_golden(golden_dir, persistent):
+    g = _load(golden_dir, "st_solve.npz")
+    sc = _st_scene(g, g["x"], g["v0"], g["sigma"])
+    eng = _engine([sc], persistent=persistent)
+    eng.build()
+    dyn = sc.is_dynamic == 1
+    eng.surface_tension_solve()
+    v = eng.get("v")
+    assert _rel(v[dyn], g["v"][dyn]) < RTOL
+    assert _rel(v[dyn] - g["v0"][dyn], g["dv"][dyn]) < 5e-3  # the correction, relative to its own size
+    assert eng.raw_stats(0).sum_st_iters >= 1
+
+
+@pytest.mark.parametrize("persistent", [True, False])
+def test_column_st_steps_vs_golden(golden_dir, persistent):
+    """Steps with surface tension, viscosity and IP, each restarted from the
+    reference's previous state."""
+    g = _load(golden_dir, "column_st_steps.npz")
+    dyn = g["is_dynamic"] == 1
+    compared = 0
+    for s in range(g["x"].shape[0]):
+        x_prev = g["x0"] if s == 0 else g["x"][s - 1]
+        v_prev = g["v0"] if s == 0 else g["v"][s - 1]
+        sc = _st_scene(g, x_prev, v_prev, g["sigma"], float(g["viscosity"]))
+        sc.gravity = tuple(float(a) for a in g["gravity"])
+        eng = _engine([sc], persistent=persistent)
+        eng.build()
+        eng.step(1)
+        st = eng.stats(0)
+        assert st.status == 0
+        raw = eng.raw_stats(0)
+        assert raw.sum_st_iters >= 1 and raw.sum_visc_iters >= 1
+        if st.stats_outer_iters != int(g["outer"][s]):
+            continue
+        compared += 1
+        assert _rel(eng.get("v")[dyn], g["v"][s][dyn]) < RTOL, s
+        assert np.abs(eng.get("x")[dyn] - g["x"][s][dyn]).max() < 1e-6, s
+    assert compared >= g["x"].shape[0] - 1
+
+
+def test_surface_tension_paths_and_batch_bitwise():
+    """Surface tension + viscosity scenes: persistent and per-phase paths, and
+    a scene in a batch with other scenes, give identical bits."""
+    a = S.column_in_box((10, 18, 10), 0.02, (0.4, 0.8, 0.4), seed=51, viscosity_method=1, viscosity_coeff=1e-3,
+                        surface_tension_method=1, surface_tension_coeff=0.05)
+    b = S.small_dam_break(3000, seed=52)
+    c = S.random_column(2000, 2.0, seed=53, surface_tension_method=1, surface_tension_coeff=0.05)
+    p = _engine([a, b, c], persistent=True)
+    q = _engine([a, b, c], persistent=False)
+    for e in (p, q):
+        e.build()
+        e.step(3)
+    for i in range(3):
+        assert np.array_equal(p.get("v", i), q.get("v", i)), i
+        assert np.array_equal(p.get("x", i), q.get("x", i)), i
+    alone = _engine([a])
+    alone.build()
+    alone.step(3)
+    assert np.array_equal(alone.get("v"), p.get("v", 0))
+    assert p.raw_stats(0).sum_st_iters > 0 and p.raw_stats(1).sum_st_iters == 0
+
+
+def test_surface_tension_free_run_vs_oracle():
+    """A small surface-tension column stepped on the GPU and by the oracle."""
+    sc = S.column_in_box((8, 14, 8), 0.02, (0.3, 0.5, 0.3), seed=61, surface_tension_method=1,
+                         surface_tension_coeff=0.05)
+    eng = _engine([sc])
+    eng.build()
+    st = O.State.from_scene(sc)
+    st.rebuild()
+    dyn = sc.is_dynamic == 1
+    for s in range(5):
+        eng.step(1)
+        st.step(fast=True)
+    assert np.abs(eng.get("x")[dyn] - st.x[dyn]).max() < 5e-4
