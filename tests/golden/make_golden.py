@@ -204,6 +204,25 @@ def make_st_solve(out, sigma=0.05):
         dv=st.dv.numpy().copy(), div=st.div_arr.numpy().copy(), b=st.b_st.numpy().copy())
 
 
+def make_scene_ingest(out):
+    """The reference's scene loader (scene_loader.py:70-545) on
+    scene_blocks.json: fluid blocks, a generated cube body, boundary walls."""
+    from scripts.io.config_builder import SimConfig
+    from scripts.io.scene_loader import SceneLoader
+    from scripts.sim.simulation_data import SimulationData
+    cfg = SimConfig.from_json(os.path.join(HERE, "scene_blocks.json"))
+    loader = SceneLoader(cfg)
+    data = loader.prepare_scene()
+    ps = SimulationData(cfg)
+    loader.populate_scene(ps, data)
+    n = int(ps.particle_num)
+    np.savez_compressed(
+        out, x=ps.x.numpy()[:n].copy(), v=ps.v.numpy()[:n].copy(), is_dynamic=ps.is_dynamic.numpy()[:n].copy(),
+        material=ps.material.numpy()[:n].copy(), density0=ps.density0.numpy()[:n].copy(),
+        m=ps.m.numpy()[:n].copy(), object_id=ps.object_id.numpy()[:n].copy(),
+        domain_size=np.asarray(cfg.domain_size, np.float32), particle_radius=np.float64(cfg.particle_radius))
+
+
 def make_column_steps(out, steps, viscosity=0.0, sigma=0.0):
     from scripts.framework import Framework
     sc = _scene_column()
@@ -269,6 +288,7 @@ def main():
             "column_visc_steps": lambda: make_column_steps(os.path.join(HERE, "column_visc_steps.npz"), 10,
                                                            viscosity=0.01),
             "st_solve": lambda: make_st_solve(os.path.join(HERE, "st_solve.npz")),
+            "scene_ingest": lambda: make_scene_ingest(os.path.join(HERE, "scene_ingest.npz")),
             "column_st_steps": lambda: make_column_steps(os.path.join(HERE, "column_st_steps.npz"), 8,
                                                          viscosity=0.01, sigma=0.05)}
     for name, job in jobs.items():
