@@ -894,6 +894,22 @@ __device__ __forceinline__ bool load_pairs(const Dev& D, int row, float3 xi, int
     return bad;
 }
 
+// The pair loop of one row: batches of PU entries per lane, `body(b)`
+// consuming one batch.  (Requesting batch k+1's entries before batch k's
+// gathers spills at the persistent kernels' 64-register budget and measured
+// 20-35 % slower.)
+template <int G, class Body>
+__device__ __forceinline__ bool pair_loop(const Dev& D, int row, float3 xi, int cnt, int lane, int self, int lo,
+                                          int hi, Body&& body) {
+    bool bad = false;
+    for (int k0 = 2 * lane; k0 < cnt; k0 += G * PU) {
+        PairBatch b;
+        bad |= load_pairs<G>(D, row, xi, k0, cnt, self, lo, hi, b);
+        body(b);
+    }
+    return bad;
+}
+
 // Shared prologue of the neighbour-sum kernels: tile, scene, particle.
 struct TileCtx {
     int4 tile;
@@ -1030,11 +1046,8 @@ __device__ __forceinline__ double cga_tile(const Dev& D, const SceneParams& P, c
         pi = make_float3(ri.x + beta * qi.x, ri.y + beta * qi.y, ri.z + beta * qi.z);
     }
     float acc = 0.0f;
-    bool bad = false;
     const int self = T.valid ? T.i : P.s_begin;
-    for (int k0 = 2 * T.lane; k0 < cnt; k0 += G * PU) {
-        PairBatch b;
-        bad |= load_pairs<G>(D, T.row, xi, k0, cnt, self, P.s_begin, P.s_end, b);
+    const bool bad = pair_loop<G>(D, T.row, xi, cnt, T.lane, self, P.s_begin, P.s_end, [&](const PairBatch& b) {
 #pragma unroll
         for (int u = 0; u < PU; ++u) {
             const int j = b.j[u];
@@ -1043,7 +1056,7 @@ __device__ __forceinline__ double cga_tile(const Dev& D, const SceneParams& P, c
             const float3 pj = make_float3(rj.x + beta * qj.x, rj.y + beta * qj.y, rj.z + beta * qj.z);
             acc += dot3(sub3(pi, pj), b.J[u]);
         }
-    }
+    });
     if (bad) flag_bad(D, T.i, 3);
     acc = group_sum<G>(acc);
     double part = 0.0;
@@ -1075,11 +1088,8 @@ __device__ __forceinline__ double cgb_tile(const Dev& D, const SceneParams& P, c
         yi = D.y[T.i];
     }
     float ax = 0.0f, ay = 0.0f, az = 0.0f;
-    bool bad = false;
     const int self = T.valid ? T.i : P.s_begin;
-    for (int k0 = 2 * T.lane; k0 < cnt; k0 += G * PU) {
-        PairBatch b;
-        bad |= load_pairs<G>(D, T.row, xi, k0, cnt, self, P.s_begin, P.s_end, b);
+    const bool bad = pair_loop<G>(D, T.row, xi, cnt, T.lane, self, P.s_begin, P.s_end, [&](const PairBatch& b) {
 #pragma unroll
         for (int u = 0; u < PU; ++u) {
             const float wgt = yi + mi * D.z[b.j[u]];
@@ -1087,7 +1097,7 @@ __device__ __forceinline__ double cgb_tile(const Dev& D, const SceneParams& P, c
             ay += wgt * b.J[u].y;
             az += wgt * b.J[u].z;
         }
-    }
+    });
     if (bad) flag_bad(D, T.i, 4);
     ax = group_sum<G>(ax);
     ay = group_sum<G>(ay);

@@ -143,8 +143,8 @@ class Engine:
     # ------------------------------------------------------------ arrays
     def _alloc_arrays(self, divergence: bool) -> dict:
         dev = self.device
-        x = np.concatenate([sc.x for sc in self.scenes]).astype(np.float32) if self.scenes else np.zeros((0, 3))
-        v = np.concatenate([sc.v for sc in self.scenes]).astype(np.float32)
+        x = np.ascontiguousarray(np.concatenate([sc.x for sc in self.scenes]), dtype=np.float32)
+        v = np.ascontiguousarray(np.concatenate([sc.v for sc in self.scenes]), dtype=np.float32)
         ms = [sc.masses() for sc in self.scenes]
         m = np.concatenate([a for a, _ in ms]).astype(np.float32)
         a = {

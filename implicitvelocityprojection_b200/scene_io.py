@@ -91,7 +91,7 @@ def load_scene(src: Union[str, dict], name: str = None) -> Scene:
     def add(x, v, rho, mat, dyn):
         n = x.shape[0]
         xs.append(np.asarray(x, np.float32))
-        vs.append(np.broadcast_to(np.asarray(v, np.float32), (n, 3)).astype(np.float32))
+        vs.append(np.ascontiguousarray(np.broadcast_to(np.asarray(v, np.float32), (n, 3)), dtype=np.float32))
         rhos.append(np.full(n, rho, np.float32))
         mats.append(np.full(n, mat, np.int32))
         dyns.append(np.full(n, dyn, np.int32))
@@ -151,7 +151,7 @@ def load_scene(src: Union[str, dict], name: str = None) -> Scene:
         surface_tension_method=int(conf.get("surfaceTensionMethod", 0)),
         surface_tension_coeff=float(conf.get("surfaceTensionCoeff", 0.01)),
     )
-    return Scene(x=x, v=np.concatenate(vs), is_dynamic=dyn, material=np.concatenate(mats),
+    return Scene(x=np.ascontiguousarray(x), v=np.ascontiguousarray(np.concatenate(vs)), is_dynamic=dyn, material=np.concatenate(mats),
                  density0=np.concatenate(rhos), particle_radius=radius,
                  domain_size=np.asarray(domain_size, dtype=np.float32), name=name or "scene", **kw)
 

@@ -107,11 +107,12 @@ class Server:
         self.chunk_steps = int(chunk_steps)
         self.budget = float(hbm_budget_bytes)
         self.keep_state = keep_state
+        self.device = device
         if engine_factory is None:
             from .engine import Engine
 
-            def engine_factory(scenes, _dev=device, _opt=options):
-                return Engine(list(scenes), device=_dev, options=_opt)
+            def engine_factory(scenes, arrays=None, _dev=device, _opt=options):
+                return Engine(list(scenes), device=_dev, options=_opt, arrays=arrays)
         self.engine_factory = engine_factory
         if footprint is None:
             from .engine import workspace_bytes
@@ -119,6 +120,31 @@ class Server:
             def footprint(sc, _opt=options):
                 return workspace_bytes([sc], _opt) + ARRAY_BYTES_PER_PARTICLE * sc.n
         self.footprint = footprint
+
+    _KEYS = ("x", "v", "m", "density0", "is_dynamic", "material", "density", "k")
+
+    def _carry(self, eng, members, active) -> dict:
+        """Bound arrays of the next engine, in `active` order: slices of the
+        current engine's tensors for continuing scenes, uploads for new ones."""
+        import torch
+        pos = {id(a): i for i, a in enumerate(members)}
+        parts = {k: [] for k in self._KEYS}
+        for a in active:
+            i = pos.get(id(a))
+            if i is not None:
+                sl = eng.scene_slice(i)
+                for k in self._KEYS:
+                    parts[k].append(eng.arrays[k][sl])
+                continue
+            sc = a.scene
+            m, _ = sc.masses()
+            dev = eng.arrays["x"].device
+            host = {"x": sc.x, "v": sc.v, "m": m, "density0": sc.density0,
+                    "is_dynamic": sc.is_dynamic.astype(np.int32), "material": sc.material.astype(np.int32),
+                    "density": sc.density0, "k": np.zeros(sc.n, np.float32)}
+            for k in self._KEYS:
+                parts[k].append(torch.from_numpy(np.ascontiguousarray(host[k])).to(dev, non_blocking=False))
+        return {k: torch.cat(v).contiguous() for k, v in parts.items()}
 
     def run(self, requests: Sequence[Request], realtime: bool = False,
             on_result: Optional[Callable[[Result], None]] = None) -> Report:
@@ -171,15 +197,21 @@ class Server:
             max_active = max(max_active, len(active))
             if dirty:
                 t0 = time.perf_counter()
+                arrays = None
                 if eng is not None:
-                    # continuing scenes carry their state into the next engine
                     live = set(id(a) for a in active)
-                    for i, a in enumerate(members):
-                        if id(a) in live:
-                            a.scene.x = eng.get("x", i)
-                            a.scene.v = eng.get("v", i)
+                    if hasattr(eng, "arrays") and hasattr(eng, "scene_slice"):
+                        # continuing scenes carry their bound arrays into the
+                        # next engine on the device; new scenes are uploaded
+                        arrays = self._carry(eng, members, active)
+                    else:
+                        for i, a in enumerate(members):
+                            if id(a) in live:
+                                a.scene.x = eng.get("x", i)
+                                a.scene.v = eng.get("v", i)
                     del eng
-                eng = self.engine_factory([a.scene for a in active])
+                eng = self.engine_factory([a.scene for a in active], arrays) if arrays is not None \
+                    else self.engine_factory([a.scene for a in active])
                 eng.build()
                 members = list(active)
                 rebuilds += 1
