@@ -199,6 +199,7 @@ struct Dev {
     // the persistent solve runs the viscosity phases (set on step launches)
     int visc_enabled;
     int force;               // implicit non-pressure solve of this launch: 0 viscosity, 1 surface tension
+    int bar_all_reduce;      // persistent solve: every CTA reduces the (few) partials itself
     // persistent solve: grid-barrier words and the phase budget
     unsigned* bar_count;
     unsigned* bar_gen;

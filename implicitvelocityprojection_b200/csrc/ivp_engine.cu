@@ -66,7 +66,7 @@ struct ivp_engine {
     bool any_st = false;
     // persistent solve
     bool persistent = false;
-    int coop_grid = 0, coop_grid_visc = 0;
+    int coop_grid = 0, coop_grid_visc = 0, coop_grid_st = 0;
     size_t coop_smem = 0;
     // graphs
     cudaGraph_t graph_step = nullptr, graph_solve = nullptr, graph_build = nullptr;
@@ -186,15 +186,16 @@ struct Kern {
 };
 
 struct KernelSet {
-    DevKernel pack, rhs, cg_a, cg_b, dens, aii, div, persist, v_setup, v_a, v_b, v_end, v_persist, st_div;
+    DevKernel pack, rhs, cg_a, cg_b, dens, aii, div, persist, v_setup, v_a, v_b, v_end, v_persist, st_div,
+        st_persist;
 };
 
 template <int G, int B>
 KernelSet make_set() {
     return {Kern<G, B>::pack(), Kern<G, B>::rhs(), Kern<G, B>::cg_a(), Kern<G, B>::cg_b(),
             Kern<G, B>::dens(), Kern<G, B>::aii(), Kern<G, B>::div(), k_ip_persistent<G, B>,
-            k_visc_setup<G, B>, k_visc_a<G, B>, k_visc_b<G, B>, k_visc_end<G, B>, k_visc_persistent<G, B>,
-            k_st_div<G, B>};
+            k_visc_setup<G, B>, k_visc_a<G, B>, k_visc_b<G, B>, k_visc_end<G, B>,
+            k_force_persistent<G, B, FORCE_VISC>, k_st_div<G, B>, k_force_persistent<G, B, FORCE_ST>};
 }
 
 // Instantiated launch shapes: G lanes per particle x {128, 256} threads.
@@ -403,8 +404,10 @@ int emit_force_persistent(ivp_engine* e, Launcher& L, int force) {
     if (force == FORCE_ST)
         CKS(L.dev(IVP_K_SURFACE_TENSION, k_slot_velocity, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, copy));
     void* args[] = {&copy};
-    return L.kernel(force == FORCE_ST ? IVP_K_SURFACE_TENSION : IVP_K_VISC, (const void*)K.v_persist,
-                    dim3(e->coop_grid_visc), dim3(e->BLOCK), args, e->coop_smem, true);
+    return L.kernel(force == FORCE_ST ? IVP_K_SURFACE_TENSION : IVP_K_VISC,
+                    (const void*)(force == FORCE_ST ? K.st_persist : K.v_persist),
+                    dim3(force == FORCE_ST ? e->coop_grid_st : e->coop_grid_visc), dim3(e->BLOCK), args, e->coop_smem,
+                    true);
 }
 
 // Non-pressure forces in the reference's order (framework.py:400-421):
@@ -625,7 +628,7 @@ void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
     P.off[i++] = L.add(sizeof(float) * N);                  // 26 fk
     P.off[i++] = L.add((P.compact ? sizeof(float2) : sizeof(float4)) * (size_t)P.n_dyn * (size_t)o->list_stride);  // 27 nbr
     P.off[i++] = L.add(sizeof(int) * std::max<size_t>((size_t)P.n_dyn, 1));       // 28 nbr_cnt
-    P.off[i++] = L.add(2 * sizeof(double) * NT);            // 29 partial (two per tile)
+    P.off[i++] = L.add(4 * sizeof(double) * NT);            // 29 partial (two per tile, two phase buffers)
     P.off[i++] = L.add(sizeof(int) * S);                    // 30 scene_counter
     P.off[i++] = L.add(sizeof(int));                        // 31 launch_counter
     P.off[i++] = L.add(sizeof(Flags));                      // 32 flags
@@ -768,6 +771,10 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
     D.n_keys = e->n_keys;
     D.stride = opt->list_stride;
     D.compact = P.compact ? 1 : 0;
+    // few partials: every CTA of the persistent solve sums them itself
+    // (2 x 8 B x tiles read per CTA per phase) instead of waiting for the
+    // last CTA's decisions to travel back
+    D.bar_all_reduce = (n_scenes <= 2 && (int)P.tiles.size() <= 4096) ? 1 : 0;
     D.hist_len = opt->max_hist;
     D.n_total = e->n_total;
 
@@ -811,12 +818,15 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)K.persist, e->BLOCK, e->coop_smem) ==
                 cudaSuccess &&
             per_sm > 0) {
-            int per_sm_v = 0;
+            int per_sm_v = 0, per_sm_s = 0;
             if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_v, (const void*)K.v_persist, e->BLOCK,
                                                               e->coop_smem) == cudaSuccess &&
-                per_sm_v > 0) {
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_s, (const void*)K.st_persist, e->BLOCK,
+                                                              e->coop_smem) == cudaSuccess &&
+                per_sm_v > 0 && per_sm_s > 0) {
                 e->coop_grid = std::min(e->n_tiles, per_sm * nsm);
                 e->coop_grid_visc = std::min(e->n_tiles, per_sm_v * nsm);
+                e->coop_grid_st = std::min(e->n_tiles, per_sm_s * nsm);
                 e->persistent = true;
             }
         }

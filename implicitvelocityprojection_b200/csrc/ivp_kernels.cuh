@@ -19,6 +19,7 @@ namespace ivp {
 // its setup (no reduction)
 enum Kind { K_PACK = 0, K_RHS = 1, K_CG_A = 2, K_CG_B = 3, K_V_SETUP = 4, K_V_A = 5, K_V_B = 6, K_ST_DIV = 7 };
 constexpr int FORCE_VISC = 0, FORCE_ST = 1;
+constexpr int MODE_IP = 0, MODE_FORCE = 1;
 
 constexpr int IVP_OK_ = 0, IVP_NOT_SPD_ = 1, IVP_NOT_CONVERGED_ = 2, IVP_TIMEOUT_ = 6;
 
@@ -1806,9 +1807,90 @@ __device__ __forceinline__ SceneCtl ctl_load(const SceneCtl* p) {
 // more are spread over the warps, one scene per warp.
 constexpr int kBlockSumScenes = 2;
 
+// Scene sums of a phase's tile partials (`partial`, second partial at
+// `partial + n_tiles`) into sum_sh / sum_sh2, then every active scene's
+// decision on the CTA's control-block copies.  `publish`: this CTA writes the
+// decided blocks (and the history) to global memory.
 template <int BLOCK>
-__device__ bool grid_reduce_barrier(const Dev& D, int kind, int* sh_flag, double* sum_sh, double* sum_sh2,
-                                    SceneCtl* sc_sh, double* red_sh) {
+__device__ void reduce_and_decide(const Dev& D, int kind, const double* partial, double* sum_sh, double* sum_sh2,
+                                  SceneCtl* sc_sh, double* red_sh, bool publish) {
+    const int ns = D.n_scenes;
+    if (ns <= kBlockSumScenes) {
+        for (int s = 0; s < ns; ++s) {
+            if (!phase_active(sc_sh[s], kind)) continue;
+            const SceneParams& P = D.scenes[s];
+            const double v = scene_sum_block<BLOCK>(partial, P.tile_begin, P.tile_end, red_sh);
+            const double v2 =
+                kind == K_V_B ? scene_sum_block<BLOCK>(partial + D.n_tiles, P.tile_begin, P.tile_end, red_sh) : 0.0;
+            if (threadIdx.x == 0) {
+                sum_sh[s] = v;
+                sum_sh2[s] = v2;
+            }
+        }
+    } else {
+        const int warp = threadIdx.x >> 5;
+        for (int s = warp; s < ns; s += BLOCK / 32) {
+            if (!phase_active(sc_sh[s], kind)) continue;
+            const SceneParams& P = D.scenes[s];
+            const double v = scene_sum_warp(partial, P.tile_begin, P.tile_end);
+            const double v2 = kind == K_V_B ? scene_sum_warp(partial + D.n_tiles, P.tile_begin, P.tile_end) : 0.0;
+            if ((threadIdx.x & 31) == 0) {
+                sum_sh[s] = v;
+                sum_sh2[s] = v2;
+            }
+        }
+    }
+    __syncthreads();
+    for (int s = threadIdx.x; s < ns; s += BLOCK) {
+        SceneCtl& c = sc_sh[s];
+        if (!phase_active(c, kind)) continue;
+        scene_decide(D, D.scenes[s], c, kind, sum_sh[s], publish, sum_sh2[s]);
+        if (publish) {
+            D.ctl[s] = c;
+            __threadfence();
+        }
+    }
+    __syncthreads();
+}
+
+// Barrier in which every CTA reduces: after all CTAs arrived (one monotonic
+// arrival counter, `target` = this barrier's count), each CTA sums the
+// partials and runs the decisions itself -- same inputs, same code, same
+// bits -- so no control block has to travel back.  CTA 0 publishes them.
+// Used when the partials are few (one or two scenes); the partials alternate
+// between two buffers by barrier parity, so a CTA that runs ahead into the
+// next phase never overwrites partials another CTA is still reading.
+template <int BLOCK>
+__device__ bool grid_all_reduce_barrier(const Dev& D, int kind, const double* partial, int* sh_flag,
+                                        double* sum_sh, double* sum_sh2, SceneCtl* sc_sh, double* red_sh,
+                                        unsigned target) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(D.bar_count, 1u);
+        volatile unsigned* cnt = D.bar_count;
+        int ok = 1;
+        const unsigned long long t0 = globaltimer_ns();
+        while ((int)(*cnt - target) < 0) {
+            __nanosleep(32);
+            if (globaltimer_ns() - t0 > kBarrierLimitNs) {
+                ok = 0;
+                D.flags->timeout = 1;
+                break;
+            }
+        }
+        __threadfence();
+        sh_flag[1] = ok;
+    }
+    __syncthreads();
+    if (!sh_flag[1]) return false;
+    if (kind >= 0) reduce_and_decide<BLOCK>(D, kind, partial, sum_sh, sum_sh2, sc_sh, red_sh, blockIdx.x == 0);
+    return true;
+}
+
+template <int BLOCK>
+__device__ bool grid_reduce_barrier(const Dev& D, int kind, const double* partial, int* sh_flag, double* sum_sh,
+                                    double* sum_sh2, SceneCtl* sc_sh, double* red_sh) {
     unsigned g = 0;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -1820,44 +1902,7 @@ __device__ bool grid_reduce_barrier(const Dev& D, int kind, int* sh_flag, double
     __syncthreads();
     if (sh_flag[0]) {
         __threadfence();
-        if (kind >= 0) {
-            const int ns = D.n_scenes;
-            if (ns <= kBlockSumScenes) {
-                for (int s = 0; s < ns; ++s) {
-                    if (!phase_active(sc_sh[s], kind)) continue;
-                    const SceneParams& P = D.scenes[s];
-                    const double v = scene_sum_block<BLOCK>(D.partial, P.tile_begin, P.tile_end, red_sh);
-                    const double v2 =
-                        kind == K_V_B ? scene_sum_block<BLOCK>(D.partial + D.n_tiles, P.tile_begin, P.tile_end, red_sh)
-                                      : 0.0;
-                    if (threadIdx.x == 0) {
-                        sum_sh[s] = v;
-                        sum_sh2[s] = v2;
-                    }
-                }
-            } else {
-                const int warp = threadIdx.x >> 5;
-                for (int s = warp; s < ns; s += BLOCK / 32) {
-                    if (!phase_active(sc_sh[s], kind)) continue;
-                    const SceneParams& P = D.scenes[s];
-                    const double v = scene_sum_warp(D.partial, P.tile_begin, P.tile_end);
-                    const double v2 =
-                        kind == K_V_B ? scene_sum_warp(D.partial + D.n_tiles, P.tile_begin, P.tile_end) : 0.0;
-                    if ((threadIdx.x & 31) == 0) {
-                        sum_sh[s] = v;
-                        sum_sh2[s] = v2;
-                    }
-                }
-            }
-            __syncthreads();
-            for (int s = threadIdx.x; s < ns; s += BLOCK) {
-                SceneCtl& c = sc_sh[s];
-                if (!phase_active(c, kind)) continue;
-                scene_decide(D, D.scenes[s], c, kind, sum_sh[s], true, sum_sh2[s]);
-                D.ctl[s] = c;
-                __threadfence();
-            }
-        }
+        if (kind >= 0) reduce_and_decide<BLOCK>(D, kind, partial, sum_sh, sum_sh2, sc_sh, red_sh, true);
         __syncthreads();
         if (threadIdx.x == 0) {
             *D.bar_count = 0;
@@ -1952,8 +1997,18 @@ struct Phaser {
         return lo;
     }
 
+    unsigned nbar = 0;  // barriers passed by this launch (the same count in every CTA)
+
+    // this phase's partial buffer (two per tile, alternating by barrier parity)
+    __device__ double* partials() const { return D.partial + (size_t)(nbar & 1u) * 2u * (size_t)D.n_tiles; }
+
     __device__ bool barrier(int kind) {
-        return grid_reduce_barrier<BLOCK>(D, kind, flag_sh, sum_sh, sum_sh2, sc_sh, red_sh);
+        const double* part = partials();
+        ++nbar;
+        if (D.bar_all_reduce)
+            return grid_all_reduce_barrier<BLOCK>(D, kind, part, flag_sh, sum_sh, sum_sh2, sc_sh, red_sh,
+                                                  nbar * gridDim.x);
+        return grid_reduce_barrier<BLOCK>(D, kind, part, flag_sh, sum_sh, sum_sh2, sc_sh, red_sh);
     }
 
     __device__ void refresh() {
@@ -1978,7 +2033,10 @@ struct Phaser {
     // The phase's active tiles (those of the scenes active in `kind`) are
     // split evenly over the grid, so scenes that converged early leave no CTA
     // idle while others work through a converging scene's tiles.
-    template <bool VISC>
+    // MODE selects the phase family compiled into the kernel: MODE_IP, or a
+    // non-pressure force (FORCE_VISC / FORCE_ST as MODE_FORCE + force); each
+    // persistent kernel keeps its own register budget
+    template <int MODE>
     __device__ bool run(int kind) {
         active_prefix(kind);
         const int A = act_sh[D.n_scenes];
@@ -1992,17 +2050,17 @@ struct Phaser {
             const SceneCtl& C = sc_sh[T.sc];
             const SceneParams& P = D.scenes[T.sc];
             double part = 0.0, part2 = 0.0;
-            if constexpr (VISC) {
-                const bool st = D.force == FORCE_ST;
+            if constexpr (MODE == MODE_FORCE + FORCE_ST) {
                 if (kind == K_ST_DIV) {
                     st_div_tile<G>(D, P, T);
                     continue;  // no reduction
                 }
-                if (kind == K_V_SETUP) part = st ? st_setup_tile<G>(D, P, T) : visc_setup_tile<G>(D, P, T);
-                else if (kind == K_V_A)
-                    part = st ? st_a_tile<G>(D, P, T, (float)C.v_beta, C.v_it)
-                              : visc_a_tile<G>(D, P, T, (float)C.v_beta, C.v_it);
-                else if (st) st_b_tile<G>(D, T, (float)C.v_alpha, C.v_it, &part, &part2);
+                if (kind == K_V_SETUP) part = st_setup_tile<G>(D, P, T);
+                else if (kind == K_V_A) part = st_a_tile<G>(D, P, T, (float)C.v_beta, C.v_it);
+                else st_b_tile<G>(D, T, (float)C.v_alpha, C.v_it, &part, &part2);
+            } else if constexpr (MODE == MODE_FORCE + FORCE_VISC) {
+                if (kind == K_V_SETUP) part = visc_setup_tile<G>(D, P, T);
+                else if (kind == K_V_A) part = visc_a_tile<G>(D, P, T, (float)C.v_beta, C.v_it);
                 else visc_b_tile<G>(D, T, (float)C.v_alpha, C.v_it, &part, &part2);
             } else {
                 if (kind == K_PACK) part = pack_tile<G>(D, P, T, C.outer_it);
@@ -2013,8 +2071,9 @@ struct Phaser {
             const double tot = block_sum_d<BLOCK>(part, red_sh);
             const double tot2 = kind == K_V_B ? block_sum_d<BLOCK>(part2, red_sh) : 0.0;
             if (threadIdx.x == 0) {
-                D.partial[t] = tot;
-                D.partial[D.n_tiles + t] = tot2;
+                double* pb = partials();
+                pb[t] = tot;
+                pb[D.n_tiles + t] = tot2;
             }
         }
         if (!barrier(kind == K_ST_DIV ? -1 : kind)) return false;
@@ -2033,8 +2092,11 @@ struct Phaser {
                 D.flags->timeout = 1;
             }
             if (!barrier(-1)) return false;
+            refresh();
+            return true;
         }
-        refresh();
+        // the all-reduce barrier decided on this CTA's own copies already
+        if (!D.bar_all_reduce) refresh();
         return true;
     }
 };
@@ -2048,10 +2110,12 @@ struct Phaser {
 template <int BLOCK>
 constexpr int persist_min_blocks() { return IVP_PERSIST_THREADS / BLOCK > 0 ? IVP_PERSIST_THREADS / BLOCK : 1; }
 
-// Weiler 2018 implicit viscosity of every scene that enables it, in one
-// persistent cooperative launch (weiler18.py:371-401).
-template <int G, int BLOCK>
-__global__ void __launch_bounds__(BLOCK, persist_min_blocks<BLOCK>()) k_visc_persistent(const Dev D) {
+// One implicit non-pressure solve of every scene that enables it, in one
+// persistent cooperative launch: Weiler 2018 viscosity (weiler18.py:371-401)
+// or Jeske 2023 surface tension (jeske23.py:585-655); D.force == FORCE.
+template <int G, int BLOCK, int FORCE>
+__global__ void __launch_bounds__(BLOCK, persist_min_blocks<BLOCK>()) k_force_persistent(const Dev D) {
+    constexpr int M = MODE_FORCE + FORCE;
     extern __shared__ double dyn_sh[];
     __shared__ double red_sh[128];
     __shared__ int flag_sh[2], any_sh;
@@ -2065,12 +2129,12 @@ __global__ void __launch_bounds__(BLOCK, persist_min_blocks<BLOCK>()) k_visc_per
     if (!ph.barrier(-1)) return;
     ph.refresh();
     if (!ph.any(K_V_SETUP)) return;
-    if (D.force == FORCE_ST && !ph.template run<true>(K_ST_DIV)) return;
-    if (!ph.template run<true>(K_V_SETUP)) return;
+    if (FORCE == FORCE_ST && !ph.template run<M>(K_ST_DIV)) return;
+    if (!ph.template run<M>(K_V_SETUP)) return;
     while (ph.any(K_V_A)) {
-        if (!ph.template run<true>(K_V_A)) return;
+        if (!ph.template run<M>(K_V_A)) return;
         if (!ph.any(K_V_B)) break;
-        if (!ph.template run<true>(K_V_B)) return;
+        if (!ph.template run<M>(K_V_B)) return;
     }
     for (int t = ph.t0; t < ph.t1; ++t) {
         const TileCtx T = tile_ctx<G>(D, t);
@@ -2110,13 +2174,13 @@ __global__ void __launch_bounds__(BLOCK, persist_min_blocks<BLOCK>()) k_ip_persi
     if (!ph.barrier(-1)) return;
     ph.refresh();
     while (ph.any(K_PACK)) {
-        if (!ph.template run<false>(K_PACK)) return;
+        if (!ph.template run<MODE_IP>(K_PACK)) return;
         if (!ph.any(K_RHS)) break;
-        if (!ph.template run<false>(K_RHS)) return;
+        if (!ph.template run<MODE_IP>(K_RHS)) return;
         while (ph.any(K_CG_A)) {
-            if (!ph.template run<false>(K_CG_A)) return;
+            if (!ph.template run<MODE_IP>(K_CG_A)) return;
             if (!ph.any(K_CG_B)) break;
-            if (!ph.template run<false>(K_CG_B)) return;
+            if (!ph.template run<MODE_IP>(K_CG_B)) return;
         }
     }
     // epilogue (ip.py:394-404): v = d/dt for scenes that did not raise,
