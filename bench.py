@@ -39,6 +39,7 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
 METRIC = "particle-steps/s at <=0.1% avg density error"
+ROW_FORMATS = {"full": 1, "compact": 2, "bf16": 3}
 UNIT = "particle-steps/s"
 
 
@@ -296,7 +297,8 @@ def run_ours(args, rank, world, local_rank):
         scenes = shard(scenes, rank, world)
     n_dyn = sum(sc.n_dynamic for sc in scenes)
     opts = EngineOptions(lanes_per_particle=args.lanes,
-                         particles_per_block=args.ppb or 256 // args.lanes, persistent=not args.per_phase)
+                         particles_per_block=args.ppb or 256 // args.lanes, persistent=not args.per_phase,
+                         row_format=ROW_FORMATS[args.row_format])
     eng = Engine(scenes, device=str(dev), options=opts, divergence=True)
     eng.build()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
@@ -378,10 +380,11 @@ def run_ours(args, rank, world, local_rank):
         so = sum(r.sum_outer_iters for r in raws)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-                "scaling": "strong" if sharded else "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "scaling": "strong" if sharded else "weak", "vs_baseline": None,
+                "dtype": "f32 (bf16 gradients)" if args.row_format == "bf16" else "f32", "data": "synthetic",
                 "config": {**workload_config(scenes, args.workload),
                            "parallelism": f"scenes sharded over {world} ranks" if sharded else f"replicas x{world}",
-                           "lanes_per_particle": args.lanes,
+                           "lanes_per_particle": args.lanes, "row_format": args.row_format,
                            "particles_per_block": opts.particles_per_block,
                            "solve": "per-phase launches" if args.per_phase else "persistent cooperative kernel"},
                 "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
@@ -586,6 +589,8 @@ def main():
     ap.add_argument("--served-duration", type=float, default=30.0, help="served: seconds of arrivals")
     ap.add_argument("--chunk-steps", type=int, default=50, help="served: steps between re-plans")
     ap.add_argument("--hbm-budget-gb", type=float, default=150.0, help="served: admission budget")
+    ap.add_argument("--row-format", default="full", choices=sorted(ROW_FORMATS),
+                    help="neighbour rows: full FP32 gradients (default), compact {j, w}, or bf16 gradients")
     ap.add_argument("--shard", action="store_true",
                     help="batched workloads under torchrun: split the scenes over the ranks instead of replicas")
     ap.add_argument("--serial-steps", type=int, default=5,

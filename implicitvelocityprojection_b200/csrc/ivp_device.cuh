@@ -23,6 +23,7 @@
 //     two scenes, so per-scene reductions are per-CTA partials summed in a
 //     fixed order by the scene's last CTA (deterministic FP64).
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -179,8 +180,11 @@ struct Dev {
     float* q;                // fk / m
     float* z;                // y / m
     // neighbour rows
-    float4* nbr;             // neighbour rows: float4 {J, j} entries, or float2 {j, w} when compact
-    int compact;
+    // neighbour rows, by row_fmt: ROW_FULL float4 {J, j}; ROW_COMPACT float2
+    // {j, w}; ROW_BF16 int j here and the gradient as 3 bf16 in nbr_g
+    float4* nbr;
+    unsigned short* nbr_g;
+    int row_fmt;
     int* nbr_cnt;
     int stride;
     // reductions
@@ -282,19 +286,34 @@ __device__ __forceinline__ float group_sum(float v) {
     return v;
 }
 
-// Entry k of a neighbour row in either layout: full rows hold {J_ij, j},
-// compact rows {j, w_ij} with J_ij = w_ij (x_i - x_j).
+constexpr int ROW_FULL = 0, ROW_COMPACT = 1, ROW_BF16 = 2;
+
+__device__ __forceinline__ float bf16_lo(unsigned w) { return __uint_as_float(w << 16); }
+__device__ __forceinline__ float bf16_hi(unsigned w) { return __uint_as_float(w & 0xffff0000u); }
+__device__ __forceinline__ unsigned short bf16_bits(float f) { return __bfloat16_as_ushort(__float2bfloat16_rn(f)); }
+
+// Entry k of a neighbour row in any layout: full rows hold {J_ij, j},
+// compact rows {j, w_ij} with J_ij = w_ij (x_i - x_j), bf16 rows j and J_ij
+// rounded to bf16.
 __device__ __forceinline__ int row_j(const Dev& D, int row, int k) {
     const size_t e = (size_t)row * D.stride + k;
-    return D.compact ? __float_as_int(reinterpret_cast<const float2*>(D.nbr)[e].x) : __float_as_int(D.nbr[e].w);
+    if (D.row_fmt == ROW_FULL) return __float_as_int(D.nbr[e].w);
+    if (D.row_fmt == ROW_COMPACT) return __float_as_int(reinterpret_cast<const float2*>(D.nbr)[e].x);
+    return reinterpret_cast<const int*>(D.nbr)[e];
 }
 
 __device__ __forceinline__ float3 row_J(const Dev& D, int row, int k, float3 xi, int* j) {
     const size_t e = (size_t)row * D.stride + k;
-    if (!D.compact) {
+    if (D.row_fmt == ROW_FULL) {
         const float4 v = D.nbr[e];
         *j = __float_as_int(v.w);
         return f3(v);
+    }
+    if (D.row_fmt == ROW_BF16) {
+        *j = reinterpret_cast<const int*>(D.nbr)[e];
+        const unsigned short* g = D.nbr_g + 3 * e;
+        return make_float3(__uint_as_float((unsigned)g[0] << 16), __uint_as_float((unsigned)g[1] << 16),
+                           __uint_as_float((unsigned)g[2] << 16));
     }
     const float2 v = reinterpret_cast<const float2*>(D.nbr)[e];
     *j = __float_as_int(v.x);

@@ -479,7 +479,7 @@ int validate(const ivp_scene_desc* sc, int n, const ivp_options* o) {
             return IVP_ERR_BAD_ARG;
     }
     if (o->list_stride <= 0 || (o->list_stride & 1) || o->max_hist <= 0) return IVP_ERR_BAD_ARG;
-    if (o->row_format < 0 || o->row_format > 2) return IVP_ERR_BAD_ARG;
+    if (o->row_format < 0 || o->row_format > 3) return IVP_ERR_BAD_ARG;
     long expect = 0;
     for (int s = 0; s < n; ++s) {
         const ivp_scene_desc& d = sc[s];
@@ -506,7 +506,7 @@ struct Plan {
     std::vector<int4> tiles;
     std::vector<int4> segs;
     int n_total = 0, n_dyn = 0, n_keys = 0, scan_blocks = 0;
-    bool compact = false;  // neighbour rows as {j, w} (8 B entries)
+    int row_fmt = 0;       // ROW_FULL (16 B entries), ROW_COMPACT ({j, w}, 8 B), ROW_BF16 (4 B id + 6 B)
     bool any_st = false;   // some scene runs the implicit surface tension
     size_t off[56];
     Layout lay;
@@ -590,8 +590,9 @@ void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
     P.n_dyn = row_base;
     // compact rows halve the list memory; they cost one more gather per
     // pair, which outweighs the halved list stream on B200, so the default
-    // is full rows
-    P.compact = o->row_format == 2;
+    // is full rows.  bf16 rows (10 B per entry) are the reduced-precision
+    // variant of the gradient.
+    P.row_fmt = o->row_format == 2 ? ROW_COMPACT : o->row_format == 3 ? ROW_BF16 : ROW_FULL;
     for (int s = 0; s < n; ++s)
         if (scene_st(sc[s])) P.any_st = true;
     P.n_keys = key_base;
@@ -626,7 +627,8 @@ void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
     P.off[i++] = L.add(sizeof(float) * N);                  // 24 y
     P.off[i++] = L.add(sizeof(float) * N);                  // 25 s
     P.off[i++] = L.add(sizeof(float) * N);                  // 26 fk
-    P.off[i++] = L.add((P.compact ? sizeof(float2) : sizeof(float4)) * (size_t)P.n_dyn * (size_t)o->list_stride);  // 27 nbr
+    const size_t entry_bytes = P.row_fmt == ROW_FULL ? sizeof(float4) : P.row_fmt == ROW_COMPACT ? sizeof(float2) : sizeof(int);
+    P.off[i++] = L.add(entry_bytes * (size_t)P.n_dyn * (size_t)o->list_stride);  // 27 nbr (ids for bf16 rows)
     P.off[i++] = L.add(sizeof(int) * std::max<size_t>((size_t)P.n_dyn, 1));       // 28 nbr_cnt
     P.off[i++] = L.add(4 * sizeof(double) * NT);            // 29 partial (two per tile, two phase buffers)
     P.off[i++] = L.add(sizeof(int) * S);                    // 30 scene_counter
@@ -647,6 +649,8 @@ void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
     P.off[i++] = L.add(P.any_st ? sizeof(float2) * (size_t)P.n_dyn * (size_t)o->list_stride : 0);  // 45 st_w
     P.off[i++] = L.add(P.any_st ? 2 * sizeof(float4) * N : 0);       // 46 st_rec
     P.off[i++] = L.add(P.any_st ? sizeof(float) * N : 0);            // 47 st_inv
+    P.off[i++] = L.add(P.row_fmt == ROW_BF16 ? 3 * sizeof(unsigned short) * (size_t)P.n_dyn * (size_t)o->list_stride
+                                             : 0);                   // 48 bf16 gradients
 }
 
 cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
@@ -757,6 +761,7 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
     D.st_w = reinterpret_cast<float2*>(w + P.off[i++]);
     D.st_rec = reinterpret_cast<float4*>(w + P.off[i++]);
     D.st_inv = reinterpret_cast<float*>(w + P.off[i++]);
+    D.nbr_g = reinterpret_cast<unsigned short*>(w + P.off[i++]);
     D.n_segs = (int)P.segs.size();
     e->n_segs = D.n_segs;
     {
@@ -770,7 +775,7 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
     D.n_tiles = e->n_tiles;
     D.n_keys = e->n_keys;
     D.stride = opt->list_stride;
-    D.compact = P.compact ? 1 : 0;
+    D.row_fmt = P.row_fmt;
     // few partials: every CTA of the persistent solve sums them itself
     // (2 x 8 B x tiles read per CTA per phase) instead of waiting for the
     // last CTA's decisions to travel back

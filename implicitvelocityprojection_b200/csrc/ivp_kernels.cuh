@@ -603,8 +603,18 @@ __global__ void __launch_bounds__(256, 4) k_nbr_build(const Dev D) {
             // from the positions with the same three products
             const float w = mj * (sg * ir);
             const float3 J = make_float3(__fmul_rn(w, r.x), __fmul_rn(w, r.y), __fmul_rn(w, r.z));
-            if (D.compact) out2[k] = make_float2(__int_as_float(j), w);
-            else out[k] = make_float4(J.x, J.y, J.z, __int_as_float(j));
+            if (D.row_fmt == ROW_FULL) {
+                out[k] = make_float4(J.x, J.y, J.z, __int_as_float(j));
+            } else if (D.row_fmt == ROW_COMPACT) {
+                out2[k] = make_float2(__int_as_float(j), w);
+            } else {
+                const size_t e = (size_t)row * D.stride + k;
+                reinterpret_cast<int*>(D.nbr)[e] = j;
+                unsigned short* g = D.nbr_g + 3 * e;
+                g[0] = bf16_bits(J.x);
+                g[1] = bf16_bits(J.y);
+                g[2] = bf16_bits(J.z);
+            }
             rho += mj * cubic_Wq(rn * inv_h, ck);
             if (j < dyn_end) aii += dot3(J, J) * __frcp_rn(mj);
             jii = sub3(jii, J);
@@ -858,7 +868,31 @@ __device__ __forceinline__ bool load_pairs(const Dev& D, int row, float3 xi, int
                                            int hi, PairBatch& b) {
     bool bad = false;
     b.live = 0u;
-    if (!D.compact) {
+    if (D.row_fmt == ROW_BF16) {
+        // entries k, k+1 (k even): ids as one 8-byte load, gradients as
+        // three 4-byte words of bf16 pairs
+        const int2* __restrict__ ids = reinterpret_cast<const int2*>(reinterpret_cast<const int*>(D.nbr) +
+                                                                     (size_t)row * D.stride);
+        const unsigned* __restrict__ gw =
+            reinterpret_cast<const unsigned*>(D.nbr_g + 3 * (size_t)row * D.stride);
+#pragma unroll
+        for (int u = 0; u < PU / 2; ++u) {
+            const int k = k0 + u * 2 * G;
+            int2 jj = make_int2(self, self);
+            unsigned w0 = 0u, w1 = 0u, w2 = 0u;
+            if (k < cnt) {
+                jj = __ldg(ids + (k >> 1));
+                const unsigned* p = gw + (3 * k >> 1);
+                w0 = __ldg(p);
+                w1 = __ldg(p + 1);
+                w2 = __ldg(p + 2);
+            }
+            const float4 e0 = make_float4(bf16_lo(w0), bf16_hi(w0), bf16_lo(w1), __int_as_float(jj.x));
+            const float4 e1 = make_float4(bf16_hi(w1), bf16_lo(w2), bf16_hi(w2), __int_as_float(jj.y));
+            pair_entry(e0, k < cnt, self, lo, hi, b.j[2 * u], b.J[2 * u], bad, b.live, 2 * u);
+            pair_entry(e1, k + 1 < cnt, self, lo, hi, b.j[2 * u + 1], b.J[2 * u + 1], bad, b.live, 2 * u + 1);
+        }
+    } else if (D.row_fmt == ROW_FULL) {
         const float4* __restrict__ nb = D.nbr + (size_t)row * D.stride;
 #pragma unroll
         for (int u = 0; u < PU / 2; ++u) {

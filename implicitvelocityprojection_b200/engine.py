@@ -31,7 +31,7 @@ class EngineOptions:
     max_hist: int = 128
     use_graphs: bool = True
     persistent: bool = True
-    row_format: int = 0  # 0 auto, 1 full {J, j}, 2 compact {j, w}
+    row_format: int = 0  # 0 default (full), 1 full {J, j}, 2 compact {j, w}, 3 bf16 gradients
 
     def to_c(self) -> _lib.Options:
         o = _lib.Options()

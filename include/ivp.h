@@ -74,7 +74,9 @@ typedef struct {
                                      0: one launch per phase, loops as conditional graph nodes */
     int32_t row_format;           /* neighbour-row entries: 0 default (= 1), 1 full {m_j gradW_ij, j}
                                      (16 B), 2 compact {j, w_ij} (8 B, gradient rebuilt from the
-                                     positions: half the list memory, slower); bit-identical results */
+                                     positions: half the list memory, slower; bit-identical to 1),
+                                     3 bf16 (4 B id + the gradient in 3 bf16: the reduced-precision
+                                     variant, 10 B per entry) */
     int32_t reserved[1];
 } ivp_options;
 
