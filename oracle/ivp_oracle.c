@@ -549,6 +549,82 @@ void orc_advect_and_clamp(int n, float* x, float* v, const int* dyn, float dt, c
     }
 }
 
+/* ------------------------------------------------- PRJ (projected Jacobi) */
+
+/*
+ * PRJ.solve (prj.py:296-340) with solve_PJ (prj.py:138-192): dt_v_0 = dt v,
+ * cumulative dt^2 lambda from 0 (no warm start), then passes of
+ *   head (pj_head_fused, prj.py:17-55): dt_v = dt_v_0 - dt^2 J^T lambda / max(m, 1e-6)
+ *   tail (pj_tail_fused, prj.py:58-117): r = dt J dt_v + c,
+ *        lambda = max(lambda + omega r D^-1, 0), err = avg max(r / rho0, 0)
+ * stopping when (err < tol and pass >= 1) or pass >= max (the pass index is
+ * the update count).  v = dt_v / dt unless it raises (check_converged).
+ * `omega` is P->omega (PRJ uses 0.5, prj.py:127).
+ */
+int orc_prj_solve(int n, const orc_params* P, float dt, const float* density, const float* rho0, const float* m,
+                  const int* dyn, const int* count, const int* ids, const float* gradW, const float* kd, float* v,
+                  double* err_hist, orc_stats* st) {
+    int cache = P->cache_size;
+    size_t n3 = 3 * (size_t)n;
+    float* c = (float*)calloc(n, sizeof(float));
+    float* lam = (float*)calloc(n, sizeof(float));
+    float* t = (float*)calloc(n, sizeof(float));
+    float* v0 = (float*)calloc(n3, sizeof(float));
+    float* dv = (float*)calloc(n3, sizeof(float));
+    for (int i = 0; i < n; ++i) c[i] = dyn[i] ? density[i] - rho0[i] : 0.0f;
+    for (int i = 0; i < n; ++i)
+        if (dyn[i])
+            for (int q = 0; q < 3; ++q) v0[3 * i + q] = dt * v[3 * i + q];
+    memcpy(dv, v0, sizeof(float) * n3);
+    double err = 0.0;
+    int pass = 0, n_err = 0;
+    for (pass = 0;; ++pass) {
+        /* head */
+#pragma omp parallel for schedule(static)
+        for (int i = 0; i < n; ++i) {
+            if (!dyn[i]) continue;
+            float acc[3] = {0.0f, 0.0f, 0.0f};
+            int cnt = clamp_cnt(count[i], cache);
+            for (int k = 0; k < cnt; ++k) {
+                long b = (long)i * cache + k;
+                int j = ids[b];
+                const float* g = gradW + 3 * b;
+                float s = dyn[j] ? (m[j] * lam[i] + m[i] * lam[j]) : (m[j] * lam[i]);
+                for (int q = 0; q < 3; ++q) acc[q] = acc[q] + s * g[q];
+            }
+            float den = m[i] < 1e-6f ? 1e-6f : m[i];
+            for (int q = 0; q < 3; ++q) dv[3 * i + q] = v0[3 * i + q] - acc[q] / den;
+        }
+        /* tail: r = J dt_v + c (the lambda update reads only its own lambda) */
+        jx_plain(n, dv, m, dyn, cache, count, ids, gradW, t);
+        for (int i = 0; i < n; ++i) {
+            if (!dyn[i]) continue;
+            t[i] = t[i] + c[i];
+            float l = lam[i] + P->omega * t[i] * kd[i];
+            lam[i] = l > 0.0f ? l : 0.0f;
+        }
+        err = avg_density_error(n, t, rho0, dyn, P->fast);
+        if (err_hist) err_hist[n_err] = err;
+        ++n_err;
+        int converged = (err < P->tol_opt) && !P->fixed_iters;
+        if ((converged && pass >= 1) || pass >= P->max_outer) break;
+    }
+    int status = ORC_OK;
+    if (!P->fixed_iters && err >= P->tol_opt && pass >= P->max_outer) status = ORC_NOT_CONVERGED;
+    if (status == ORC_OK) {
+        float inv_dt = 1.0f / dt;
+        for (int i = 0; i < n; ++i)
+            if (dyn[i])
+                for (int q = 0; q < 3; ++q) v[3 * i + q] = inv_dt * dv[3 * i + q];
+    }
+    st->outer_iters = pass;
+    st->n_err = n_err;
+    st->final_err = err;
+    st->status = status;
+    free(c); free(lam); free(t); free(v0); free(dv);
+    return status;
+}
+
 /* ----------------------------------------------- Weiler 2018 viscosity */
 
 /* wp.inverse of a 3x3 matrix: adjugate / determinant in FP32 */
@@ -983,7 +1059,8 @@ int orc_jeske23_solve(int n, const orc_st_params* S, const float* x, float* v, c
 int orc_step(int n, const orc_params* P, float dt, const float* g, const float* domain, float* x, float* v,
              const float* rho0, const float* m, const float* m_inv, const int* dyn, int* count, int* ids,
              float* gradW, float* density, float* kd, double* err_hist, int* pcg_hist, orc_stats* st,
-             long* overflow, const int* material, float visc, int* visc_iters, float sigma, int* st_iters) {
+             long* overflow, const int* material, float visc, int* visc_iters, float sigma, int* st_iters,
+             int prj) {
     orc_apply_gravity(n, v, dyn, g, dt);
     if (material && sigma > 0.0f) {
         /* Jeske23 implicit surface tension (framework.py:417-418) */
@@ -997,8 +1074,16 @@ int orc_step(int n, const orc_params* P, float dt, const float* g, const float* 
         int it = orc_weiler18_solve(n, &V, x, v, m, density, rho0, material, dyn, count, ids, gradW);
         if (visc_iters) *visc_iters = it;
     }
-    int status = orc_ip_solve(n, P, dt, density, rho0, m, dyn, count, ids, gradW, kd, v, err_hist, pcg_hist,
+    int status;
+    if (prj) {
+        /* PRJ (pressureMethod 0, framework.py:168-174) with its own omega (prj.py:127) */
+        orc_params Q = *P;
+        Q.omega = 0.5f;
+        status = orc_prj_solve(n, &Q, dt, density, rho0, m, dyn, count, ids, gradW, kd, v, err_hist, st);
+    } else {
+        status = orc_ip_solve(n, P, dt, density, rho0, m, dyn, count, ids, gradW, kd, v, err_hist, pcg_hist,
                               NULL, NULL, st);
+    }
     orc_advect_and_clamp(n, x, v, dyn, dt, domain, P->h);
     long ov = orc_build_neighbor_cache(n, x, dyn, 1, P->h, P->cache_size, count, ids, gradW);
     if (overflow) *overflow = ov;

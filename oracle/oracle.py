@@ -98,11 +98,14 @@ def lib():
         L.orc_apply_gravity.argtypes = [i, P, P, P, f]
         L.orc_advect_and_clamp.argtypes = [i, P, P, P, f, P, f]
         L.orc_step.argtypes = [i, ctypes.POINTER(Params), f, P, P, P, P, P, P, P, P, P, P, P, P, P, P, P,
-                               ctypes.POINTER(Stats), ctypes.POINTER(l), P, f, P, f, P]
+                               ctypes.POINTER(Stats), ctypes.POINTER(l), P, f, P, f, P, i]
         L.orc_weiler18_solve.argtypes = [i, ctypes.POINTER(ViscParams), P, P, P, P, P, P, P, P, P, P]
         L.orc_weiler18_solve.restype = i
         L.orc_jeske23_solve.argtypes = [i, ctypes.POINTER(StParams), P, P, P, P, P, P, P, P, P, P, P]
         L.orc_jeske23_solve.restype = i
+        L.orc_prj_solve.argtypes = [i, ctypes.POINTER(Params), f, P, P, P, P, P, P, P, P, P, P,
+                                    ctypes.POINTER(Stats)]
+        L.orc_prj_solve.restype = i
         L.orc_step.restype = i
         L.orc_cg_f64.argtypes = [i, f, i, P, P, P, P, P, P, P, P, d, i, P]
         L.orc_cg_f64.restype = i
@@ -174,6 +177,7 @@ class State:
     visc_iters: int = 0
     surface_tension: float = 0.0  # Jeske23 sigma (0 = off)
     st_iters: int = 0
+    pressure_method: int = 1      # pressureMethod: 1 IP, 0 PRJ
     count: Optional[np.ndarray] = None
     ids: Optional[np.ndarray] = None
     gradW: Optional[np.ndarray] = None
@@ -198,7 +202,8 @@ class State:
                   max_pcg=sc.max_iteration_pcg, fixed_iters=sc.fixed_outer_iters,
                   material=_i32(sc.material),
                   viscosity=float(sc.viscosity_coeff) if int(sc.viscosity_method) == 1 else 0.0,
-                  surface_tension=float(sc.surface_tension_coeff) if int(sc.surface_tension_method) == 1 else 0.0)
+                  surface_tension=float(sc.surface_tension_coeff) if int(sc.surface_tension_method) == 1 else 0.0,
+                  pressure_method=int(getattr(sc, "pressure_method", 1)))
         kw.update(over)
         return cls(**kw)
 
@@ -271,11 +276,26 @@ class State:
                                 _p(self.is_dynamic), _p(self.count), _p(self.ids), _p(self.gradW),
                                 _p(self.density), _p(self.k), _p(err), _p(pcg), ctypes.byref(st), ctypes.byref(ov),
                                 _p(self.material), float(self.viscosity), ctypes.byref(vit),
-                                float(self.surface_tension), ctypes.byref(sit))
+                                float(self.surface_tension), ctypes.byref(sit), int(self.pressure_method == 0))
         self.visc_iters = int(vit.value)
         self.st_iters = int(sit.value)
         self._record(st, err, pcg)
         self.overflow = int(ov.value)
+        self.status = int(status)
+        return int(status)
+
+    # --- PRJ.solve (prj.py:296-340) on the current lists
+    def prj_solve(self, fast: bool = True, omega: float = 0.5) -> int:
+        n = self.n
+        P = self.params(fast)
+        P.omega = float(omega)
+        err = np.zeros(self.max_outer + 2, np.float64)
+        st = Stats()
+        status = lib().orc_prj_solve(n, ctypes.byref(P), float(self.dt), _p(self.density), _p(self.density0),
+                                     _p(self.m), _p(self.is_dynamic), _p(self.count), _p(self.ids), _p(self.gradW),
+                                     _p(self.k), _p(self.v), _p(err), ctypes.byref(st))
+        self._record(st, err, np.zeros(1, np.int32))
+        self.stats_pcg_iters = []
         self.status = int(status)
         return int(status)
 

@@ -15,6 +15,9 @@ kernels.npz       cubic_kernel / spiky_kernel_derivative at sampled radii;
 visc_solve.npz    one Weiler18 implicit-viscosity solve (weiler18.py:371-401) on
                   the moving block;
 column_visc_steps.npz  Framework.forward() steps with Weiler18 viscosity on;
+prj_solve.npz     one PRJ solve (prj.py:296-340) on the moving block;
+column_prj_steps.npz  Framework.forward() steps with PRJ as the pressure solver;
+scene_ingest.npz  the reference scene loader's particles for scene_blocks.json;
 st_solve.npz      one Jeske23 implicit surface-tension solve (jeske23.py:585-655)
                   on the moving block;
 column_st_steps.npz  Framework.forward() steps with Jeske23 surface tension and
@@ -75,12 +78,13 @@ class _Cfg:
     """Stand-in for config_builder.SimConfig with the keys the hot path reads."""
 
 
-def _make_objects(sc, viscosity_method=0, viscosity_coeff=0.0, st_method=0, st_coeff=0.0):
+def _make_objects(sc, viscosity_method=0, viscosity_coeff=0.0, st_method=0, st_coeff=0.0, pressure_method=1):
     from scripts.io.config_builder import SimConfig
     from scripts.sim.simulation_data import SimulationData
     from scripts.sim.neighbour_search import NeighbourSearch
 
     conf = sc.config()
+    conf["pressureMethod"] = pressure_method
     cfg = SimConfig(domain_size=tuple(float(s) for s in sc.domain_size), domain_start=(0.0, 0.0, 0.0),
                     particle_radius=sc.particle_radius, dt=sc.dt, density0=1000.0,
                     gravity=tuple(sc.gravity), viscosity_method=viscosity_method, surface_tension_method=st_method,
@@ -204,6 +208,30 @@ def make_st_solve(out, sigma=0.05):
         dv=st.dv.numpy().copy(), div=st.div_arr.numpy().copy(), b=st.b_st.numpy().copy())
 
 
+def make_prj_solve(out):
+    """One PRJ.solve (prj.py:296-340) on the moving block, after the
+    reference's neighbour build, density and Aii."""
+    from scripts.sim.forces.pressure.prj import PRJ
+    sc = _scene_block()
+    cfg, ps, ns = _make_objects(sc)
+    solver = PRJ(ps, ns, cfg)
+    ns.build(ps.x, ps.particle_num)
+    ns.build_cache(ps.x, ps.particle_num, int(ps.cache_size), ps.neighbor_count, ps.neighbor_ids,
+                   ps.neighbor_gradW)
+    solver.compute_density()
+    solver.compute_Aii()
+    t0 = time.time()
+    solver.solve(sc.dt)
+    print(f"prj_solve: {time.time() - t0:.1f}s passes={solver.stats_outer_iters}")
+    np.savez_compressed(
+        out, x=sc.x, v0=sc.v, is_dynamic=sc.is_dynamic, material=sc.material, density0=sc.density0,
+        particle_radius=np.float64(sc.particle_radius), domain_size=sc.domain_size, dt=np.float64(sc.dt),
+        v=ps.v.numpy().copy(), omega=np.float64(solver.omega),
+        stats_density_errors=np.array(solver.stats_density_errors, np.float64),
+        stats_outer_iters=np.int32(solver.stats_outer_iters),
+        stats_final_density_error=np.float64(solver.stats_final_density_error))
+
+
 def make_scene_ingest(out):
     """The reference's scene loader (scene_loader.py:70-545) on
     scene_blocks.json: fluid blocks, a generated cube body, boundary walls."""
@@ -223,10 +251,11 @@ def make_scene_ingest(out):
         domain_size=np.asarray(cfg.domain_size, np.float32), particle_radius=np.float64(cfg.particle_radius))
 
 
-def make_column_steps(out, steps, viscosity=0.0, sigma=0.0):
+def make_column_steps(out, steps, viscosity=0.0, sigma=0.0, pressure_method=1):
     from scripts.framework import Framework
     sc = _scene_column()
-    cfg, ps, ns = _make_objects(sc, 1 if viscosity > 0 else 0, viscosity, 1 if sigma > 0 else 0, sigma)
+    cfg, ps, ns = _make_objects(sc, 1 if viscosity > 0 else 0, viscosity, 1 if sigma > 0 else 0, sigma,
+                                pressure_method)
     fw = Framework(ps, ns, cfg)
     if viscosity <= 0:
         fw.viscosity = _NoForce()
@@ -245,13 +274,13 @@ def make_column_steps(out, steps, viscosity=0.0, sigma=0.0):
         rec["density"].append(ps.density.numpy().copy())
         rec["k"].append(p.k.numpy().copy())
         rec["err"].append(np.array(p.stats_density_errors, np.float64))
-        rec["pcg"].append(np.array(p.stats_pcg_iters, np.int32))
+        rec["pcg"].append(np.array(getattr(p, "stats_pcg_iters", []), np.int32))
         rec["outer"].append(p.stats_outer_iters)
         rec["final_err"].append(p.stats_final_density_error)
         rec["cnt"].append(cnt)
         rec["off"].append(off)
         rec["ids"].append(flat)
-        print(f"  step {s}: outer={p.stats_outer_iters} pcg={p.stats_pcg_iters} "
+        print(f"  step {s}: outer={p.stats_outer_iters} pcg={getattr(p, 'stats_pcg_iters', [])} "
               f"err={['%.2e' % e for e in p.stats_density_errors]} ({time.time() - t0:.0f}s)")
 
     def ragged(lst, dt):
@@ -289,6 +318,9 @@ def main():
                                                            viscosity=0.01),
             "st_solve": lambda: make_st_solve(os.path.join(HERE, "st_solve.npz")),
             "scene_ingest": lambda: make_scene_ingest(os.path.join(HERE, "scene_ingest.npz")),
+            "prj_solve": lambda: make_prj_solve(os.path.join(HERE, "prj_solve.npz")),
+            "column_prj_steps": lambda: make_column_steps(os.path.join(HERE, "column_prj_steps.npz"), 6,
+                                                          pressure_method=0),
             "column_st_steps": lambda: make_column_steps(os.path.join(HERE, "column_st_steps.npz"), 8,
                                                          viscosity=0.01, sigma=0.05)}
     for name, job in jobs.items():

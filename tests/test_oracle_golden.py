@@ -270,3 +270,36 @@ def test_column_st_steps_one_step_parity(golden_dir):
         assert _rel(st.v[dyn], g["v"][s][dyn]) < RTOL, s
         assert np.abs(st.x[dyn] - g["x"][s][dyn]).max() < 1e-6, s
     assert compared >= g["x"].shape[0] - 1
+
+
+# --------------------------------------------------------- PRJ (projected Jacobi)
+
+@pytest.mark.parametrize("fast", [False, True])
+def test_prj_solve_golden(golden_dir, fast):
+    g = _load(golden_dir, "prj_solve.npz")
+    st = _state_from(g, g["x"], g["v0"])
+    st.rebuild()
+    dyn = st.is_dynamic == 1
+    assert st.prj_solve(fast=fast, omega=float(g["omega"])) == O.OK
+    assert st.stats_outer_iters == int(g["stats_outer_iters"])
+    assert _rel(st.v[dyn], g["v"][dyn]) < RTOL
+    np.testing.assert_allclose(st.stats_density_errors, g["stats_density_errors"], rtol=1e-4, atol=1e-9)
+    assert abs(st.stats_final_density_error - float(g["stats_final_density_error"])) < 1e-7
+
+
+def test_column_prj_steps_one_step_parity(golden_dir):
+    g = _load(golden_dir, "column_prj_steps.npz")
+    dyn = g["is_dynamic"] == 1
+    for s in range(g["x"].shape[0]):
+        x_prev = g["x0"] if s == 0 else g["x"][s - 1]
+        v_prev = g["v0"] if s == 0 else g["v"][s - 1]
+        st = _state_from(g, x_prev, v_prev)
+        st.pressure_method = 0
+        st.rebuild()
+        st.step(fast=True)
+        assert st.status == O.OK
+        assert abs(st.stats_outer_iters - int(g["outer"][s])) <= 1
+        if st.stats_outer_iters != int(g["outer"][s]):
+            continue
+        assert _rel(st.v[dyn], g["v"][s][dyn]) < RTOL, s
+        assert np.abs(st.x[dyn] - g["x"][s][dyn]).max() < 1e-6, s
