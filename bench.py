@@ -49,6 +49,8 @@ def make_scene(name: str):
         return S.tall_column(viscosity=True)
     if name == "tall_column_ip":
         return S.tall_column(viscosity=False)
+    if name == "tall_column_prj":  # PRJ (pressureMethod 0) beside IP on the viscous column
+        return S.tall_column(viscosity=True, pressure_method=0, omega=0.5)
     if name == "small_column":
         return S.small_column()
     if name == "dam_break":  # Weiler18 nu = 1e-3 and Jeske23 sigma = 0.05 on
@@ -85,7 +87,8 @@ def workload_config(scenes, name: str) -> dict:
                 "densityErrorTol": scenes[0].density_error_tol, "viscosity": "off", "surface_tension": "off",
                 **common}
     sc = scenes[0]
-    return {"workload": sc.name + ("_ip_only" if name in ("tall_column_ip", "dam_break_ip") else ""),
+    suffix = {"tall_column_ip": "_ip_only", "dam_break_ip": "_ip_only", "tall_column_prj": "_prj"}.get(name, "")
+    return {"workload": sc.name + suffix, "pressure_solver": "PRJ" if sc.pressure_method == 0 else "IP",
             "fluid_particles": sc.n_dynamic, "boundary_particles": sc.n - sc.n_dynamic,
             "spacing_m": sc.particle_diameter, "dt_s": sc.dt, "densityErrorTol": sc.density_error_tol,
             "viscosity": ("weiler18 nu=%g" % sc.viscosity_coeff) if sc.viscosity_method == 1 else "off",
@@ -157,6 +160,9 @@ def algorithmic_bytes(kernel: str, n_dyn: int, n_all: int, pairs: int, it=None) 
     per-step phase counts for the persistent solve (outer updates, CG and
     viscosity-CG iterations)."""
     P = float(pairs)
+    if kernel == "prj":  # per pass: head (list + q gathers, dt_v write) and tail (list + dt_v gathers)
+        L = it["outer"]
+        return (L + 1) * ((16 * P + 40 * n_dyn) + (16 * P + 44 * n_dyn)) + 48 * n_dyn
     if kernel == "ip_solve":
         L, I = it["outer"], it["cg"]
         b = (L + 1) * algorithmic_bytes("pack", n_dyn, n_all, pairs) + L * algorithmic_bytes("rhs", n_dyn, n_all, pairs)
@@ -341,10 +347,12 @@ def run_ours(args, rank, world, local_rank):
     # CUDA events around each kernel, after the timed region)
     prof = eng.profile_step(3)
     pairs = [int(r.neighbour_pairs) for r in eng_stats(eng, len(scenes))]
-    if "ip_solve" in prof:
-        # gravity, viscosity (if on), persistent IP solve, advect, keys, 2
-        # scan passes, place, order, neighbour build, static outputs
-        n_launch = (10 + int("visc" in prof) + int("surface_tension" in prof)) * args.steps
+    if not args.per_phase:
+        # gravity, advect, keys, 2 scan passes, place, order, neighbour build,
+        # static outputs; one persistent kernel per solve that runs (IP, PRJ,
+        # viscosity) and two for surface tension (slot velocities + solve)
+        n_launch = (9 + int("ip_solve" in prof) + int("prj" in prof) + int("visc" in prof) +
+                    2 * int("surface_tension" in prof)) * args.steps
     else:
         so = sum(r.sum_outer_iters for r in raws)
         n_launch = 12 * args.steps + (so + args.steps) + so + 2 * sum(r.sum_pcg_iters for r in raws)

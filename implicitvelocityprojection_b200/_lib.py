@@ -41,7 +41,8 @@ class SceneDesc(ctypes.Structure):
         ("viscosity_method", ctypes.c_int32),
         ("surface_tension_method", ctypes.c_int32),
         ("surface_tension_coeff", ctypes.c_float),
-        ("reserved", ctypes.c_int32 * 2),
+        ("pressure_solver", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 1),
     ]
 
 
@@ -97,7 +98,7 @@ class SolveStats(ctypes.Structure):
 # kernel ids of ivp_profile_step (include/ivp.h)
 KERNEL_NAMES = ["gravity", "solve_begin", "pack", "rhs", "cg_a", "cg_b", "solve_end", "divergence", "advect",
                 "keys", "scan_local", "scan_add", "place", "order", "nbr_build", "static_out", "visc", "ip_solve",
-                "surface_tension"]
+                "surface_tension", "prj"]
 K_COUNT = 24
 NOALLOC_MAX_PARTICLES = 65536
 NOALLOC_MAX_CELLS = 262144
@@ -120,6 +121,7 @@ SIGNATURES = {
     "ivp_ip_solve": (_I, [_P, _P]),
     "ivp_viscosity_solve": (_I, [_P, _P]),
     "ivp_surface_tension_solve": (_I, [_P, _P]),
+    "ivp_prj_solve": (_I, [_P, _P]),
     "ivp_apply_gravity": (_I, [_P, _P]),
     "ivp_advect": (_I, [_P, _P]),
     "ivp_step": (_I, [_P, _I, _P]),

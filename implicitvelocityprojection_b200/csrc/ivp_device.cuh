@@ -30,6 +30,7 @@
 namespace ivp {
 
 constexpr int kMaxHistDefault = 128;
+constexpr int SOLVER_IP = 0, SOLVER_PRJ = 1;
 
 struct SceneParams {
     int p_begin, p_end;        // particle range in the bound arrays
@@ -55,6 +56,7 @@ struct SceneParams {
     int st_method;
     float st_d;                // particle diameter d (W^st clamps r at d)
     float st_h;                // surface-tension support h_st = 2 d (jeske23.py:455)
+    int solver;                // SOLVER_IP or SOLVER_PRJ
     int max_outer, max_pcg, fixed_iters, cache;
     int tile_begin, tile_end;
     int hist_base;

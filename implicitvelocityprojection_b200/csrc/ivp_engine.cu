@@ -64,13 +64,14 @@ struct ivp_engine {
     bool want_divergence = false;
     bool any_visc = false;
     bool any_st = false;
+    bool any_ip = false, any_prj = false;
     // persistent solve
     bool persistent = false;
-    int coop_grid = 0, coop_grid_visc = 0, coop_grid_st = 0;
+    int coop_grid = 0, coop_grid_visc = 0, coop_grid_st = 0, coop_grid_prj = 0;
     size_t coop_smem = 0;
     // graphs
-    cudaGraph_t graph_step = nullptr, graph_solve = nullptr, graph_build = nullptr;
-    cudaGraphExec_t exec_step = nullptr, exec_solve = nullptr, exec_build = nullptr;
+    cudaGraph_t graph_step = nullptr, graph_solve = nullptr, graph_build = nullptr, graph_prj = nullptr;
+    cudaGraphExec_t exec_step = nullptr, exec_solve = nullptr, exec_build = nullptr, exec_prj = nullptr;
     // host mirrors
     SceneCtl* h_ctl = nullptr;   // pinned
     Flags* h_flags = nullptr;    // pinned
@@ -187,7 +188,7 @@ struct Kern {
 
 struct KernelSet {
     DevKernel pack, rhs, cg_a, cg_b, dens, aii, div, persist, v_setup, v_a, v_b, v_end, v_persist, st_div,
-        st_persist;
+        st_persist, pj_head, pj_tail, prj_persist;
 };
 
 template <int G, int B>
@@ -195,7 +196,8 @@ KernelSet make_set() {
     return {Kern<G, B>::pack(), Kern<G, B>::rhs(), Kern<G, B>::cg_a(), Kern<G, B>::cg_b(),
             Kern<G, B>::dens(), Kern<G, B>::aii(), Kern<G, B>::div(), k_ip_persistent<G, B>,
             k_visc_setup<G, B>, k_visc_a<G, B>, k_visc_b<G, B>, k_visc_end<G, B>,
-            k_force_persistent<G, B, FORCE_VISC>, k_st_div<G, B>, k_force_persistent<G, B, FORCE_ST>};
+            k_force_persistent<G, B, FORCE_VISC>, k_st_div<G, B>, k_force_persistent<G, B, FORCE_ST>,
+            k_pj_head<G, B>, k_pj_tail<G, B>, k_prj_persistent<G, B>};
 }
 
 // Instantiated launch shapes: G lanes per particle x {128, 256} threads.
@@ -327,6 +329,46 @@ int emit_solve_loop(ivp_engine* e, Launcher& L) {
 
 bool force_any(const ivp_engine* e, int force) { return force == FORCE_ST ? e->any_st : e->any_visc; }
 
+// PRJ.solve of every PRJ scene (prj.py:296-340): persistent, or one launch
+// per pass half with the pass loop as a conditional WHILE node.
+int emit_prj(ivp_engine* e, Launcher& L) {
+    if (e->n_tiles == 0 || !e->any_prj) return IVP_OK;
+    KernelSet K;
+    if (!kernel_set(e->G, e->BLOCK, &K)) return IVP_ERR_BAD_ARG;
+    const int nt = e->n_tiles, B = e->BLOCK;
+    if (e->persistent) {
+        CKS(L.memset0(e->D.bar_count, sizeof(unsigned)));
+        Dev copy = e->D;
+        void* args[] = {&copy};
+        return L.kernel(IVP_K_PRJ, (const void*)K.prj_persist, dim3(e->coop_grid_prj), dim3(e->BLOCK), args,
+                        e->coop_smem, true);
+    }
+    CKS(L.dev(IVP_K_PRJ, k_prj_begin, nt, e->T, e->D));
+    if (!L.graph) {
+        for (int guard = 0; guard < 1000000; ++guard) {
+            CKS(L.dev(IVP_K_PRJ, K.pj_head, nt, B, e->D));
+            CKS(L.dev(IVP_K_PRJ, K.pj_tail, nt, B, e->D));
+            CK(cudaMemcpyAsync(e->h_flags, e->D.flags, sizeof(Flags), cudaMemcpyDeviceToHost, L.stream));
+            CK(cudaStreamSynchronize(L.stream));
+            if (!e->h_flags->any_outer) break;
+        }
+    } else {
+        cudaGraphConditionalHandle h;
+        CK(cudaGraphConditionalHandleCreate(&h, L.graph, 1, cudaGraphCondAssignDefault));
+        cudaGraph_t body;
+        CKS(add_conditional(L.graph, L, h, cudaGraphCondTypeWhile, &body));
+        Launcher Lb;
+        Lb.graph = body;
+        Dev d = e->D;
+        d.h_outer = (unsigned long long)h;
+        CKS(Lb.dev(IVP_K_PRJ, K.pj_head, nt, B, d));
+        CKS(Lb.dev(IVP_K_PRJ, K.pj_tail, nt, B, d));
+    }
+    CKS(L.dev(IVP_K_PRJ, k_prj_end, nt, e->T, e->D));
+    if (e->want_divergence && e->D.div_out) CKS(L.dev(IVP_K_DIVERGENCE, K.div, nt, B, e->D));
+    return IVP_OK;
+}
+
 // An implicit non-pressure solve, one launch per phase: Jeske 2023 surface
 // tension (force 1, with its divergence pass) or Weiler 2018 viscosity
 // (force 0).  The persistent kernel runs the same phases itself.
@@ -368,7 +410,7 @@ int emit_force(ivp_engine* e, Launcher& L, int force) {
 }
 
 int emit_solve(ivp_engine* e, Launcher& L, bool with_visc = false) {
-    if (e->n_tiles == 0) return IVP_OK;
+    if (e->n_tiles == 0 || !e->any_ip) return IVP_OK;
     if (e->persistent) {
         KernelSet K;
         kernel_set(e->G, e->BLOCK, &K);
@@ -424,6 +466,7 @@ int emit_step(ivp_engine* e, Launcher& L) {
     CKS(L.dev(IVP_K_GRAVITY, k_gravity, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, e->D));
     CKS(emit_forces(e, L));
     CKS(emit_solve(e, L, true));
+    CKS(emit_prj(e, L));
     {
         Dev d = e->D;
         d.advect_skip_failed = 1;
@@ -436,6 +479,10 @@ int emit_step(ivp_engine* e, Launcher& L) {
 void destroy_graphs(ivp_engine* e) {
     if (e->exec_step) cudaGraphExecDestroy(e->exec_step);
     if (e->exec_solve) cudaGraphExecDestroy(e->exec_solve);
+    if (e->exec_prj) cudaGraphExecDestroy(e->exec_prj);
+    if (e->graph_prj) cudaGraphDestroy(e->graph_prj);
+    e->exec_prj = nullptr;
+    e->graph_prj = nullptr;
     if (e->exec_build) cudaGraphExecDestroy(e->exec_build);
     if (e->graph_step) cudaGraphDestroy(e->graph_step);
     if (e->graph_solve) cudaGraphDestroy(e->graph_solve);
@@ -565,6 +612,7 @@ void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
         q.st_method = d.surface_tension_method;
         q.st_d = 2.0f * d.particle_radius;  // jeske23.py:454-455
         q.st_h = 2.0f * q.st_d;
+        q.solver = d.pressure_solver == IVP_SOLVER_PRJ ? SOLVER_PRJ : SOLVER_IP;
         q.max_outer = d.max_outer_iters;
         q.max_pcg = d.max_iteration_pcg;
         q.fixed_iters = d.fixed_outer_iters;
@@ -708,6 +756,8 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
         if (scenes[sc].viscosity_method == 1 && scenes[sc].viscosity_coeff > 0.0f && scenes[sc].n_dynamic > 0)
             e->any_visc = true;
         if (scene_st(scenes[sc])) e->any_st = true;
+        if (scenes[sc].pressure_solver == IVP_SOLVER_PRJ) e->any_prj = true;
+        else e->any_ip = true;
     }
     char* w = static_cast<char*>(workspace);
     Dev& D = e->D;
@@ -823,15 +873,18 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)K.persist, e->BLOCK, e->coop_smem) ==
                 cudaSuccess &&
             per_sm > 0) {
-            int per_sm_v = 0, per_sm_s = 0;
+            int per_sm_v = 0, per_sm_s = 0, per_sm_p = 0;
             if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_v, (const void*)K.v_persist, e->BLOCK,
                                                               e->coop_smem) == cudaSuccess &&
                 cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_s, (const void*)K.st_persist, e->BLOCK,
                                                               e->coop_smem) == cudaSuccess &&
-                per_sm_v > 0 && per_sm_s > 0) {
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_p, (const void*)K.prj_persist, e->BLOCK,
+                                                              e->coop_smem) == cudaSuccess &&
+                per_sm_v > 0 && per_sm_s > 0 && per_sm_p > 0) {
                 e->coop_grid = std::min(e->n_tiles, per_sm * nsm);
                 e->coop_grid_visc = std::min(e->n_tiles, per_sm_v * nsm);
                 e->coop_grid_st = std::min(e->n_tiles, per_sm_s * nsm);
+                e->coop_grid_prj = std::min(e->n_tiles, per_sm_p * nsm);
                 e->persistent = true;
             }
         }
@@ -880,6 +933,7 @@ int ivp_update_scene(ivp_engine* e, int32_t scene, const ivp_scene_desc* d, void
         d->domain_size[2] != o.domain_size[2])
         return IVP_ERR_BAD_ARG;
     if (!(d->dt > 0.0f) || d->max_outer_iters < 0 || d->max_iteration_pcg < 0) return IVP_ERR_BAD_ARG;
+    if (d->pressure_solver != e->desc[scene].pressure_solver) return IVP_ERR_BAD_ARG;  // planned at creation
     e->desc[scene] = *d;
     SceneParams& q = e->hp[scene];
     q.dt = d->dt;
@@ -937,6 +991,11 @@ int emit_ip_only(ivp_engine* e, Launcher& L) { return emit_solve(e, L, false); }
 int ivp_ip_solve(ivp_engine* e, void* stream) {
     if (!e) return IVP_ERR_BAD_ARG;
     return run(e, emit_ip_only, &e->graph_solve, &e->exec_solve, as_stream(stream));
+}
+
+int ivp_prj_solve(ivp_engine* e, void* stream) {
+    if (!e) return IVP_ERR_BAD_ARG;
+    return run(e, emit_prj, &e->graph_prj, &e->exec_prj, as_stream(stream));
 }
 
 int ivp_viscosity_solve(ivp_engine* e, void* stream) {

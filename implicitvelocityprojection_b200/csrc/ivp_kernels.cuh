@@ -17,9 +17,13 @@ namespace ivp {
 // K_V_*: the implicit non-pressure CG (surface tension or viscosity, the
 // launch's Dev::force); K_ST_DIV: the surface-tension divergence pass before
 // its setup (no reduction)
-enum Kind { K_PACK = 0, K_RHS = 1, K_CG_A = 2, K_CG_B = 3, K_V_SETUP = 4, K_V_A = 5, K_V_B = 6, K_ST_DIV = 7 };
+// K_PJ_*: the two passes of a PRJ iteration (head without a reduction)
+enum Kind {
+    K_PACK = 0, K_RHS = 1, K_CG_A = 2, K_CG_B = 3, K_V_SETUP = 4, K_V_A = 5, K_V_B = 6, K_ST_DIV = 7,
+    K_PJ_HEAD = 8, K_PJ_TAIL = 9
+};
 constexpr int FORCE_VISC = 0, FORCE_ST = 1;
-constexpr int MODE_IP = 0, MODE_FORCE = 1;
+constexpr int MODE_IP = 0, MODE_FORCE = 1, MODE_PRJ = 3;
 
 constexpr int IVP_OK_ = 0, IVP_NOT_SPD_ = 1, IVP_NOT_CONVERGED_ = 2, IVP_TIMEOUT_ = 6;
 
@@ -90,6 +94,22 @@ __device__ void scene_decide(const Dev& D, const SceneParams& P, SceneCtl& C, in
         } else {
             C.v_beta = s2 / (C.v_rz > 1e-12 ? C.v_rz : 1e-12);
             C.v_rz = s2;
+        }
+        return;
+    }
+    if (kind == K_PJ_TAIL) {
+        // prj.py:175-187: the pass index is the update count
+        const double err = P.n_dyn > 0 ? s / (double)P.n_dyn : 0.0;
+        C.err = err;
+        if (hist && C.n_err < D.hist_len) D.err_hist[P.hist_base + C.n_err] = err;
+        C.n_err += 1;
+        const bool converged = err < P.tol_opt && !P.fixed_iters;
+        if ((converged && C.outer_it >= 1) || C.outer_it >= P.max_outer) {
+            C.outer_active = 0;
+            C.final_err = err;
+            if (!P.fixed_iters && err >= P.tol_opt && C.outer_it >= P.max_outer) C.status = IVP_NOT_CONVERGED_;
+        } else {
+            C.outer_it += 1;
         }
         return;
     }
@@ -235,13 +255,13 @@ __device__ __forceinline__ void guard_begin(const Dev& D) {
 
 // Control-block reset at the start of IP.solve (reset_stats,
 // pressure_base.py:497-502).
-__device__ __forceinline__ void ctl_begin(const SceneParams& P, SceneCtl& C) {
+__device__ __forceinline__ void ctl_begin(const SceneParams& P, SceneCtl& C, int solver = SOLVER_IP) {
     C.err = 0.0;
     C.rr_old = C.pap = C.alpha = C.beta = C.rr0 = 0.0;
     C.final_err = 0.0;
     C.outer_it = 0;
     C.cg_it = 0;
-    C.outer_active = P.n_dyn > 0 ? 1 : 0;
+    C.outer_active = (P.n_dyn > 0 && P.solver == solver) ? 1 : 0;
     C.solve_pending = 0;
     C.cg_active = 0;
     C.status = IVP_OK_;
@@ -282,6 +302,8 @@ __device__ void launch_finalize(const Dev& D, int kind) {
     if (kind == K_PACK) {
         set_cond(D.h_outer, any_outer);
         set_cond(D.h_solve, any_solve);
+    } else if (kind == K_PJ_TAIL) {
+        set_cond(D.h_outer, any_outer);
     } else if (kind == K_RHS || kind == K_CG_B) {
         set_cond(D.h_cg, any_cg);
     } else if (kind == K_V_SETUP || kind == K_V_B) {
@@ -749,6 +771,7 @@ __global__ void k_solve_begin(const Dev D) {
     const SceneParams& P = D.scenes[tile.x];
     if (blockIdx.x == 0 && threadIdx.x == 0) guard_begin(D);
     if (blockIdx.x == P.tile_begin && threadIdx.x == 0) ctl_begin(P, D.ctl[tile.x]);
+    if (P.solver != SOLVER_IP) return;
     const int i = tile.y + threadIdx.x;
     if (i >= tile.z) return;
     const int p = D.pid[i];
@@ -762,6 +785,7 @@ __global__ void k_solve_begin(const Dev D) {
 __global__ void k_solve_end(const Dev D) {
     const int4 tile = D.tiles[blockIdx.x];
     const SceneParams& P = D.scenes[tile.x];
+    if (P.solver != SOLVER_IP) return;
     const SceneCtl& C = D.ctl[tile.x];
     if (blockIdx.x == P.tile_begin && threadIdx.x == 0) {
         SceneCtl& W = D.ctl[tile.x];
@@ -1644,6 +1668,154 @@ __device__ __forceinline__ void st_b_tile(const Dev& D, const TileCtx& T, float 
     *part2 = (double)dot3(rr, z);
 }
 
+
+// ---- PRJ: projected Jacobi on the constant-density constraint (prj.py)
+//
+// Slot arrays: r = dt v (dt_v_0, own), d0 = dt_v (gathered by the tail),
+// fk = dt^2 lambda (own), q = dt^2 lambda / m (gathered by the head; zero at
+// static slots), c = rho - rho0 and k = D^-1 from the build.
+
+// pj_head_fused (prj.py:17-55): dt_v = dt_v_0 - dt^2 J^T lambda / max(m, 1e-6),
+// J^T lambda in gather form (m_j l_i + m_i l_j) grad W = (l_i + m_i q_j) J_ij.
+template <int G>
+__device__ __forceinline__ void pj_head_tile(const Dev& D, const SceneParams& P, const TileCtx& T) {
+    const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
+    float3 xi = make_float3(0.f, 0.f, 0.f);
+    float li = 0.0f, mi = 1.0f;
+    if (T.valid) {
+        const float4 a = D.xm[T.i];
+        xi = f3(a);
+        mi = a.w;
+        li = D.fk[T.i];
+    }
+    float ax = 0.0f, ay = 0.0f, az = 0.0f;
+    const int self = T.valid ? T.i : P.s_begin;
+    const bool bad = pair_loop<G>(D, T.row, xi, cnt, T.lane, self, P.s_begin, P.s_end, [&](const PairBatch& b) {
+#pragma unroll
+        for (int u = 0; u < PU; ++u) {
+            const float wgt = li + mi * D.q[b.j[u]];
+            ax += wgt * b.J[u].x;
+            ay += wgt * b.J[u].y;
+            az += wgt * b.J[u].z;
+        }
+    });
+    if (bad) flag_bad(D, T.i, 11);
+    ax = group_sum<G>(ax);
+    ay = group_sum<G>(ay);
+    az = group_sum<G>(az);
+    if (T.valid && T.lane == 0) {
+        const float den = mi < 1e-6f ? 1e-6f : mi;
+        const float4 v0 = D.r[T.i];
+        D.d0[T.i] = make_float4(v0.x - ax / den, v0.y - ay / den, v0.z - az / den, 0.0f);
+    }
+}
+
+// pj_tail_fused (prj.py:58-117): r = dt J dt_v + c, lambda = max(lambda +
+// omega r D^-1, 0); partial max(r / max(rho0, 1e-6), 0).
+template <int G>
+__device__ __forceinline__ double pj_tail_tile(const Dev& D, const SceneParams& P, const TileCtx& T) {
+    const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
+    float3 xi = make_float3(0.f, 0.f, 0.f), vi = xi;
+    if (T.valid) {
+        xi = f3(D.xm[T.i]);
+        vi = f3(D.d0[T.i]);
+    }
+    float acc = 0.0f;
+    const int self = T.valid ? T.i : P.s_begin;
+    const bool bad = pair_loop<G>(D, T.row, xi, cnt, T.lane, self, P.s_begin, P.s_end, [&](const PairBatch& b) {
+#pragma unroll
+        for (int u = 0; u < PU; ++u) acc += dot3(sub3(vi, f3(D.d0[b.j[u]])), b.J[u]);
+    });
+    if (bad) flag_bad(D, T.i, 12);
+    acc = group_sum<G>(acc);
+    double part = 0.0;
+    if (T.valid && T.lane == 0) {
+        const float r = acc + D.c[T.i];
+        const float l = D.fk[T.i] + P.omega * r * D.kd[T.i];
+        const float lc = l > 0.0f ? l : 0.0f;
+        D.fk[T.i] = lc;
+        D.q[T.i] = lc * D.inv_m[T.i];
+        const float r0 = D.rho0s[T.i];
+        const float e = r / (r0 < 1e-6f ? 1e-6f : r0);
+        part = (double)(e > 0.0f ? e : 0.0f);
+    }
+    return part;
+}
+
+// PRJ.solve prologue (prj.py:307-330): dt_v_0 = dt v, dt_v = dt_v_0,
+// lambda = 0, for the slots of one tile.
+__device__ __forceinline__ void pj_begin_tile(const Dev& D, const SceneParams& P, int4 tile, int first, int step) {
+    for (int i = tile.y + first; i < tile.z; i += step) {
+        const int p = D.pid[i];
+        const float dt = P.dt;
+        const float4 v0 = make_float4(dt * D.v[3 * p], dt * D.v[3 * p + 1], dt * D.v[3 * p + 2], 0.0f);
+        D.r[i] = v0;
+        D.d0[i] = v0;
+        D.fk[i] = 0.0f;
+        D.q[i] = 0.0f;
+    }
+}
+
+// v = dt_v / dt (prj.py:332-336) for a scene that did not raise.
+__device__ __forceinline__ void pj_end_slot(const Dev& D, const SceneParams& P, int i) {
+    const float4 d = D.d0[i];
+    const int p = D.pid[i];
+    const float s = P.inv_dt;
+    D.v[3 * p] = s * d.x;
+    D.v[3 * p + 1] = s * d.y;
+    D.v[3 * p + 2] = s * d.z;
+}
+
+// Statistics of a finished solve into the sticky counters.
+__device__ __forceinline__ void solve_account(SceneCtl& c) {
+    c.acc_solves += 1;
+    c.acc_outer += c.outer_it;
+    c.acc_cg += c.total_cg;
+    if (c.final_err > c.acc_max_final_err) c.acc_max_final_err = c.final_err;
+    if (c.status != IVP_OK_) {
+        c.acc_failed += 1;
+        c.acc_last_failure = c.status;
+    }
+}
+
+// ---- PRJ, one launch per phase
+__global__ void k_prj_begin(const Dev D) {
+    const int4 tile = D.tiles[blockIdx.x];
+    const SceneParams& P = D.scenes[tile.x];
+    if (blockIdx.x == 0 && threadIdx.x == 0) guard_begin(D);
+    if (P.solver != SOLVER_PRJ) return;
+    if (blockIdx.x == P.tile_begin && threadIdx.x == 0) ctl_begin(P, D.ctl[tile.x], SOLVER_PRJ);
+    pj_begin_tile(D, P, tile, threadIdx.x, blockDim.x);
+}
+
+template <int G, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_pj_head(const Dev D) {
+    const TileCtx T = tile_ctx<G>(D, blockIdx.x);
+    if (D.ctl[T.sc].outer_active) pj_head_tile<G>(D, D.scenes[T.sc], T);
+}
+
+template <int G, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_pj_tail(const Dev D) {
+    const TileCtx T = tile_ctx<G>(D, blockIdx.x);
+    __shared__ int sh_active;
+    if (threadIdx.x == 0) sh_active = D.ctl[T.sc].outer_active;
+    __syncthreads();
+    const bool active = sh_active != 0;
+    double part = 0.0;
+    if (active) part = pj_tail_tile<G>(D, D.scenes[T.sc], T);
+    block_finish<BLOCK>(D, T.sc, active, part, K_PJ_TAIL);
+}
+
+__global__ void k_prj_end(const Dev D) {
+    const int4 tile = D.tiles[blockIdx.x];
+    const SceneParams& P = D.scenes[tile.x];
+    if (P.solver != SOLVER_PRJ) return;
+    SceneCtl& C = D.ctl[tile.x];
+    if (blockIdx.x == P.tile_begin && threadIdx.x == 0) solve_account(C);
+    if (C.status != IVP_OK_) return;
+    for (int i = tile.y + threadIdx.x; i < tile.z; i += blockDim.x) pj_end_slot(D, P, i);
+}
+
 // ---- one launch per phase (device-side control through graph conditionals)
 
 template <int G, int BLOCK>
@@ -1712,7 +1884,8 @@ __global__ void __launch_bounds__(BLOCK) k_cg_b(const Dev D) {
 template <int G, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_divergence(const Dev D) {
     const TileCtx T = tile_ctx<G>(D, blockIdx.x);
-    div_tile<G>(D, D.scenes[T.sc], T, D.ctl[T.sc].outer_it);
+    const SceneParams& P = D.scenes[T.sc];
+    div_tile<G>(D, P, T, P.solver == SOLVER_PRJ ? 0 : D.ctl[T.sc].outer_it);
 }
 
 // viscosity, one launch per phase
@@ -1818,7 +1991,9 @@ constexpr unsigned long long kBarrierLimitNs = 2000000000ull;
 
 __device__ __forceinline__ bool phase_active(const SceneCtl& C, int kind) {
     switch (kind) {
-        case K_PACK: return C.outer_active != 0;
+        case K_PACK:
+        case K_PJ_HEAD:
+        case K_PJ_TAIL: return C.outer_active != 0;
         case K_RHS: return C.solve_pending != 0;
         case K_CG_A:
         case K_CG_B: return C.cg_active != 0;
@@ -2092,6 +2267,12 @@ struct Phaser {
                 if (kind == K_V_SETUP) part = st_setup_tile<G>(D, P, T);
                 else if (kind == K_V_A) part = st_a_tile<G>(D, P, T, (float)C.v_beta, C.v_it);
                 else st_b_tile<G>(D, T, (float)C.v_alpha, C.v_it, &part, &part2);
+            } else if constexpr (MODE == MODE_PRJ) {
+                if (kind == K_PJ_HEAD) {
+                    pj_head_tile<G>(D, P, T);
+                    continue;  // no reduction
+                }
+                part = pj_tail_tile<G>(D, P, T);
             } else if constexpr (MODE == MODE_FORCE + FORCE_VISC) {
                 if (kind == K_V_SETUP) part = visc_setup_tile<G>(D, P, T);
                 else if (kind == K_V_A) part = visc_a_tile<G>(D, P, T, (float)C.v_beta, C.v_it);
@@ -2110,7 +2291,7 @@ struct Phaser {
                 pb[D.n_tiles + t] = tot2;
             }
         }
-        if (!barrier(kind == K_ST_DIV ? -1 : kind)) return false;
+        if (!barrier((kind == K_ST_DIV || kind == K_PJ_HEAD) ? -1 : kind)) return false;
         if (++phases > D.phase_limit) {
             // guard: every CTA reaches the same count; CTA 0 stops the scenes,
             // a barrier publishes it
@@ -2223,6 +2404,7 @@ __global__ void __launch_bounds__(BLOCK, persist_min_blocks<BLOCK>()) k_ip_persi
         const TileCtx T = tile_ctx<G>(D, t);
         const SceneCtl& C = ph.sc_sh[T.sc];
         const SceneParams& P = D.scenes[T.sc];
+        if (P.solver != SOLVER_IP) continue;
         if (C.status == IVP_OK_ && T.lane == 0 && T.valid) {
             const float4 d = (C.outer_it & 1) ? D.d1[T.i] : D.d0[T.i];
             const int p = D.pid[T.i];
@@ -2235,15 +2417,49 @@ __global__ void __launch_bounds__(BLOCK, persist_min_blocks<BLOCK>()) k_ip_persi
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         for (int s = 0; s < D.n_scenes; ++s) {
+            if (D.scenes[s].solver != SOLVER_IP) continue;
             SceneCtl c = ctl_load(D.ctl + s);
-            c.acc_solves += 1;
-            c.acc_outer += c.outer_it;
-            c.acc_cg += c.total_cg;
-            if (c.final_err > c.acc_max_final_err) c.acc_max_final_err = c.final_err;
-            if (c.status != IVP_OK_) {
-                c.acc_failed += 1;
-                c.acc_last_failure = c.status;
-            }
+            solve_account(c);
+            D.ctl[s] = c;
+        }
+    }
+}
+
+// The whole PRJ.solve of every PRJ scene in one persistent cooperative
+// launch: passes of head (no reduction) and tail (error, decision).
+template <int G, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, persist_min_blocks<BLOCK>()) k_prj_persistent(const Dev D) {
+    extern __shared__ double dyn_sh[];
+    __shared__ double red_sh[128];
+    __shared__ int flag_sh[2], any_sh;
+    Phaser<G, BLOCK> ph(D, dyn_sh, red_sh, flag_sh, &any_sh);
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        for (int s = 0; s < D.n_scenes; ++s)
+            if (D.scenes[s].solver == SOLVER_PRJ) ctl_begin(D.scenes[s], D.ctl[s], SOLVER_PRJ);
+    for (int t = ph.t0; t < ph.t1; ++t) {
+        const int4 tile = __ldg(D.tiles + t);
+        const SceneParams& P = D.scenes[tile.x];
+        if (P.solver == SOLVER_PRJ) pj_begin_tile(D, P, tile, threadIdx.x, BLOCK);
+    }
+    if (!ph.barrier(-1)) return;
+    ph.refresh();
+    while (ph.any(K_PJ_HEAD)) {
+        if (!ph.template run<MODE_PRJ>(K_PJ_HEAD)) return;
+        if (!ph.template run<MODE_PRJ>(K_PJ_TAIL)) return;
+    }
+    for (int t = ph.t0; t < ph.t1; ++t) {
+        const TileCtx T = tile_ctx<G>(D, t);
+        const SceneParams& P = D.scenes[T.sc];
+        if (P.solver != SOLVER_PRJ) continue;
+        const SceneCtl& C = ph.sc_sh[T.sc];
+        if (C.status == IVP_OK_ && T.lane == 0 && T.valid) pj_end_slot(D, P, T.i);
+        if (D.div_out) div_tile<G>(D, P, T, 0);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        for (int s = 0; s < D.n_scenes; ++s) {
+            if (D.scenes[s].solver != SOLVER_PRJ) continue;
+            SceneCtl c = ctl_load(D.ctl + s);
+            solve_account(c);
             D.ctl[s] = c;
         }
     }

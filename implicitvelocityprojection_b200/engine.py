@@ -67,6 +67,8 @@ def scene_desc(sc, offset: int) -> _lib.SceneDesc:
     d.viscosity_method = sc.viscosity_method
     d.surface_tension_method = int(getattr(sc, "surface_tension_method", 0))
     d.surface_tension_coeff = float(getattr(sc, "surface_tension_coeff", 0.0))
+    # pressureMethod (framework.py:168-174): 1 IP, 0 PRJ
+    d.pressure_solver = 1 if int(getattr(sc, "pressure_method", 1)) == 0 else 0
     return d
 
 
@@ -217,6 +219,10 @@ class Engine:
     def viscosity_solve(self, stream=None):
         """Weiler18.solve(coeff, dt) of every scene with implicit viscosity."""
         check(self.L.ivp_viscosity_solve(self._handle, ctypes.c_void_p(_stream_ptr(stream))), "ivp_viscosity_solve")
+
+    def prj_solve(self, stream=None):
+        """PRJ.solve(dt) of every scene whose pressure method is PRJ (0)."""
+        check(self.L.ivp_prj_solve(self._handle, ctypes.c_void_p(_stream_ptr(stream))), "ivp_prj_solve")
 
     def surface_tension_solve(self, stream=None):
         """Jeske23.solve(sigma, sigma, dt) of every scene with implicit surface tension."""

@@ -15,6 +15,7 @@ import time
 import torch
 
 from .ip import IP
+from .prj import PRJ
 
 
 class Framework:
@@ -33,11 +34,13 @@ class Framework:
         self.initial_particle_num = simulation_data.particle_num
         self.stats_pressure_ms = 0.0
         self.stats_elasticity_ms = 0.0
-        # framework.py:168-174: only IP (pressureMethod 1) is built here
+        # framework.py:168-174: IP (1) and PRJ (0) are built here; SISPH (3)
+        # and PBF (5) are position-based solvers outside this engine
         pressure_method = int(config.get_cfg("pressureMethod", 1))
-        if pressure_method != 1:
-            raise NotImplementedError(f"pressureMethod {pressure_method}: only IP (1) is implemented on this engine")
-        self.pressure = IP(simulation_data, neighbour_search, config)
+        if pressure_method not in (0, 1):
+            raise NotImplementedError(f"pressureMethod {pressure_method}: only PRJ (0) and IP (1) are implemented "
+                                      "on this engine")
+        self.pressure = (IP if pressure_method == 1 else PRJ)(simulation_data, neighbour_search, config)
         # non-pressure forces (framework.py:176-187): Jeske 2023 implicit
         # surface tension and Weiler 2018 implicit viscosity run inside the
         # engine's step; the explicit forms (Akinci 2013 surface tension,

@@ -150,6 +150,7 @@ def load_scene(src: Union[str, dict], name: str = None) -> Scene:
         viscosity_coeff=float(conf.get("viscosityCoeff", 0.01)),
         surface_tension_method=int(conf.get("surfaceTensionMethod", 0)),
         surface_tension_coeff=float(conf.get("surfaceTensionCoeff", 0.01)),
+        pressure_method=int(conf.get("pressureMethod", 1)),
     )
     return Scene(x=np.ascontiguousarray(x), v=np.ascontiguousarray(np.concatenate(vs)), is_dynamic=dyn, material=np.concatenate(mats),
                  density0=np.concatenate(rhos), particle_radius=radius,

@@ -63,6 +63,8 @@ class Scene:
     viscosity_coeff: float = 0.0
     surface_tension_method: int = 0
     surface_tension_coeff: float = 0.0
+    # pressureMethod (framework.py:168-174): 1 IP, 0 PRJ
+    pressure_method: int = 1
     name: str = "scene"
 
     @property
@@ -101,7 +103,7 @@ class Scene:
             "gravitation": list(self.gravity),
             "domainStart": [0.0, 0.0, 0.0],
             "domainEnd": [float(s) for s in self.domain_size],
-            "pressureMethod": 1,
+            "pressureMethod": self.pressure_method,
             "omega": self.omega,
             "tol_pcg": self.tol_pcg,
             "densityErrorTol": self.density_error_tol,

@@ -38,6 +38,7 @@ class SceneSpec:
     viscosity_method: int = 0
     surface_tension_coeff: float = 0.0
     surface_tension_method: int = 0
+    pressure_method: int = 1  # 1 IP, 0 PRJ
 
 
 class SimulationData:
@@ -173,6 +174,7 @@ class SimulationData:
                        surface_tension_method=int(cfg.surface_tension_method)
                        if float(cfg.surface_tension_coeff) > 0 else 0)
         if solver is not None:
+            sp.pressure_method = int(getattr(solver, "pressure_method", 1))
             sp.omega = float(solver.omega)
             sp.tol_pcg = float(getattr(solver, "tol_pcg", 1e-6))
             sp.density_error_tol = float(solver.tol_opt)
@@ -193,7 +195,11 @@ class SimulationData:
         from `solver` / `dt` when they changed."""
         from .engine import Engine
         sp = self.spec(solver, dt)
-        key = (sp.n, sp.n_dynamic, self.x.data_ptr() if self.allocated else 0)
+        # solver choice and enabled forces fix the engine's plan (launches and
+        # buffers): a change rebuilds the engine
+        key = (sp.n, sp.n_dynamic, self.x.data_ptr() if self.allocated else 0, sp.pressure_method,
+               sp.viscosity_method == 1 and sp.viscosity_coeff > 0,
+               sp.surface_tension_method == 1 and sp.surface_tension_coeff > 0)
         if self._engine is None or self._engine_key != key:
             self._engine = Engine([sp], device=str(self.device), arrays=self.live())
             self._engine_key = key

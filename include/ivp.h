@@ -61,7 +61,8 @@ typedef struct {
     int32_t viscosity_method;   /* 0 off, 1 Weiler 2018 implicit */
     int32_t surface_tension_method;  /* 0 off, 1 Jeske 2023 implicit (surfaceTensionMethod) */
     float surface_tension_coeff;     /* sigma (surfaceTensionCoeff) */
-    int32_t reserved[2];
+    int32_t pressure_solver;         /* IVP_SOLVER_IP (0, pressureMethod 1) or IVP_SOLVER_PRJ (1, pressureMethod 0) */
+    int32_t reserved[1];
 } ivp_scene_desc;
 
 typedef struct {
@@ -116,11 +117,15 @@ typedef struct {
     int64_t sum_st_iters;         /* implicit surface-tension CG iterations */
 } ivp_solve_stats;
 
+/* Pressure solvers (ivp_scene_desc.pressure_solver). */
+enum { IVP_SOLVER_IP = 0, IVP_SOLVER_PRJ = 1 };
+
 /* Kernel ids reported by ivp_profile_step. */
 enum {
     IVP_K_GRAVITY = 0, IVP_K_SOLVE_BEGIN, IVP_K_PACK, IVP_K_RHS, IVP_K_CG_A, IVP_K_CG_B, IVP_K_SOLVE_END,
     IVP_K_DIVERGENCE, IVP_K_ADVECT, IVP_K_KEYS, IVP_K_SCAN_LOCAL, IVP_K_SCAN_ADD, IVP_K_PLACE, IVP_K_ORDER,
-    IVP_K_NBR_BUILD, IVP_K_STATIC_OUT, IVP_K_VISC, IVP_K_PERSISTENT, IVP_K_SURFACE_TENSION, IVP_K_COUNT = 24
+    IVP_K_NBR_BUILD, IVP_K_STATIC_OUT, IVP_K_VISC, IVP_K_PERSISTENT, IVP_K_SURFACE_TENSION, IVP_K_PRJ,
+    IVP_K_COUNT = 24
 };
 
 typedef struct ivp_engine ivp_engine;
@@ -179,6 +184,13 @@ int ivp_viscosity_solve(ivp_engine* e, void* stream);
  * neighbour lists and densities.  ivp_step runs it after gravity and before
  * the viscosity (framework.py:400-421). */
 int ivp_surface_tension_solve(ivp_engine* e, void* stream);
+
+/* PRJ.solve(dt) (scripts/sim/forces/pressure/prj.py:296-340): projected
+ * Jacobi on the constant-density constraint (IISPH-style, omega 0.5, no warm
+ * start, no divergence-free pass) for every scene whose pressure_solver is
+ * IVP_SOLVER_PRJ; v = dt_v / dt unless the scene does not converge.  Stats as
+ * for the IP solve (stats_outer_iters = passes). */
+int ivp_prj_solve(ivp_engine* e, void* stream);
 
 /* apply_gravity (framework.py:26-41). */
 int ivp_apply_gravity(ivp_engine* e, void* stream);
