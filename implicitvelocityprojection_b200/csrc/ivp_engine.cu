@@ -242,10 +242,10 @@ int emit_build(ivp_engine* e, Launcher& L) {
     CKS(L.dev(IVP_K_PLACE, k_place, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D));
     CKS(L.dev(IVP_K_ORDER, k_order, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D));
     {
-        // cell-tiled build: one CTA per row segment, 8 lanes per particle
+        // cell-tiled build: one CTA per row segment, one warp per cell
         Dev copy = D;
         void* args[] = {&copy};
-        CKS(L.kernel(IVP_K_NBR_BUILD, (const void*)k_nbr_build<8>, dim3(e->n_segs), dim3(256), args,
+        CKS(L.kernel(IVP_K_NBR_BUILD, (const void*)k_nbr_build<kBuildPP>, dim3(e->n_segs), dim3(256), args,
                      sizeof(float4) * kStageCap));
     }
     CKS(L.dev(IVP_K_STATIC_OUT, k_static_outputs, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D));

@@ -481,27 +481,40 @@ __global__ void k_order(const Dev D) {
 // Cell-tiled: one CTA per segment of kSegW cells along x of one (y, z) cell
 // row.  The CTA stages the candidates of the 9 neighbouring rows x {dynamic,
 // static} -- 18 contiguous slot ranges covering x_lo-1 .. x_hi+1 -- into
-// shared memory with coalesced loads, together with their cell starts; then
-// G lanes per particle test the particle's own candidate ranges from shared
-// memory.  A group ballot orders the hits of each round by slot, so each list
-// keeps the sequential candidate order (rows dz, dy ascending; dynamic cells
-// before static cells; slots ascending) and the first-cache_size truncation
-// of the sequential scan.  Segments whose neighbourhood exceeds the staging
-// capacity read the candidates from global memory instead.
+// shared memory with coalesced loads, together with their cell starts.
+//
+// One warp per cell: the particles of a cell share their 27-cell candidate
+// window, so a warp takes up to PP particles of one cell and walks the window
+// once.  Each lane loads one candidate per round and tests it against all PP
+// particles; one warp ballot per particle orders that round's hits by
+// candidate, so each list keeps the sequential candidate order (rows dz, dy
+// ascending; dynamic cells before static cells; slots ascending) and the
+// first-cache_size truncation of the sequential scan.  The window is the
+// concatenation of the cell's 18 slot ranges, so rounds run over all 32
+// lanes across range ends; a lane finds its range by a binary search over
+// the range starts.  The dense pass (J, density, Aii) then runs 32/PP lanes
+// per particle.  Segments whose neighbourhood exceeds the staging capacity
+// read the candidates from global memory instead.
 constexpr int kSegW = 8;
-constexpr int kStageCap = 2048;  // staged candidates per CTA (32 KB of float4)
+constexpr int kStageCap = 2048;  // staged candidates per CTA (32 KB): with PP = 4, static + dynamic shared stay under 48 KB
+constexpr int kBuildPP = 4;      // particles per warp
 
-template <int G>
+template <int PP>
 __global__ void __launch_bounds__(256, 4) k_nbr_build(const Dev D) {
-    constexpr int NG = 256 / G;
+    constexpr int NW = 8;          // warps per CTA
     constexpr int NC = kSegW + 3;  // cell starts x_lo-1 .. x_hi+2
-    constexpr int HB = 64;         // hit buffer per particle (>= list stride is not required: capped at cap)
+    constexpr int HB = 64;         // hit buffer per particle (cap <= 64)
+    constexpr int LPP = 32 / PP;   // lanes per particle in the dense pass
+    static_assert(PP == 2 || PP == 4, "PP: 2 or 4 particles per warp (shared memory stays under 48 KB)");
     extern __shared__ float4 stage[];
     __shared__ int sh_cs[18][NC];
     __shared__ int sh_off[18], sh_base[18];
     __shared__ int sh_total, sh_pairs;
-    __shared__ int hit_j[NG][HB];
-    __shared__ short hit_q[NG][HB];
+    __shared__ int sh_vst[NW][32];  // per warp: window offset of each range, INT_MAX past the 18th
+    __shared__ int sh_rj[NW][18];   // first slot of each range in the window
+    __shared__ int sh_rs[NW][18];   // its stage index
+    __shared__ int hit_j[NW][PP][HB];
+    __shared__ short hit_s[NW][PP][HB];
     const int4 seg = D.segs[blockIdx.x];  // (scene, cy, cz, x_lo)
     const int sc = seg.x, cy = seg.y, cz = seg.z, x_lo = seg.w;
     const SceneParams& P = D.scenes[sc];
@@ -510,7 +523,6 @@ __global__ void __launch_bounds__(256, 4) k_nbr_build(const Dev D) {
     const int kd0 = P.key_base + (cz * P.dims[1] + cy) * dimx;
     const int s0 = __ldg(D.cell_start + kd0 + x_lo), s1 = __ldg(D.cell_start + kd0 + x_hi + 1);
     if (s0 == s1) return;  // no dynamic particle in this segment (block-uniform)
-    // cell starts of the 18 neighbour ranges (column c <-> x = x_lo - 1 + c)
     for (int e = threadIdx.x; e < 18 * NC; e += blockDim.x) {
         const int q = e / NC, c = e % NC;
         const int rr = q >> 1, pass = q & 1;
@@ -523,10 +535,9 @@ __global__ void __launch_bounds__(256, 4) k_nbr_build(const Dev D) {
     }
     if (threadIdx.x == 0) sh_pairs = 0;
     __syncthreads();
-    const int ca = (x_lo > 0 ? x_lo - 1 : 0) - (x_lo - 1);                    // first staged column
-    const int cb = (x_hi < dimx - 1 ? x_hi + 1 : dimx - 1) + 1 - (x_lo - 1);  // one past the last
+    const int ca = (x_lo > 0 ? x_lo - 1 : 0) - (x_lo - 1);
+    const int cb = (x_hi < dimx - 1 ? x_hi + 1 : dimx - 1) + 1 - (x_lo - 1);
     if (threadIdx.x < 32) {
-        // prefix of the 18 range lengths (one warp)
         const int q = threadIdx.x;
         int len = 0, b = 0;
         if (q < 18) {
@@ -548,72 +559,130 @@ __global__ void __launch_bounds__(256, 4) k_nbr_build(const Dev D) {
     }
     __syncthreads();
     const bool staged = sh_total <= kStageCap;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (staged) {
-        // one flat pass over the staged candidates: every thread's loads are
-        // independent (issued together), not one range after another
+        // one flat pass over the staged candidates (every thread's loads are
+        // independent); a binary search over the range offsets finds each
+        // candidate's range
         const int total = sh_total;
 #pragma unroll 4
         for (int k = threadIdx.x; k < total; k += blockDim.x) {
             int q = 0;
 #pragma unroll
-            for (int t = 1; t < 18; ++t) q += (k >= sh_off[t]) ? 1 : 0;
+            for (int st = 16; st > 0; st >>= 1)
+                if (q + st < 18 && sh_off[q + st] <= k) q += st;
             stage[k] = __ldg(D.xm + sh_base[q] + (k - sh_off[q]));
         }
     }
     __syncthreads();
-    const int g = threadIdx.x / G, lane = threadIdx.x % G;
-    const int wl = threadIdx.x & 31;
-    const int gshift = wl & ~(G - 1);
-    const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << gshift;
-    const unsigned below = (1u << lane) - 1u;
+    const unsigned lt = (1u << lane) - 1u;
     const float h = P.h, inv_h = P.inv_h, r2max = P.r2_max, spk = P.spiky_k, ck = P.cubic_k;
     const int dyn_end = P.s_dyn_end;
     const int cap = min(min(P.cache, D.stride), HB);
+    const int ncell = x_hi - x_lo + 1;
+    // work items: (cell, run of up to PP of its dynamic particles), dealt to
+    // the warps round-robin; the segment's own cells are row q = 8
+    // (dz = dy = 0, dynamic), columns 1 .. ncell + 1
+    int nitems = 0;
+    for (int k = 0; k < ncell; ++k) nitems += (sh_cs[8][k + 2] - sh_cs[8][k + 1] + PP - 1) / PP;
     int my_pairs = 0;
-    for (int i = s0 + g; i < s1; i += NG) {
-        const float4 xi4 = D.xm[i];
-        const float3 xi = f3(xi4);
-        const float mi = xi4.w;
-        const int cx = cell_coord(xi.x, P.cell_inv, dimx);
+    for (int it = w; it < nitems; it += NW) {
+        int k = 0, acc = 0, pb = 0, pe = 0;
+        for (; k < ncell; ++k) {
+            const int b = sh_cs[8][k + 1], e = sh_cs[8][k + 2];
+            const int nch = (e - b + PP - 1) / PP;
+            if (it < acc + nch) {
+                pb = b + (it - acc) * PP;
+                pe = min(pb + PP, e);
+                break;
+            }
+            acc += nch;
+        }
+        const int cx = x_lo + k;
         const int c0 = (cx > 0 ? cx - 1 : 0) - (x_lo - 1);
         const int c1 = (cx < dimx - 1 ? cx + 1 : dimx - 1) + 1 - (x_lo - 1);
-        // phase 1: filter -- the ordered hit indices of the first `cap` neighbours
-        int cnt = 0, found = 0;
-#pragma unroll 1
-        for (int q = 0; q < 18; ++q) {
-            const int jb = sh_cs[q][c0], je = sh_cs[q][c1];
-            if (jb < 0) continue;
-            const int sb = sh_base[q], so = sh_off[q];
-            for (int base = jb; base < je; base += G) {
-                const int j = base + lane;
-                bool hit = false;
-                if (j < je && j != i) {
-                    const float4 xj4 = staged ? stage[so + (j - sb)] : __ldg(D.xm + j);
-                    hit = norm2_rn(sub3(xi, f3(xj4))) <= r2max;
+        // the cell's window: 18 ranges, concatenated in scan order
+        int L;
+        {
+            int len = 0, jb = 0, so = 0;
+            if (lane < 18) {
+                jb = sh_cs[lane][c0];
+                const int je = sh_cs[lane][c1];
+                len = (jb >= 0 && je > jb) ? je - jb : 0;
+                so = sh_off[lane] + (jb - sh_base[lane]);
+            }
+            int incl = len;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            sh_vst[w][lane] = lane < 18 ? incl - len : INT_MAX;
+            if (lane < 18) {
+                sh_rj[w][lane] = jb;
+                sh_rs[w][lane] = so;
+            }
+            L = __shfl_sync(0xffffffffu, incl, 31);
+            __syncwarp();
+        }
+        const int np = pe - pb;
+        float3 xi[PP];
+        int cnt[PP];
+#pragma unroll
+        for (int p = 0; p < PP; ++p) {
+            xi[p] = f3(D.xm[pb + (p < np ? p : 0)]);
+            cnt[p] = 0;
+        }
+        // phase 1: filter
+        for (int base = 0; base < L; base += 32) {
+            const int v = base + lane;
+            const bool valid = v < L;
+            const int vv = valid ? v : L - 1;
+            int q = 0;
+#pragma unroll
+            for (int st = 16; st > 0; st >>= 1)
+                if (sh_vst[w][q + st] <= vv) q += st;
+            const int off = vv - sh_vst[w][q];
+            const int j = sh_rj[w][q] + off;
+            const int s = sh_rs[w][q] + off;
+            const float4 xj4 = staged ? stage[s] : __ldg(D.xm + j);
+            const float3 xj = f3(xj4);
+            const int jr = j - pb;
+#pragma unroll
+            for (int p = 0; p < PP; ++p) {
+                if (p < np) {
+                    const bool hit = valid && jr != p && norm2_rn(sub3(xi[p], xj)) <= r2max;
+                    const unsigned ball = __ballot_sync(0xffffffffu, hit);
+                    const int pos = cnt[p] + __popc(ball & lt);
+                    if (hit && pos < cap) {
+                        hit_j[w][p][pos] = j;
+                        hit_s[w][p][pos] = (short)s;
+                    }
+                    cnt[p] += __popc(ball);
                 }
-                const unsigned ball = (__ballot_sync(gmask, hit) >> gshift);
-                const int pos = cnt + __popc(ball & below);
-                if (hit && pos < cap) {
-                    hit_j[g][pos] = j;
-                    hit_q[g][pos] = (short)q;
-                }
-                const int nh = __popc(ball);
-                found += nh;
-                cnt = min(cnt + nh, cap);
             }
         }
-        __syncwarp(gmask);
-        // phase 2: dense over the hits -- J_ij = m_j grad W_ij, density, Aii
+        __syncwarp();
+        // phase 2: dense over the hits, LPP lanes per particle
+        const int p = lane / LPP, sub = lane % LPP;
+        int found = 0;
+#pragma unroll
+        for (int t = 0; t < PP; ++t)
+            if (t == p) found = cnt[t];
+        const bool act = p < np;
+        const int n_hit = act ? min(found, cap) : 0;
+        const int i = pb + (act ? p : 0);
+        const float4 xi4 = D.xm[i];
+        const float3 xs = f3(xi4);
         const int row = P.row_base + (i - P.s_begin);
         float4* out = D.nbr + (size_t)row * D.stride;
         float2* out2 = reinterpret_cast<float2*>(D.nbr) + (size_t)row * D.stride;
         float rho = 0.0f, aii = 0.0f;
         float3 jii = make_float3(0.0f, 0.0f, 0.0f);
-        for (int k = lane; k < cnt; k += G) {
-            const int j = hit_j[g][k];
-            const int q = hit_q[g][k];
-            const float4 xj4 = staged ? stage[sh_off[q] + (j - sh_base[q])] : __ldg(D.xm + j);
-            const float3 r = sub3(xi, f3(xj4));
+        for (int kk = sub; kk < n_hit; kk += LPP) {
+            const int j = hit_j[w][p][kk];
+            const float4 xj4 = staged ? stage[hit_s[w][p][kk]] : __ldg(D.xm + j);
+            const float3 r = sub3(xs, f3(xj4));
             // spiky gradient (sph_kernel.py:52-61): -k (h - |r|)^2 r / |r|
             const float rn = sqrtf(norm2_rn(r));
             const float rc = rn < 1e-6f ? 1e-6f : rn;
@@ -621,54 +690,55 @@ __global__ void __launch_bounds__(256, 4) k_nbr_build(const Dev D) {
             const float sg = -spk * (t * t);
             const float ir = __frcp_rn(rc);
             const float mj = xj4.w;
-            // J = w (x_i - x_j): the compact rows keep w and recompute J
-            // from the positions with the same three products
-            const float w = mj * (sg * ir);
-            const float3 J = make_float3(__fmul_rn(w, r.x), __fmul_rn(w, r.y), __fmul_rn(w, r.z));
+            const float wgt = mj * (sg * ir);
+            const float3 J = make_float3(__fmul_rn(wgt, r.x), __fmul_rn(wgt, r.y), __fmul_rn(wgt, r.z));
             if (D.row_fmt == ROW_FULL) {
-                out[k] = make_float4(J.x, J.y, J.z, __int_as_float(j));
+                out[kk] = make_float4(J.x, J.y, J.z, __int_as_float(j));
             } else if (D.row_fmt == ROW_COMPACT) {
-                out2[k] = make_float2(__int_as_float(j), w);
+                out2[kk] = make_float2(__int_as_float(j), wgt);
             } else {
-                const size_t e = (size_t)row * D.stride + k;
+                const size_t e = (size_t)row * D.stride + kk;
                 reinterpret_cast<int*>(D.nbr)[e] = j;
-                unsigned short* g = D.nbr_g + 3 * e;
-                g[0] = bf16_bits(J.x);
-                g[1] = bf16_bits(J.y);
-                g[2] = bf16_bits(J.z);
+                unsigned short* gb = D.nbr_g + 3 * e;
+                gb[0] = bf16_bits(J.x);
+                gb[1] = bf16_bits(J.y);
+                gb[2] = bf16_bits(J.z);
             }
             rho += mj * cubic_Wq(rn * inv_h, ck);
             if (j < dyn_end) aii += dot3(J, J) * __frcp_rn(mj);
             jii = sub3(jii, J);
         }
-        rho = group_sum_masked<G>(rho, gmask);
-        aii = group_sum_masked<G>(aii, gmask);
-        jii.x = group_sum_masked<G>(jii.x, gmask);
-        jii.y = group_sum_masked<G>(jii.y, gmask);
-        jii.z = group_sum_masked<G>(jii.z, gmask);
-        if (lane == 0) {
+#pragma unroll
+        for (int o = LPP / 2; o > 0; o >>= 1) {
+            rho += __shfl_xor_sync(0xffffffffu, rho, o);
+            aii += __shfl_xor_sync(0xffffffffu, aii, o);
+            jii.x += __shfl_xor_sync(0xffffffffu, jii.x, o);
+            jii.y += __shfl_xor_sync(0xffffffffu, jii.y, o);
+            jii.z += __shfl_xor_sync(0xffffffffu, jii.z, o);
+        }
+        if (act && sub == 0) {
+            const float mi = xi4.w;
             float dens = 0.0f;
             dens = dens + mi * P.W0;
             dens += rho;
             aii += dot3(jii, jii) * __frcp_rn(mi);
             const float kd = __frcp_rn(aii + 1e-3f);
-            D.nbr_cnt[row] = cnt;
+            D.nbr_cnt[row] = n_hit;
             D.dens[i] = dens;
             D.kd[i] = kd;
             D.c[i] = dens - D.rho0s[i];
-            const int p = D.pid[i];
-            D.rflu[i] = D.material[p] == 1 ? __frcp_rn(dens) : 0.0f;
-            D.density_out[p] = dens;
-            D.k_out[p] = kd;
+            const int pid = D.pid[i];
+            D.rflu[i] = D.material[pid] == 1 ? __frcp_rn(dens) : 0.0f;
+            D.density_out[pid] = dens;
+            D.k_out[pid] = kd;
             if (found > cap) atomicAdd(&D.overflow[sc], 1);
-            my_pairs += cnt;
+            my_pairs += n_hit;
         }
-        __syncwarp(gmask);
+        __syncwarp();
     }
-    // one pair-count atomic per CTA
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) my_pairs += __shfl_xor_sync(0xffffffffu, my_pairs, o);
-    if (wl == 0 && my_pairs) atomicAdd(&sh_pairs, my_pairs);
+    if (lane == 0 && my_pairs) atomicAdd(&sh_pairs, my_pairs);
     __syncthreads();
     if (threadIdx.x == 0 && sh_pairs) atomicAdd(&D.pairs[sc], (unsigned long long)sh_pairs);
 }
