@@ -2207,12 +2207,12 @@ __device__ bool grid_reduce_barrier(const Dev& D, int kind, const double* partia
     return sh_flag[1] != 0;
 }
 
-// Phase driver shared by the persistent kernels: per-CTA tile range, local
-// copies of the control blocks, one grid barrier + reduction per phase.
+// Phase driver shared by the persistent kernels: tiles dealt round-robin over
+// the CTAs, local copies of the control blocks, one grid barrier + reduction
+// per phase.
 template <int G, int BLOCK>
 struct Phaser {
     const Dev& D;
-    int t0, t1;
     double* sum_sh;
     double* sum_sh2;
     SceneCtl* sc_sh;
@@ -2227,8 +2227,6 @@ struct Phaser {
 
     __device__ Phaser(const Dev& d, double* dyn, double* red, int* flag, int* anyp)
         : D(d), red_sh(red), flag_sh(flag), any_sh(anyp), phases(0) {
-        t0 = (int)(((long long)blockIdx.x * D.n_tiles) / gridDim.x);
-        t1 = (int)(((long long)(blockIdx.x + 1) * D.n_tiles) / gridDim.x);
         sum_sh = dyn;
         sum_sh2 = dyn + D.n_scenes;
         sc_sh = reinterpret_cast<SceneCtl*>(dyn + 2 * D.n_scenes);
@@ -2319,10 +2317,12 @@ struct Phaser {
     __device__ bool run(int kind) {
         active_prefix(kind);
         const int A = act_sh[D.n_scenes];
-        const int a0 = (int)(((long long)blockIdx.x * A) / gridDim.x);
-        const int a1 = (int)(((long long)(blockIdx.x + 1) * A) / gridDim.x);
-        int sc = a0 < a1 ? scene_of(a0) : 0;
-        for (int a = a0; a < a1; ++a) {
+        // active tiles dealt round-robin: at any moment the CTAs work on one
+        // window of consecutive tiles, whose rows and neighbour records are
+        // close in memory (L2 reuse of the gathers), as in a launch of one CTA
+        // per tile
+        int sc = (int)blockIdx.x < A ? scene_of(blockIdx.x) : 0;
+        for (int a = blockIdx.x; a < A; a += gridDim.x) {
             while (a >= act_sh[sc + 1]) ++sc;
             const int t = tb_sh[sc] + (a - act_sh[sc]);
             const TileCtx T = tile_ctx<G>(D, t);
@@ -2421,7 +2421,7 @@ __global__ void __launch_bounds__(BLOCK, persist_min_blocks<BLOCK>()) k_force_pe
         if (!ph.any(K_V_B)) break;
         if (!ph.template run<M>(K_V_B)) return;
     }
-    for (int t = ph.t0; t < ph.t1; ++t) {
+    for (int t = blockIdx.x; t < D.n_tiles; t += gridDim.x) {
         const TileCtx T = tile_ctx<G>(D, t);
         if (ph.sc_sh[T.sc].v_on) visc_end_tile(D, T);
     }
@@ -2447,7 +2447,7 @@ __global__ void __launch_bounds__(BLOCK, persist_min_blocks<BLOCK>()) k_ip_persi
     if (blockIdx.x == 0 && threadIdx.x == 0)
         for (int s = 0; s < D.n_scenes; ++s) ctl_begin(D.scenes[s], D.ctl[s]);
     // d = dt v (ip.py:343) for the owned particles
-    for (int t = ph.t0; t < ph.t1; ++t) {
+    for (int t = blockIdx.x; t < D.n_tiles; t += gridDim.x) {
         const int4 tile = __ldg(D.tiles + t);
         const SceneParams& P = D.scenes[tile.x];
         for (int i = tile.y + threadIdx.x; i < tile.z; i += BLOCK) {
@@ -2470,7 +2470,7 @@ __global__ void __launch_bounds__(BLOCK, persist_min_blocks<BLOCK>()) k_ip_persi
     }
     // epilogue (ip.py:394-404): v = d/dt for scenes that did not raise,
     // divergence, statistics
-    for (int t = ph.t0; t < ph.t1; ++t) {
+    for (int t = blockIdx.x; t < D.n_tiles; t += gridDim.x) {
         const TileCtx T = tile_ctx<G>(D, t);
         const SceneCtl& C = ph.sc_sh[T.sc];
         const SceneParams& P = D.scenes[T.sc];
@@ -2506,7 +2506,7 @@ __global__ void __launch_bounds__(BLOCK, persist_min_blocks<BLOCK>()) k_prj_pers
     if (blockIdx.x == 0 && threadIdx.x == 0)
         for (int s = 0; s < D.n_scenes; ++s)
             if (D.scenes[s].solver == SOLVER_PRJ) ctl_begin(D.scenes[s], D.ctl[s], SOLVER_PRJ);
-    for (int t = ph.t0; t < ph.t1; ++t) {
+    for (int t = blockIdx.x; t < D.n_tiles; t += gridDim.x) {
         const int4 tile = __ldg(D.tiles + t);
         const SceneParams& P = D.scenes[tile.x];
         if (P.solver == SOLVER_PRJ) pj_begin_tile(D, P, tile, threadIdx.x, BLOCK);
@@ -2517,7 +2517,7 @@ __global__ void __launch_bounds__(BLOCK, persist_min_blocks<BLOCK>()) k_prj_pers
         if (!ph.template run<MODE_PRJ>(K_PJ_HEAD)) return;
         if (!ph.template run<MODE_PRJ>(K_PJ_TAIL)) return;
     }
-    for (int t = ph.t0; t < ph.t1; ++t) {
+    for (int t = blockIdx.x; t < D.n_tiles; t += gridDim.x) {
         const TileCtx T = tile_ctx<G>(D, t);
         const SceneParams& P = D.scenes[T.sc];
         if (P.solver != SOLVER_PRJ) continue;
