@@ -303,7 +303,7 @@ def run_ours(args, rank, world, local_rank):
         scenes = shard(scenes, rank, world)
     n_dyn = sum(sc.n_dynamic for sc in scenes)
     opts = EngineOptions(lanes_per_particle=args.lanes,
-                         particles_per_block=args.ppb or 256 // args.lanes, persistent=not args.per_phase,
+                         particles_per_block=args.ppb, persistent=not args.per_phase,
                          row_format=ROW_FORMATS[args.row_format])
     eng = Engine(scenes, device=str(dev), options=opts, divergence=True)
     eng.build()
@@ -372,6 +372,7 @@ def run_ours(args, rank, world, local_rank):
             "algorithmic_bytes_per_launch": alg, "avg_launch_us": avg_s * 1e6,
             "share_of_step": dom_ms / sum(v[0] for v in prof.values()),
             "kernels_ms_per_step": {k: round(v[0] / 3, 4) for k, v in prof.items()}}
+    lanes, ppb = eng.lanes_per_particle, eng.particles_per_block
     del eng
     torch.cuda.synchronize()
 
@@ -392,8 +393,8 @@ def run_ours(args, rank, world, local_rank):
                 "dtype": "f32 (bf16 gradients)" if args.row_format == "bf16" else "f32", "data": "synthetic",
                 "config": {**workload_config(scenes, args.workload),
                            "parallelism": f"scenes sharded over {world} ranks" if sharded else f"replicas x{world}",
-                           "lanes_per_particle": args.lanes, "row_format": args.row_format,
-                           "particles_per_block": opts.particles_per_block,
+                           "lanes_per_particle": lanes, "row_format": args.row_format,
+                           "particles_per_block": ppb,
                            "solve": "per-phase launches" if args.per_phase else "persistent cooperative kernel"},
                 "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
                 "valid": bool(valid), "max_final_density_error": max(r.max_final_density_error for r in raws),
@@ -420,7 +421,7 @@ def run_served(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     reqs = S.request_stream(rate=args.served_rate, duration_s=args.served_duration, seed=rank)
-    opts = EngineOptions(lanes_per_particle=args.lanes, particles_per_block=args.ppb or 256 // args.lanes)
+    opts = EngineOptions(lanes_per_particle=args.lanes, particles_per_block=args.ppb)
     # warm-up: one small request through the same path (library, graphs, allocator)
     Server(device=str(dev), options=opts, chunk_steps=args.chunk_steps, keep_state=False).run(
         [S.Request(arrival_s=0.0, scene=S.random_column(4096, 2.0, seed=99), steps=3)])
@@ -583,7 +584,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="tall_column")
-    ap.add_argument("--lanes", type=int, default=4)
+    ap.add_argument("--lanes", type=int, default=0, help="lanes per particle (default: chosen by the engine)")
     ap.add_argument("--ppb", type=int, default=0, help="particles per CTA (default 256 / lanes)")
     ap.add_argument("--per-phase", action="store_true", help="one launch per solver phase instead of the "
                     "persistent cooperative solve")

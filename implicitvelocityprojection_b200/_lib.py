@@ -110,6 +110,7 @@ _I = ctypes.c_int32
 SIGNATURES = {
     "ivp_default_options": (None, [ctypes.POINTER(Options)]),
     "ivp_workspace_bytes": (_I, [ctypes.POINTER(SceneDesc), _I, ctypes.POINTER(Options), ctypes.POINTER(ctypes.c_size_t)]),
+    "ivp_resolve_options": (_I, [ctypes.POINTER(SceneDesc), _I, ctypes.POINTER(Options), ctypes.POINTER(Options)]),
     "ivp_engine_create": (_I, [ctypes.POINTER(SceneDesc), _I, ctypes.POINTER(Options), _P, ctypes.c_size_t, _P,
                                ctypes.POINTER(_P)]),
     "ivp_engine_destroy": (_I, [_P]),

@@ -515,6 +515,33 @@ int run(ivp_engine* e, Emitter emit, cudaGraph_t* g, cudaGraphExec_t* x, cudaStr
     return emit(e, L);
 }
 
+// Lane count 0: 4 lanes x 64 particles per tile while the dynamic particles
+// fill at most kAutoTilesPerSM tiles of 64 per SM, else 2 lanes x 128.  With
+// many tiles per CTA the persistent solves walk fewer, larger tiles per phase
+// (one block reduction per tile); with few, 4 lanes split each row wider.
+constexpr long kAutoTilesPerSM = 16;
+
+int resolve_options(const ivp_scene_desc* sc, int n, const ivp_options* in, ivp_options* out) {
+    if (!in || !out) return IVP_ERR_BAD_ARG;
+    *out = *in;
+    if (in->lanes_per_particle == 0) {
+        if (n <= 0 || !sc) return IVP_ERR_BAD_ARG;
+        long tiles = 0;
+        for (int s = 0; s < n; ++s)
+            if (sc[s].n_dynamic > 0) tiles += ((long)sc[s].n_dynamic + 63) / 64;
+        int dev = 0, sms = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) {
+            cudaGetLastError();  // no device here: size for a B200
+            sms = 148;
+        }
+        out->lanes_per_particle = tiles > kAutoTilesPerSM * sms ? 2 : 4;
+    }
+    if (in->particles_per_block == 0 && out->lanes_per_particle > 0)
+        out->particles_per_block = 256 / out->lanes_per_particle;
+    return IVP_OK;
+}
+
 int validate(const ivp_scene_desc* sc, int n, const ivp_options* o) {
     if (n <= 0 || !sc || !o) return IVP_ERR_BAD_ARG;
     if (o->lanes_per_particle != 1 && o->lanes_per_particle != 2 && o->lanes_per_particle != 4 &&
@@ -711,14 +738,21 @@ extern "C" {
 
 void ivp_default_options(ivp_options* o) {
     memset(o, 0, sizeof(*o));
-    o->lanes_per_particle = 4;
-    o->particles_per_block = 64;
+    o->lanes_per_particle = 0;  // chosen from the scenes
+    o->particles_per_block = 0;
     o->list_stride = 64;
     o->max_hist = kMaxHistDefault;
     o->use_graphs = 1;
 }
 
-int ivp_workspace_bytes(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_options* opt, size_t* bytes) {
+int ivp_resolve_options(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_options* opt, ivp_options* out) {
+    return resolve_options(scenes, n_scenes, opt, out);
+}
+
+int ivp_workspace_bytes(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_options* opt_in, size_t* bytes) {
+    ivp_options ro;
+    CKS(resolve_options(scenes, n_scenes, opt_in, &ro));
+    const ivp_options* opt = &ro;
     CKS(validate(scenes, n_scenes, opt));
     if (!bytes) return IVP_ERR_BAD_ARG;
     Plan P;
@@ -727,10 +761,13 @@ int ivp_workspace_bytes(const ivp_scene_desc* scenes, int32_t n_scenes, const iv
     return IVP_OK;
 }
 
-int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_options* opt, void* workspace,
+int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_options* opt_in, void* workspace,
                       size_t workspace_bytes, void* stream, ivp_engine** out) {
     if (!out || !workspace) return IVP_ERR_BAD_ARG;
     *out = nullptr;
+    ivp_options ro;
+    CKS(resolve_options(scenes, n_scenes, opt_in, &ro));
+    const ivp_options* opt = &ro;
     CKS(validate(scenes, n_scenes, opt));
     if (reinterpret_cast<uintptr_t>(workspace) & 255) return IVP_ERR_BAD_ARG;
     Plan P;

@@ -25,8 +25,8 @@ def _stream_ptr(stream: Optional[torch.cuda.Stream] = None) -> int:
 
 @dataclasses.dataclass
 class EngineOptions:
-    lanes_per_particle: int = 4
-    particles_per_block: int = 64
+    lanes_per_particle: int = 0   # 0: chosen from the scenes (ivp_resolve_options)
+    particles_per_block: int = 0  # 0: follows the lane count (256 threads per CTA)
     list_stride: int = 64
     max_hist: int = 128
     use_graphs: bool = True
@@ -124,6 +124,12 @@ class Engine:
         self._descs = descs
         opt = self.options.to_c()
         self._opt = opt
+        res = _lib.Options()
+        check(self.L.ivp_resolve_options(descs, len(self.scenes), ctypes.byref(opt), ctypes.byref(res)),
+              "ivp_resolve_options")
+        # the lane count and tile size the engine runs with
+        self.lanes_per_particle = int(res.lanes_per_particle)
+        self.particles_per_block = int(res.particles_per_block)
         nbytes = ctypes.c_size_t(0)
         check(self.L.ivp_workspace_bytes(descs, len(self.scenes), ctypes.byref(opt), ctypes.byref(nbytes)),
               "ivp_workspace_bytes")

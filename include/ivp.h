@@ -66,8 +66,10 @@ typedef struct {
 } ivp_scene_desc;
 
 typedef struct {
-    int32_t lanes_per_particle;   /* 1, 2, 4 or 8 lanes share one particle's neighbour sum */
-    int32_t particles_per_block;  /* particles per CTA in the neighbour-sum kernels */
+    int32_t lanes_per_particle;   /* 1, 2, 4 or 8 lanes share one particle's neighbour sum; 0 (default):
+                                     chosen from the scenes (ivp_resolve_options) */
+    int32_t particles_per_block;  /* particles per CTA in the neighbour-sum kernels; 0: chosen with
+                                     the lane count */
     int32_t list_stride;          /* neighbour-list row stride: even, >= every scene's cache_size */
     int32_t max_hist;             /* per-scene stats history length (outer iterations) */
     int32_t use_graphs;           /* 1: whole steps as CUDA graphs (device-side control, no host sync) */
@@ -132,6 +134,15 @@ typedef struct ivp_engine ivp_engine;
 
 /* Defaults for ivp_options. */
 void ivp_default_options(ivp_options* opt);
+
+/* The options an engine over these scenes runs with: a lane count of 0
+ * becomes 4 lanes x 64 particles per CTA while the scenes' dynamic
+ * particles fill at most 16 such tiles per SM of the current device, else 2
+ * lanes x 128 particles (many tiles per CTA: fewer, larger tiles per phase);
+ * a particles-per-block of 0 follows the lane count (256 threads).  Other
+ * fields are copied.  ivp_workspace_bytes and ivp_engine_create resolve the
+ * options the same way. */
+int ivp_resolve_options(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_options* opt, ivp_options* out);
 
 /* Workspace bytes for a set of scenes (no allocation). */
 int ivp_workspace_bytes(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_options* opt, size_t* bytes);
