@@ -137,6 +137,8 @@ struct Dev {
     const int4* tiles;       // (scene, slot begin, slot end, row begin)
     const int4* segs;        // neighbour-build cell segments (scene, cy, cz, x_lo)
     int n_segs;
+    int* live_segs;          // segments holding dynamic particles in the current build (any order)
+    int* seg_ctr;            // [0] live segment count
     int n_tiles;
     const int* pscene;       // scene of each particle
     // sort

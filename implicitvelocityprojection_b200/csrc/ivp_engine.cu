@@ -227,6 +227,7 @@ int emit_build(ivp_engine* e, Launcher& L) {
     CKS(L.memset0(D.cell_count, sizeof(int) * (size_t)e->n_keys));
     CKS(L.memset0(D.overflow, sizeof(int) * (size_t)e->n_scenes));
     CKS(L.memset0(D.pairs, sizeof(unsigned long long) * (size_t)e->n_scenes));
+    CKS(L.memset0(D.seg_ctr, sizeof(int)));
     CKS(L.dev(IVP_K_KEYS, k_keys, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D));
     {
         int* in = D.cell_count;
@@ -239,10 +240,11 @@ int emit_build(ivp_engine* e, Launcher& L) {
         void* a2[] = {&out, &bs, &n, &nb};
         CKS(L.kernel(IVP_K_SCAN_ADD, (const void*)k_scan_add, dim3(e->scan_blocks), dim3(SCAN_BLOCK), a2));
     }
-    CKS(L.dev(IVP_K_PLACE, k_place, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D));
+    CKS(L.dev(IVP_K_PLACE, k_place, blocks_for(std::max(e->n_total, e->n_segs), ELEM_BLOCK), ELEM_BLOCK, D));
     CKS(L.dev(IVP_K_ORDER, k_order, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D));
-    {
-        // cell-tiled build: one CTA per row segment, one warp per cell
+    if (e->n_segs > 0) {
+        // cell-tiled build: one CTA per segment holding dynamic particles
+        // (k_place listed them), one warp per cell
         Dev copy = D;
         void* args[] = {&copy};
         CKS(L.kernel(IVP_K_NBR_BUILD, (const void*)k_nbr_build<kBuildPP>, dim3(e->n_segs), dim3(256), args,
@@ -726,6 +728,8 @@ void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
     P.off[i++] = L.add(P.any_st ? sizeof(float) * N : 0);            // 47 st_inv
     P.off[i++] = L.add(P.row_fmt == ROW_BF16 ? 3 * sizeof(unsigned short) * (size_t)P.n_dyn * (size_t)o->list_stride
                                              : 0);                   // 48 bf16 gradients
+    P.off[i++] = L.add(sizeof(int) * std::max<size_t>(P.segs.size(), 1));  // 49 live_segs
+    P.off[i++] = L.add(sizeof(int));                                         // 50 seg_ctr (live segment count)
 }
 
 cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
@@ -849,6 +853,8 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
     D.st_rec = reinterpret_cast<float4*>(w + P.off[i++]);
     D.st_inv = reinterpret_cast<float*>(w + P.off[i++]);
     D.nbr_g = reinterpret_cast<unsigned short*>(w + P.off[i++]);
+    D.live_segs = reinterpret_cast<int*>(w + P.off[i++]);
+    D.seg_ctr = reinterpret_cast<int*>(w + P.off[i++]);
     D.n_segs = (int)P.segs.size();
     e->n_segs = D.n_segs;
     {

@@ -443,10 +443,33 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_add(int* __restrict__ out, 
         if (base + k < n) out[base + k] += off;
 }
 
+// Build segments: kSegW cells along x of one (y, z) cell row of a scene.
+constexpr int kSegW = 8;
+
+// Places every particle (thread p < n_total) and, once the cell starts are
+// known, appends the build segments that hold dynamic particles (thread
+// g < n_segs) to D.live_segs in any order, one atomic per warp; D.seg_ctr[0]
+// (zeroed before) ends as their count.  Most segments of a scene's grid are
+// empty (air above the fluid), so the build then runs only CTAs that work.
 __global__ void k_place(const Dev D) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= D.n_total) return;
-    D.placed[D.cell_start[D.key[p]] + D.rank[p]] = p;
+    if (p < D.n_total) D.placed[D.cell_start[D.key[p]] + D.rank[p]] = p;
+    bool live = false;
+    if (p < D.n_segs) {
+        const int4 seg = D.segs[p];
+        const SceneParams& P = D.scenes[seg.x];
+        const int dimx = P.dims[0];
+        const int x_hi = min(seg.w + kSegW, dimx) - 1;
+        const int kd0 = P.key_base + (seg.z * P.dims[1] + seg.y) * dimx;
+        live = D.cell_start[kd0 + x_hi + 1] > D.cell_start[kd0 + seg.w];
+    }
+    const unsigned ball = __ballot_sync(0xffffffffu, live);
+    if (!ball) return;
+    const int lane = threadIdx.x & 31;
+    int base = 0;
+    if (lane == 0) base = atomicAdd(D.seg_ctr, __popc(ball));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (live) D.live_segs[base + __popc(ball & ((1u << lane) - 1u))] = p;
 }
 
 // Stable order inside each cell (by particle id), then gather the particle
@@ -478,10 +501,12 @@ __global__ void k_order(const Dev D) {
 // diagonal k = 1/(Aii + 1e-3) (pressure_base.py:49-87) and the constraint
 // c = rho - rho0 (pressure_base.py:169-184).
 //
-// Cell-tiled: one CTA per segment of kSegW cells along x of one (y, z) cell
-// row.  The CTA stages the candidates of the 9 neighbouring rows x {dynamic,
-// static} -- 18 contiguous slot ranges covering x_lo-1 .. x_hi+1 -- into
-// shared memory with coalesced loads, together with their cell starts.
+// Cell-tiled: one CTA per build segment that holds dynamic particles (CTA b
+// takes D.live_segs[b]; the grid covers every segment and the CTAs past the
+// live count return at once).  The CTA stages the candidates of the 9
+// neighbouring rows x {dynamic, static} -- 18 contiguous slot ranges covering
+// x_lo-1 .. x_hi+1 -- into shared memory with coalesced loads, together with
+// their cell starts.
 //
 // One warp per cell: the particles of a cell share their 27-cell candidate
 // window, so a warp takes up to PP particles of one cell and walks the window
@@ -495,7 +520,6 @@ __global__ void k_order(const Dev D) {
 // the range starts.  The dense pass (J, density, Aii) then runs 32/PP lanes
 // per particle.  Segments whose neighbourhood exceeds the staging capacity
 // read the candidates from global memory instead.
-constexpr int kSegW = 8;
 constexpr int kStageCap = 2048;  // staged candidates per CTA (32 KB): with PP = 4, static + dynamic shared stay under 48 KB
 constexpr int kBuildPP = 4;      // particles per warp
 
@@ -515,7 +539,8 @@ __global__ void __launch_bounds__(256, 4) k_nbr_build(const Dev D) {
     __shared__ int sh_rs[NW][18];   // its stage index
     __shared__ int hit_j[NW][PP][HB];
     __shared__ short hit_s[NW][PP][HB];
-    const int4 seg = D.segs[blockIdx.x];  // (scene, cy, cz, x_lo)
+    if ((int)blockIdx.x >= D.seg_ctr[0]) return;  // past the live segments (block-uniform)
+    const int4 seg = D.segs[D.live_segs[blockIdx.x]];  // (scene, cy, cz, x_lo)
     const int sc = seg.x, cy = seg.y, cz = seg.z, x_lo = seg.w;
     const SceneParams& P = D.scenes[sc];
     const int dimx = P.dims[0];
