@@ -2232,6 +2232,9 @@ __device__ bool grid_reduce_barrier(const Dev& D, int kind, const double* partia
     return sh_flag[1] != 0;
 }
 
+// Tiles whose partials a persistent CTA collects before one combining pass.
+constexpr int kFlushTiles = 16;
+
 // Phase driver shared by the persistent kernels: tiles dealt round-robin over
 // the CTAs, local copies of the control blocks, one grid barrier + reduction
 // per phase.
@@ -2346,6 +2349,36 @@ struct Phaser {
         // window of consecutive tiles, whose rows and neighbour records are
         // close in memory (L2 reuse of the gathers), as in a launch of one CTA
         // per tile
+        // Tile partials: each warp sums its lanes (warp_sum_d) and parks the
+        // warp sum; every kFlushTiles tiles (and at the end) one CTA barrier,
+        // then warp s combines the parked sums of tile s exactly as
+        // block_sum_d does.  Warps run ahead into the next tile instead of
+        // waiting for a CTA-wide reduction after every tile.
+        constexpr int NW = BLOCK / 32;
+        __shared__ double ws_sh[2][kFlushTiles][NW];
+        __shared__ int wt_sh[kFlushTiles];
+        const int wid = threadIdx.x >> 5, wl = threadIdx.x & 31;
+        int nb = 0;
+        auto flush = [&]() {
+            __syncthreads();
+            double* pb = partials();
+            for (int s = wid; s < nb; s += NW) {
+                double t1 = wl < NW ? ws_sh[0][s][wl] : 0.0;
+                t1 = warp_sum_d(t1);
+                double t2 = 0.0;
+                if (kind == K_V_B) {
+                    t2 = wl < NW ? ws_sh[1][s][wl] : 0.0;
+                    t2 = warp_sum_d(t2);
+                }
+                if (wl == 0) {
+                    pb[wt_sh[s]] = t1;
+                    pb[D.n_tiles + wt_sh[s]] = t2;
+                    __threadfence();
+                }
+            }
+            __syncthreads();
+            nb = 0;
+        };
         int sc = (int)blockIdx.x < A ? scene_of(blockIdx.x) : 0;
         for (int a = blockIdx.x; a < A; a += gridDim.x) {
             while (a >= act_sh[sc + 1]) ++sc;
@@ -2378,14 +2411,16 @@ struct Phaser {
                 else if (kind == K_CG_A) part = cga_tile<G>(D, P, T, (float)C.beta, C.cg_it);
                 else part = cgb_tile<G>(D, P, T, (float)C.alpha, C.cg_it);
             }
-            const double tot = block_sum_d<BLOCK>(part, red_sh);
-            const double tot2 = kind == K_V_B ? block_sum_d<BLOCK>(part2, red_sh) : 0.0;
-            if (threadIdx.x == 0) {
-                double* pb = partials();
-                pb[t] = tot;
-                pb[D.n_tiles + t] = tot2;
+            const double w1 = warp_sum_d(part);
+            const double w2 = kind == K_V_B ? warp_sum_d(part2) : 0.0;
+            if (wl == 0) {
+                ws_sh[0][nb][wid] = w1;
+                ws_sh[1][nb][wid] = w2;
             }
+            if (threadIdx.x == 0) wt_sh[nb] = t;
+            if (++nb == kFlushTiles) flush();
         }
+        if (nb) flush();  // nb is the same in every thread
         if (!barrier((kind == K_ST_DIV || kind == K_PJ_HEAD) ? -1 : kind)) return false;
         if (++phases > D.phase_limit) {
             // guard: every CTA reaches the same count; CTA 0 stops the scenes,
