@@ -162,6 +162,7 @@ struct Dev {
     float4* d0;
     float4* d1;
     float4* sol;
+    float4* e;               // IP: d - sol of own slots (rhs, every CG-B), gathered by the next pack
     float4* r;               // viscosity residual (own slot only)
     // CG records, two float4 per slot (one 32-byte sector): [2i] the vector
     // the next direction is formed from (IP residual r, or the viscosity
@@ -326,17 +327,21 @@ __device__ __forceinline__ float3 row_J(const Dev& D, int row, int k, float3 xi,
 }
 
 // One 32-byte CG record (two float4, 32-byte aligned) in a single 256-bit
-// load: one L1 request per lane instead of two for a neighbour gather.
+// load: one L1 request per lane instead of two for a neighbour gather.  The
+// records of a tile's neighbourhood are gathered by many of its particles,
+// so they are kept in L1 ahead of streamed data.
 __device__ __forceinline__ void ld_rec(const float4* p, float4& a, float4& b) {
-    asm volatile("ld.global.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+    asm volatile("ld.global.L1::evict_last.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
                  : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
                  : "l"(p));
 }
 
 // Two consecutive neighbour-list entries (32-byte aligned, read-only for the
-// launch) in one 256-bit load through the non-coherent path.
+// launch) in one 256-bit load through the non-coherent path.  A row is read
+// once per pass, so it does not allocate in L1, which keeps L1 for the
+// neighbour records that the particles of a tile share.
 __device__ __forceinline__ void ld_rec_nc(const float4* p, float4& a, float4& b) {
-    asm volatile("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+    asm volatile("ld.global.nc.L1::no_allocate.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
                  : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
                  : "l"(p));
 }

@@ -730,6 +730,7 @@ void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
                                              : 0);                   // 48 bf16 gradients
     P.off[i++] = L.add(sizeof(int) * std::max<size_t>(P.segs.size(), 1));  // 49 live_segs
     P.off[i++] = L.add(sizeof(int));                                         // 50 seg_ctr (live segment count)
+    P.off[i++] = L.add(sizeof(float4) * N);                                  // 51 e = d - sol
 }
 
 cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
@@ -855,6 +856,7 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
     D.nbr_g = reinterpret_cast<unsigned short*>(w + P.off[i++]);
     D.live_segs = reinterpret_cast<int*>(w + P.off[i++]);
     D.seg_ctr = reinterpret_cast<int*>(w + P.off[i++]);
+    D.e = reinterpret_cast<float4*>(w + P.off[i++]);
     D.n_segs = (int)P.segs.size();
     e->n_segs = D.n_segs;
     {

@@ -1096,12 +1096,14 @@ __device__ __forceinline__ double pack_tile(const Dev& D, const SceneParams& P, 
     const bool upd = it >= 1;
     const float4* src = (upd && ((it - 1) & 1)) ? D.d1 : D.d0;
     float4* dst = (it & 1) ? D.d1 : D.d0;
+    // after an update the displacement is d - sol, which rhs and every CG-B
+    // stored per slot in D.e (one gather per neighbour instead of two)
+    const float4* dsrc = upd ? D.e : src;
     const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
     float3 xi = make_float3(0.f, 0.f, 0.f), di = xi;
     if (T.valid) {
         xi = f3(D.xm[T.i]);
-        di = f3(src[T.i]);
-        if (upd) di = sub3(di, f3(D.sol[T.i]));
+        di = f3(dsrc[T.i]);
     }
     float acc = 0.0f;
     bool bad = false;
@@ -1111,9 +1113,7 @@ __device__ __forceinline__ double pack_tile(const Dev& D, const SceneParams& P, 
         bad |= load_pairs<G>(D, T.row, xi, k0, cnt, self, P.s_begin, P.s_end, b);
 #pragma unroll
         for (int u = 0; u < PU; ++u) {
-            const int j = b.j[u];
-            float3 dj = f3(src[j]);
-            if (upd) dj = sub3(dj, f3(D.sol[j]));
+            const float3 dj = f3(dsrc[b.j[u]]);
             acc += dot3(sub3(di, dj), b.J[u]);
         }
     }
@@ -1139,7 +1139,8 @@ __device__ __forceinline__ double pack_tile(const Dev& D, const SceneParams& P, 
 // ip_rhs_fused (ip.py:174-215) fused with the CG start: sol = 0 (ip.py:384),
 // r = rhs, p_prev = 0, rr = r.r (ip.py:293-296).
 template <int G>
-__device__ __forceinline__ double rhs_tile(const Dev& D, const SceneParams& P, const TileCtx& T) {
+__device__ __forceinline__ double rhs_tile(const Dev& D, const SceneParams& P, const TileCtx& T,
+                                           const float4* __restrict__ dcur) {
     const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
     float3 xi = make_float3(0.f, 0.f, 0.f);
     float fki = 0.0f, mi = 0.0f;
@@ -1174,6 +1175,7 @@ __device__ __forceinline__ double rhs_tile(const Dev& D, const SceneParams& P, c
         D.cg0[2 * T.i] = rhs;
         D.cg0[2 * T.i + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
         D.sol[T.i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        D.e[T.i] = dcur[T.i];  // d - 0
         part = (double)dot3(f3(rhs), f3(rhs));
     }
     return part;
@@ -1229,7 +1231,7 @@ __device__ __forceinline__ double cga_tile(const Dev& D, const SceneParams& P, c
 // r -= alpha Ap (pcg_update_x_r_scalar, math_utils.py:181-195), rr = r.r.
 template <int G>
 __device__ __forceinline__ double cgb_tile(const Dev& D, const SceneParams& P, const TileCtx& T, float alpha,
-                                           int cg_it) {
+                                           int cg_it, const float4* __restrict__ dcur) {
     const float4* cc = (cg_it & 1) ? D.cg1 : D.cg0;  // own r
     float4* cn = (cg_it & 1) ? D.cg0 : D.cg1;        // own p; receives the new r
     const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
@@ -1269,6 +1271,8 @@ __device__ __forceinline__ double cgb_tile(const Dev& D, const SceneParams& P, c
         rs.y = rs.y - alpha * ap.y;
         rs.z = rs.z - alpha * ap.z;
         D.sol[T.i] = xs;
+        const float4 dd = dcur[T.i];
+        D.e[T.i] = make_float4(dd.x - xs.x, dd.y - xs.y, dd.z - xs.z, 0.0f);
         cn[2 * T.i] = rs;
         part = (double)dot3(f3(rs), f3(rs));
     }
@@ -1932,11 +1936,15 @@ template <int G, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_rhs(const Dev D) {
     const TileCtx T = tile_ctx<G>(D, blockIdx.x);
     __shared__ int sh_active;
-    if (threadIdx.x == 0) sh_active = D.ctl[T.sc].solve_pending;
+    __shared__ int sh_outer;
+    if (threadIdx.x == 0) {
+        sh_active = D.ctl[T.sc].solve_pending;
+        sh_outer = D.ctl[T.sc].outer_it;
+    }
     __syncthreads();
     const bool active = sh_active != 0;
     double part = 0.0;
-    if (active) part = rhs_tile<G>(D, D.scenes[T.sc], T);
+    if (active) part = rhs_tile<G>(D, D.scenes[T.sc], T, (sh_outer & 1) ? D.d1 : D.d0);
     block_finish<BLOCK>(D, T.sc, active, part, K_RHS);
 }
 
@@ -1961,18 +1969,19 @@ __global__ void __launch_bounds__(BLOCK) k_cg_a(const Dev D) {
 template <int G, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_cg_b(const Dev D) {
     const TileCtx T = tile_ctx<G>(D, blockIdx.x);
-    __shared__ int sh_active, sh_it;
+    __shared__ int sh_active, sh_it, sh_outer;
     __shared__ float sh_alpha;
     if (threadIdx.x == 0) {
         const SceneCtl& C = D.ctl[T.sc];
         sh_active = C.cg_active;
         sh_it = C.cg_it;
         sh_alpha = (float)C.alpha;
+        sh_outer = C.outer_it;
     }
     __syncthreads();
     const bool active = sh_active != 0;
     double part = 0.0;
-    if (active) part = cgb_tile<G>(D, D.scenes[T.sc], T, sh_alpha, sh_it);
+    if (active) part = cgb_tile<G>(D, D.scenes[T.sc], T, sh_alpha, sh_it, (sh_outer & 1) ? D.d1 : D.d0);
     block_finish<BLOCK>(D, T.sc, active, part, K_CG_B);
 }
 
@@ -2407,9 +2416,9 @@ struct Phaser {
                 else visc_b_tile<G>(D, T, (float)C.v_alpha, C.v_it, &part, &part2);
             } else {
                 if (kind == K_PACK) part = pack_tile<G>(D, P, T, C.outer_it);
-                else if (kind == K_RHS) part = rhs_tile<G>(D, P, T);
+                else if (kind == K_RHS) part = rhs_tile<G>(D, P, T, (C.outer_it & 1) ? D.d1 : D.d0);
                 else if (kind == K_CG_A) part = cga_tile<G>(D, P, T, (float)C.beta, C.cg_it);
-                else part = cgb_tile<G>(D, P, T, (float)C.alpha, C.cg_it);
+                else part = cgb_tile<G>(D, P, T, (float)C.alpha, C.cg_it, (C.outer_it & 1) ? D.d1 : D.d0);
             }
             const double w1 = warp_sum_d(part);
             const double w2 = kind == K_V_B ? warp_sum_d(part2) : 0.0;
