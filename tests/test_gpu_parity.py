@@ -225,6 +225,27 @@ def test_deterministic_across_execution_paths(small):
         assert o[2] == outs[0][2]
 
 
+def test_persistent_equals_per_phase_with_many_tiles_per_cta():
+    """About 600k fluid particles in 32-particle tiles: every persistent CTA
+    walks more than 16 tiles per phase, so it combines its parked per-warp
+    tile sums several times within one phase.  The results stay bit-identical
+    to one launch per phase."""
+    scs = [S.random_column(150_000, 2.0, seed=31 + k) for k in range(4)]
+    opts = dict(lanes_per_particle=8, particles_per_block=32)
+    n_tiles = sum((sc.n_dynamic + 31) // 32 for sc in scs)
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    assert n_tiles > 16 * 4 * sms  # 256-thread CTAs, at most 4 per SM at 64 registers
+    a = _engine(scs, persistent=True, **opts)
+    b = _engine(scs, persistent=False, **opts)
+    for e in (a, b):
+        e.build()
+        e.step(2)
+    for i in range(len(scs)):
+        assert np.array_equal(a.get("x", i), b.get("x", i)), i
+        assert np.array_equal(a.get("v", i), b.get("v", i)), i
+        assert a.stats(i).stats_pcg_iters == b.stats(i).stats_pcg_iters
+
+
 def test_multi_scene_persistent_equals_per_phase():
     scs = [S.random_column(2500, 1.5, seed=21), S.small_dam_break(4000, seed=22), S.random_column(900, 3.0, seed=23)]
     a = _engine(scs, persistent=True)
