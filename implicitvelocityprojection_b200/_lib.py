@@ -130,6 +130,8 @@ SIGNATURES = {
     "ivp_profile_step": (_I, [_P, _I, _P, _P, _P]),
     "ivp_read_stats": (_I, [_P, _I, _P, ctypes.POINTER(SolveStats)]),
     "ivp_read_history": (_I, [_P, _I, _P, _P, _P, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    "ivp_read_solve": (_I, [_P, _I, _P, ctypes.POINTER(SolveStats), _P, _P, _I, ctypes.POINTER(_I),
+                            ctypes.POINTER(_I)]),
     "ivp_export_neighbours": (_I, [_P, _I, _P, _P, _I, _P]),
     "ivp_density_aii_noalloc": (_I, [_P, _P, _P, _I, ctypes.c_float, _P, _I, _P, _P, _P]),
     "ivp_status_string": (ctypes.c_char_p, [_I]),

@@ -77,6 +77,8 @@ struct ivp_engine {
     Flags* h_flags = nullptr;    // pinned
     int* h_overflow = nullptr;   // pinned
     unsigned long long* h_pairs = nullptr;  // pinned
+    double* h_err = nullptr;     // pinned, max_hist: one scene's density-error history
+    int* h_pcg = nullptr;        // pinned, max_hist: one scene's CG counts per outer iteration
 };
 
 // ------------------------------------------------------------ launching
@@ -735,6 +737,72 @@ void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
 
 cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Reading a scene's solve statistics: the copies into the engine's pinned
+// mirrors are enqueued on the caller's stream, the caller synchronises once,
+// then the fill functions convert.
+int enqueue_stats(ivp_engine* e, int scene, cudaStream_t s) {
+    CK(cudaMemcpyAsync(e->h_ctl + scene, e->D.ctl + scene, sizeof(SceneCtl), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(e->h_overflow + scene, e->D.overflow + scene, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(e->h_flags, e->D.flags, sizeof(Flags), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(e->h_pairs + scene, e->D.pairs + scene, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    return IVP_OK;
+}
+
+// the scene's whole history rows (max_hist entries each)
+int enqueue_history(ivp_engine* e, int scene, cudaStream_t s) {
+    const int H = e->opt.max_hist;
+    const size_t base = (size_t)scene * H;
+    CK(cudaMemcpyAsync(e->h_err, e->D.err_hist + base, sizeof(double) * H, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(e->h_pcg, e->D.pcg_hist + base, sizeof(int) * H, cudaMemcpyDeviceToHost, s));
+    return IVP_OK;
+}
+
+int fill_stats(ivp_engine* e, int scene, ivp_solve_stats* out) {
+    const SceneCtl& C = e->h_ctl[scene];
+    memset(out, 0, sizeof(*out));
+    out->status = C.status;
+    out->outer_iters = C.outer_it;
+    out->n_density_errors = C.n_err;
+    out->overflow_particles = e->h_overflow[scene];
+    out->final_density_error = C.final_err;
+    out->last_density_error = C.err;
+    out->total_pcg_iters = C.total_cg;
+    out->solves = C.acc_solves;
+    out->failed_solves = C.acc_failed;
+    out->last_failure = C.acc_last_failure;
+    out->sum_outer_iters = C.acc_outer;
+    out->sum_pcg_iters = C.acc_cg;
+    out->max_final_density_error = C.acc_max_final_err;
+    out->neighbour_pairs = (int64_t)e->h_pairs[scene];
+    out->sum_visc_iters = C.acc_visc;
+    out->sum_st_iters = C.acc_st;
+    if (e->h_flags->timeout) {
+        g_err = "a solve exceeded its iteration budget or a grid barrier timed out";
+        out->status = IVP_ERR_TIMEOUT;
+    }
+    if (e->h_flags->bad) {
+        char buf[128];
+        snprintf(buf, sizeof(buf), "device bounds check failed: index %d at site %d", e->h_flags->bad_index,
+                 e->h_flags->bad_where);
+        g_err = buf;
+        return IVP_ERR_DEVICE_CHECK;
+    }
+    return IVP_OK;
+}
+
+// first n_err errors and outer_it CG counts of the control block in h_ctl
+void fill_history(ivp_engine* e, int scene, double* errors, int32_t* pcg_iters, int cap, int32_t* n_errors,
+                  int32_t* n_pcg) {
+    const SceneCtl& C = e->h_ctl[scene];
+    const int H = e->opt.max_hist;
+    const int ne = std::min(std::min(C.n_err, H), cap);
+    const int np = std::min(std::min(C.outer_it, H), cap);
+    if (errors && ne > 0) memcpy(errors, e->h_err, sizeof(double) * ne);
+    if (pcg_iters && np > 0) memcpy(pcg_iters, e->h_pcg, sizeof(int) * np);
+    if (n_errors) *n_errors = ne;
+    if (n_pcg) *n_pcg = np;
+}
+
 }  // namespace
 
 // ================================================================ C ABI
@@ -892,7 +960,9 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
     if (cudaHostAlloc((void**)&e->h_ctl, sizeof(SceneCtl) * n_scenes, cudaHostAllocDefault) != cudaSuccess ||
         cudaHostAlloc((void**)&e->h_flags, sizeof(Flags), cudaHostAllocDefault) != cudaSuccess ||
         cudaHostAlloc((void**)&e->h_overflow, sizeof(int) * n_scenes, cudaHostAllocDefault) != cudaSuccess ||
-        cudaHostAlloc((void**)&e->h_pairs, sizeof(unsigned long long) * n_scenes, cudaHostAllocDefault) != cudaSuccess)
+        cudaHostAlloc((void**)&e->h_pairs, sizeof(unsigned long long) * n_scenes, cudaHostAllocDefault) != cudaSuccess ||
+        cudaHostAlloc((void**)&e->h_err, sizeof(double) * opt->max_hist, cudaHostAllocDefault) != cudaSuccess ||
+        cudaHostAlloc((void**)&e->h_pcg, sizeof(int) * opt->max_hist, cudaHostAllocDefault) != cudaSuccess)
         return fail(IVP_ERR_CUDA);
     if (cudaMemcpyAsync((void*)D.scenes, P.hp.data(), sizeof(SceneParams) * n_scenes, cudaMemcpyHostToDevice, s) !=
             cudaSuccess ||
@@ -945,6 +1015,8 @@ int ivp_engine_destroy(ivp_engine* e) {
     if (e->h_flags) cudaFreeHost(e->h_flags);
     if (e->h_overflow) cudaFreeHost(e->h_overflow);
     if (e->h_pairs) cudaFreeHost(e->h_pairs);
+    if (e->h_err) cudaFreeHost(e->h_err);
+    if (e->h_pcg) cudaFreeHost(e->h_pcg);
     delete e;
     return IVP_OK;
 }
@@ -1084,59 +1156,31 @@ int ivp_step(ivp_engine* e, int32_t n_steps, void* stream) {
 int ivp_read_stats(ivp_engine* e, int32_t scene, void* stream, ivp_solve_stats* out) {
     if (!e || !out || scene < 0 || scene >= e->n_scenes) return IVP_ERR_BAD_ARG;
     cudaStream_t s = as_stream(stream);
-    CK(cudaMemcpyAsync(e->h_ctl + scene, e->D.ctl + scene, sizeof(SceneCtl), cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(e->h_overflow + scene, e->D.overflow + scene, sizeof(int), cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(e->h_flags, e->D.flags, sizeof(Flags), cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(e->h_pairs + scene, e->D.pairs + scene, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    CKS(enqueue_stats(e, scene, s));
     CK(cudaStreamSynchronize(s));
-    const SceneCtl& C = e->h_ctl[scene];
-    memset(out, 0, sizeof(*out));
-    out->status = C.status;
-    out->outer_iters = C.outer_it;
-    out->n_density_errors = C.n_err;
-    out->overflow_particles = e->h_overflow[scene];
-    out->final_density_error = C.final_err;
-    out->last_density_error = C.err;
-    out->total_pcg_iters = C.total_cg;
-    out->solves = C.acc_solves;
-    out->failed_solves = C.acc_failed;
-    out->last_failure = C.acc_last_failure;
-    out->sum_outer_iters = C.acc_outer;
-    out->sum_pcg_iters = C.acc_cg;
-    out->max_final_density_error = C.acc_max_final_err;
-    out->neighbour_pairs = (int64_t)e->h_pairs[scene];
-    out->sum_visc_iters = C.acc_visc;
-    out->sum_st_iters = C.acc_st;
-    if (e->h_flags->timeout) {
-        g_err = "a solve exceeded its iteration budget or a grid barrier timed out";
-        out->status = IVP_ERR_TIMEOUT;
-    }
-    if (e->h_flags->bad) {
-        char buf[128];
-        snprintf(buf, sizeof(buf), "device bounds check failed: index %d at site %d", e->h_flags->bad_index,
-                 e->h_flags->bad_where);
-        g_err = buf;
-        return IVP_ERR_DEVICE_CHECK;
-    }
-    return IVP_OK;
+    return fill_stats(e, scene, out);
 }
 
 int ivp_read_history(ivp_engine* e, int32_t scene, void* stream, double* errors, int32_t* pcg_iters, int32_t cap,
                      int32_t* n_errors, int32_t* n_pcg) {
     if (!e || scene < 0 || scene >= e->n_scenes || cap < 0) return IVP_ERR_BAD_ARG;
     cudaStream_t s = as_stream(stream);
-    SceneCtl C;
-    CK(cudaMemcpyAsync(&C, e->D.ctl + scene, sizeof(SceneCtl), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(e->h_ctl + scene, e->D.ctl + scene, sizeof(SceneCtl), cudaMemcpyDeviceToHost, s));
+    CKS(enqueue_history(e, scene, s));
     CK(cudaStreamSynchronize(s));
-    const int H = e->opt.max_hist;
-    const int ne = std::min(std::min(C.n_err, H), cap);
-    const int np = std::min(std::min(C.outer_it, H), cap);
-    const size_t base = (size_t)scene * H;
-    if (errors && ne > 0) CK(cudaMemcpy(errors, e->D.err_hist + base, sizeof(double) * ne, cudaMemcpyDeviceToHost));
-    if (pcg_iters && np > 0) CK(cudaMemcpy(pcg_iters, e->D.pcg_hist + base, sizeof(int) * np, cudaMemcpyDeviceToHost));
-    if (n_errors) *n_errors = ne;
-    if (n_pcg) *n_pcg = np;
+    fill_history(e, scene, errors, pcg_iters, cap, n_errors, n_pcg);
     return IVP_OK;
+}
+
+int ivp_read_solve(ivp_engine* e, int32_t scene, void* stream, ivp_solve_stats* out, double* errors,
+                   int32_t* pcg_iters, int32_t cap, int32_t* n_errors, int32_t* n_pcg) {
+    if (!e || !out || scene < 0 || scene >= e->n_scenes || cap < 0) return IVP_ERR_BAD_ARG;
+    cudaStream_t s = as_stream(stream);
+    CKS(enqueue_stats(e, scene, s));
+    CKS(enqueue_history(e, scene, s));
+    CK(cudaStreamSynchronize(s));
+    fill_history(e, scene, errors, pcg_iters, cap, n_errors, n_pcg);
+    return fill_stats(e, scene, out);
 }
 
 int ivp_export_neighbours(ivp_engine* e, int32_t scene, int32_t* count, int32_t* ids, int32_t cache, void* stream) {

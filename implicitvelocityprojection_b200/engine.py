@@ -265,14 +265,16 @@ class Engine:
         return s
 
     def stats(self, scene: int = 0, stream=None) -> Stats:
-        s = self.raw_stats(scene, stream)
-        cap = self.options.max_hist
-        err = np.zeros(cap, np.float64)
-        pcg = np.zeros(cap, np.int32)
-        ne, npc = ctypes.c_int32(0), ctypes.c_int32(0)
-        check(self.L.ivp_read_history(self._handle, scene, ctypes.c_void_p(_stream_ptr(stream)),
-                                      err.ctypes.data_as(ctypes.c_void_p), pcg.ctypes.data_as(ctypes.c_void_p),
-                                      cap, ctypes.byref(ne), ctypes.byref(npc)), "ivp_read_history")
+        """The last solve's statistics and per-outer-iteration history of a
+        scene (one stream synchronisation)."""
+        if getattr(self, "_hist", None) is None:
+            cap = self.options.max_hist
+            self._hist = (np.zeros(cap, np.float64), np.zeros(cap, np.int32), ctypes.c_int32(0), ctypes.c_int32(0))
+        err, pcg, ne, npc = self._hist
+        s = _lib.SolveStats()
+        check(self.L.ivp_read_solve(self._handle, scene, ctypes.c_void_p(_stream_ptr(stream)), ctypes.byref(s),
+                                    err.ctypes.data_as(ctypes.c_void_p), pcg.ctypes.data_as(ctypes.c_void_p),
+                                    len(err), ctypes.byref(ne), ctypes.byref(npc)), "ivp_read_solve")
         return Stats(status=int(s.status), stats_outer_iters=int(s.outer_iters),
                      stats_final_density_error=float(s.final_density_error),
                      stats_density_errors=[float(e) for e in err[:ne.value]],

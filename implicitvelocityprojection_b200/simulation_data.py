@@ -204,7 +204,7 @@ class SimulationData:
             self._engine = Engine([sp], device=str(self.device), arrays=self.live())
             self._engine_key = key
             self._engine_spec = sp
-        elif dataclasses.astuple(sp) != dataclasses.astuple(self._engine_spec):
+        elif sp != self._engine_spec:  # field-wise dataclass comparison
             self._engine.update_scene(0, sp)
             self._engine_spec = sp
         return self._engine

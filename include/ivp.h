@@ -232,6 +232,13 @@ int ivp_read_stats(ivp_engine* e, int32_t scene, void* stream, ivp_solve_stats* 
 int ivp_read_history(ivp_engine* e, int32_t scene, void* stream, double* errors, int32_t* pcg_iters, int32_t cap,
                      int32_t* n_errors, int32_t* n_pcg);
 
+/* ivp_read_stats and ivp_read_history of one scene with a single stream
+ * synchronisation: everything IP.solve leaves in its statistics attributes
+ * after a solve (pressure_base.py:331-339, ip.py:394-404), as read after
+ * every Framework.forward(). */
+int ivp_read_solve(ivp_engine* e, int32_t scene, void* stream, ivp_solve_stats* out, double* errors,
+                   int32_t* pcg_iters, int32_t cap, int32_t* n_errors, int32_t* n_pcg);
+
 /* Exports the neighbour lists of one scene in the reference's cache layout
  * (neighbor_count[N], neighbor_ids[N*cache]) with original particle indices,
  * for parity checks.  Synchronous, device pointers. */

@@ -246,6 +246,34 @@ def test_persistent_equals_per_phase_with_many_tiles_per_cta():
         assert a.stats(i).stats_pcg_iters == b.stats(i).stats_pcg_iters
 
 
+def test_read_solve_equals_stats_and_history():
+    """ivp_read_solve (one synchronisation) returns what ivp_read_stats and
+    ivp_read_history return separately, for every scene of a batch."""
+    import ctypes
+    from implicitvelocityprojection_b200 import _lib
+    scs = [S.random_column(2500, 1.5, seed=41), S.small_dam_break(4000, seed=42)]
+    eng = _engine(scs)
+    eng.build()
+    eng.step(2)
+    L, h, st = eng.L, eng._handle, ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    cap = 16
+    for i in range(len(scs)):
+        a = _lib.SolveStats()
+        assert L.ivp_read_stats(h, i, st, ctypes.byref(a)) == _lib.OK
+        e1, p1 = np.zeros(cap), np.zeros(cap, np.int32)
+        n1, m1 = ctypes.c_int32(0), ctypes.c_int32(0)
+        assert L.ivp_read_history(h, i, st, e1.ctypes.data_as(ctypes.c_void_p), p1.ctypes.data_as(ctypes.c_void_p),
+                                  cap, ctypes.byref(n1), ctypes.byref(m1)) == _lib.OK
+        b = _lib.SolveStats()
+        e2, p2 = np.full(cap, -1.0), np.full(cap, -1, np.int32)
+        n2, m2 = ctypes.c_int32(0), ctypes.c_int32(0)
+        assert L.ivp_read_solve(h, i, st, ctypes.byref(b), e2.ctypes.data_as(ctypes.c_void_p),
+                                p2.ctypes.data_as(ctypes.c_void_p), cap, ctypes.byref(n2), ctypes.byref(m2)) == _lib.OK
+        assert bytes(a) == bytes(b)
+        assert (n1.value, m1.value) == (n2.value, m2.value) and n1.value >= 1
+        assert np.array_equal(e1[:n1.value], e2[:n2.value]) and np.array_equal(p1[:m1.value], p2[:m2.value])
+
+
 def test_multi_scene_persistent_equals_per_phase():
     scs = [S.random_column(2500, 1.5, seed=21), S.small_dam_break(4000, seed=22), S.random_column(900, 3.0, seed=23)]
     a = _engine(scs, persistent=True)
