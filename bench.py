@@ -507,7 +507,7 @@ def run_e2e_batch(args, scenes, dev, opts):
     x_h.copy_(x_d)
     v_h.copy_(v_d)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    steps = max(1, min(args.steps, args.e2e_steps))
+    steps = args.steps if args.e2e_steps <= 0 else max(1, min(args.steps, args.e2e_steps))
 
     def one():
         x_d.copy_(x_h, non_blocking=True)
@@ -517,7 +517,7 @@ def run_e2e_batch(args, scenes, dev, opts):
         v_h.copy_(v_d, non_blocking=True)
         torch.cuda.synchronize()
 
-    for _ in range(min(args.warmup, 3)):
+    for _ in range(args.warmup):
         one()
     tot = 0.0
     for _ in range(steps):
@@ -553,8 +553,8 @@ def run_e2e(args, sc, dev):
     x_h.copy_(ps.x[:n])
     v_h.copy_(ps.v[:n])
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    steps = max(1, min(args.steps, args.e2e_steps))
-    for _ in range(min(args.warmup, 3)):
+    steps = args.steps if args.e2e_steps <= 0 else max(1, min(args.steps, args.e2e_steps))
+    for _ in range(args.warmup):
         ps.x[:n].copy_(x_h, non_blocking=True)
         ps.v[:n].copy_(v_h, non_blocking=True)
         fw.forward()
@@ -588,7 +588,8 @@ def main():
     ap.add_argument("--ppb", type=int, default=0, help="particles per CTA (default 256 / lanes)")
     ap.add_argument("--per-phase", action="store_true", help="one launch per solver phase instead of the "
                     "persistent cooperative solve")
-    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--e2e-steps", type=int, default=0,
+                    help="steps of the end-to-end measurement (default: the same as --steps)")
     ap.add_argument("--cpu-budget-s", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
