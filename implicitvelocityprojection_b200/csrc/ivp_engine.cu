@@ -224,13 +224,15 @@ bool kernel_set(int G, int B, KernelSet* out) {
     return false;
 }
 
-int emit_build(ivp_engine* e, Launcher& L) {
+// with_advect: the step's advection runs fused with the key pass
+int emit_build_impl(ivp_engine* e, Launcher& L, bool with_advect) {
     const Dev& D = e->D;
     CKS(L.memset0(D.cell_count, sizeof(int) * (size_t)e->n_keys));
     CKS(L.memset0(D.overflow, sizeof(int) * (size_t)e->n_scenes));
     CKS(L.memset0(D.pairs, sizeof(unsigned long long) * (size_t)e->n_scenes));
     CKS(L.memset0(D.seg_ctr, sizeof(int)));
-    CKS(L.dev(IVP_K_KEYS, k_keys, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D));
+    if (with_advect) CKS(L.dev(IVP_K_ADVECT, k_advect_keys, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D));
+    else CKS(L.dev(IVP_K_KEYS, k_keys, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D));
     {
         int* in = D.cell_count;
         int* out = D.cell_start;
@@ -255,6 +257,8 @@ int emit_build(ivp_engine* e, Launcher& L) {
     CKS(L.dev(IVP_K_STATIC_OUT, k_static_outputs, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D));
     return IVP_OK;
 }
+
+int emit_build(ivp_engine* e, Launcher& L) { return emit_build_impl(e, L, false); }
 
 int add_conditional(cudaGraph_t g, Launcher& L, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type,
                     cudaGraph_t* body) {
@@ -471,12 +475,7 @@ int emit_step(ivp_engine* e, Launcher& L) {
     CKS(emit_forces(e, L));
     CKS(emit_solve(e, L, true));
     CKS(emit_prj(e, L));
-    {
-        Dev d = e->D;
-        d.advect_skip_failed = 1;
-        CKS(L.dev(IVP_K_ADVECT, k_advect, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, d));
-    }
-    CKS(emit_build(e, L));
+    CKS(emit_build_impl(e, L, true));  // advection (skipping scenes whose solve failed) + the next build
     return IVP_OK;
 }
 

@@ -358,12 +358,8 @@ __device__ void block_finish(const Dev& D, int sc, bool active, double part, int
 
 // Cell key and rank within the cell for every particle (neighbour_search.py:116-129,
 // the HashGrid build, as a counting sort).
-__global__ void k_keys(const Dev D) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= D.n_total) return;
-    const int sc = D.pscene[p];
+__device__ __forceinline__ void cell_key(const Dev& D, int p, int sc, float px, float py, float pz) {
     const SceneParams& P = D.scenes[sc];
-    const float px = D.x[3 * p], py = D.x[3 * p + 1], pz = D.x[3 * p + 2];
     const int cx = cell_coord(px, P.cell_inv, P.dims[0]);
     const int cy = cell_coord(py, P.cell_inv, P.dims[1]);
     const int cz = cell_coord(pz, P.cell_inv, P.dims[2]);
@@ -371,6 +367,12 @@ __global__ void k_keys(const Dev D) {
     const int key = P.key_base + (D.dyn[p] ? 0 : P.ncell) + cell;
     D.key[p] = key;
     D.rank[p] = atomicAdd(&D.cell_count[key], 1);
+}
+
+__global__ void k_keys(const Dev D) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= D.n_total) return;
+    cell_key(D, p, D.pscene[p], D.x[3 * p], D.x[3 * p + 1], D.x[3 * p + 2]);
 }
 
 // Exclusive scan, pass 1: per-block scan of 4 elements per thread.
@@ -904,11 +906,7 @@ __global__ void k_solve_end(const Dev D) {
 }
 
 // advect_position (framework.py:117-136) + enforce_boundary (boundary.py:27-91)
-__global__ void k_advect(const Dev D) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= D.n_total) return;
-    const int sc = D.pscene[p];
-    if (D.advect_skip_failed && D.ctl[sc].status != IVP_OK_) return;
+__device__ __forceinline__ void advect_particle(const Dev& D, int p, int sc, float pos_out[3]) {
     const SceneParams& P = D.scenes[sc];
     float* x = D.x + 3 * p;
     float* v = D.v + 3 * p;
@@ -945,6 +943,37 @@ __global__ void k_advect(const Dev D) {
     x[0] = pos[0];
     x[1] = pos[1];
     x[2] = pos[2];
+    pos_out[0] = pos[0];
+    pos_out[1] = pos[1];
+    pos_out[2] = pos[2];
+}
+
+__global__ void k_advect(const Dev D) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= D.n_total) return;
+    const int sc = D.pscene[p];
+    if (D.advect_skip_failed && D.ctl[sc].status != IVP_OK_) return;
+    float pos[3];
+    advect_particle(D, p, sc, pos);
+}
+
+// The end of a step: advection fused with the first pass of the next
+// neighbour build (the cell key and in-cell rank of the moved particle).
+// Particles of a scene whose solve failed keep their positions, as in
+// k_advect with advect_skip_failed.
+__global__ void k_advect_keys(const Dev D) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= D.n_total) return;
+    const int sc = D.pscene[p];
+    float pos[3];
+    if (D.ctl[sc].status != IVP_OK_) {
+        pos[0] = D.x[3 * p];
+        pos[1] = D.x[3 * p + 1];
+        pos[2] = D.x[3 * p + 2];
+    } else {
+        advect_particle(D, p, sc, pos);
+    }
+    cell_key(D, p, sc, pos[0], pos[1], pos[2]);
 }
 
 // ------------------------------------------------------------- IP solve
