@@ -254,7 +254,6 @@ int emit_build_impl(ivp_engine* e, Launcher& L, bool with_advect) {
         CKS(L.kernel(IVP_K_NBR_BUILD, (const void*)k_nbr_build<kBuildPP>, dim3(e->n_segs), dim3(256), args,
                      sizeof(float4) * kStageCap));
     }
-    CKS(L.dev(IVP_K_STATIC_OUT, k_static_outputs, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D));
     return IVP_OK;
 }
 

@@ -495,6 +495,7 @@ __global__ void k_order(const Dev D) {
     D.xm[slot] = make_float4(D.x[3 * p], D.x[3 * p + 1], D.x[3 * p + 2], m);
     D.rho0s[slot] = D.rho0[p];
     D.inv_m[slot] = D.dyn[p] ? __frcp_rn(m) : 0.0f;  // the reference's m_inv (simulation_data.py:53-56)
+    if (!D.dyn[p]) D.k_out[p] = 0.0f;  // static k is zero (pressure_base.py:65-67); the build writes dynamic k
 }
 
 // Neighbour lists of every dynamic particle (build_neighbor_cache,
