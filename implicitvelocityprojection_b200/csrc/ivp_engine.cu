@@ -227,12 +227,16 @@ bool kernel_set(int G, int B, KernelSet* out) {
 // with_advect: the step's advection runs fused with the key pass
 int emit_build_impl(ivp_engine* e, Launcher& L, bool with_advect) {
     const Dev& D = e->D;
-    CKS(L.memset0(D.cell_count, sizeof(int) * (size_t)e->n_keys));
-    CKS(L.memset0(D.overflow, sizeof(int) * (size_t)e->n_scenes));
-    CKS(L.memset0(D.pairs, sizeof(unsigned long long) * (size_t)e->n_scenes));
-    CKS(L.memset0(D.seg_ctr, sizeof(int)));
-    if (with_advect) CKS(L.dev(IVP_K_ADVECT, k_advect_keys, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D));
-    else CKS(L.dev(IVP_K_KEYS, k_keys, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D));
+    // cell_count is all zero between builds (k_place clears what it used)
+    if (with_advect) {
+        CKS(L.dev(IVP_K_ADVECT, k_advect_keys, blocks_for(std::max(e->n_total, e->n_scenes), ELEM_BLOCK), ELEM_BLOCK,
+                  D));
+    } else {
+        CKS(L.memset0(D.overflow, sizeof(int) * (size_t)e->n_scenes));
+        CKS(L.memset0(D.pairs, sizeof(unsigned long long) * (size_t)e->n_scenes));
+        CKS(L.memset0(D.seg_ctr, sizeof(int)));
+        CKS(L.dev(IVP_K_KEYS, k_keys, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D));
+    }
     {
         int* in = D.cell_count;
         int* out = D.cell_start;

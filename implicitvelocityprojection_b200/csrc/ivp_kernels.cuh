@@ -455,7 +455,14 @@ constexpr int kSegW = 8;
 // empty (air above the fluid), so the build then runs only CTAs that work.
 __global__ void k_place(const Dev D) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p < D.n_total) D.placed[D.cell_start[D.key[p]] + D.rank[p]] = p;
+    if (p < D.n_total) {
+        const int key = D.key[p];
+        D.placed[D.cell_start[key] + D.rank[p]] = p;
+        // the scan has consumed the counts: every nonzero count belongs to
+        // some particle's key, so this leaves cell_count all zero for the
+        // next build (the workspace starts zeroed)
+        D.cell_count[key] = 0;
+    }
     bool live = false;
     if (p < D.n_segs) {
         const int4 seg = D.segs[p];
@@ -959,11 +966,18 @@ __global__ void k_advect(const Dev D) {
 }
 
 // The end of a step: advection fused with the first pass of the next
-// neighbour build (the cell key and in-cell rank of the moved particle).
+// neighbour build (the cell key and in-cell rank of the moved particle),
+// and the zeroing of the build's per-scene counters.
 // Particles of a scene whose solve failed keep their positions, as in
 // k_advect with advect_skip_failed.
 __global__ void k_advect_keys(const Dev D) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    // the build's per-scene counters start from zero (read from k_place on)
+    if (p < D.n_scenes) {
+        D.overflow[p] = 0;
+        D.pairs[p] = 0ull;
+    }
+    if (p == 0) D.seg_ctr[0] = 0;
     if (p >= D.n_total) return;
     const int sc = D.pscene[p];
     float pos[3];
