@@ -391,7 +391,8 @@ int emit_force(ivp_engine* e, Launcher& L, int force) {
     const int kid = force == FORCE_ST ? IVP_K_SURFACE_TENSION : IVP_K_VISC;
     Dev D0 = e->D;
     D0.force = force;
-    if (force == FORCE_ST) CKS(L.dev(kid, k_slot_velocity, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D0));
+    // slot-ordered {v, 1/rho if fluid} for the setup's neighbour gathers
+    CKS(L.dev(kid, k_slot_velocity, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D0));
     CKS(L.dev(kid, k_visc_begin, nt, e->T, D0));
     if (force == FORCE_ST) CKS(L.dev(kid, K.st_div, nt, B, D0));
     if (!L.graph) {

@@ -1364,11 +1364,10 @@ __device__ __forceinline__ double visc_setup_tile(const Dev& D, const SceneParam
     const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
     const bool fluid = T.valid && D.rflu[T.i] != 0.0f;
     float3 xi = make_float3(0.f, 0.f, 0.f), vi = xi;
+    // vs holds every slot's {v, 1/rho if fluid} (written before the setup)
     if (T.valid) {
         xi = f3(D.xm[T.i]);
-        const int p = D.pid[T.i];
-        vi = make_float3(D.v[3 * p], D.v[3 * p + 1], D.v[3 * p + 2]);
-        D.vs[T.i] = make_float4(vi.x, vi.y, vi.z, 0.0f);
+        vi = f3(D.vs[T.i]);
     }
     const float eps2 = 0.01f * P.h * P.h;
     float L[9];
@@ -1384,10 +1383,10 @@ __device__ __forceinline__ double visc_setup_tile(const Dev& D, const SceneParam
         for (int u = 0; u < PU; ++u) {
             const int j = b.j[u];
             const float3 xij = sub3(xi, f3(__ldg(D.xm + j)));
-            const int pj = D.pid[j];
-            const float3 vij = sub3(vi, make_float3(D.v[3 * pj], D.v[3 * pj + 1], D.v[3 * pj + 2]));
+            const float4 vj = D.vs[j];
+            const float3 vij = sub3(vi, f3(vj));
             const float rsq = dot3(xij, xij);
-            const float c = (10.0f * __ldg(D.rflu + j)) * __frcp_rn(rsq + eps2);
+            const float c = (10.0f * vj.w) * __frcp_rn(rsq + eps2);
             const float3 J = b.J[u];
             const float Jv[3] = {J.x, J.y, J.z}, Xv[3] = {xij.x, xij.y, xij.z};
 #pragma unroll
@@ -2524,6 +2523,15 @@ __global__ void __launch_bounds__(BLOCK, persist_min_blocks<BLOCK>()) k_force_pe
             force_begin(D, D.scenes[s], c);
             D.ctl[s] = c;
         }
+    if constexpr (FORCE == FORCE_VISC) {
+        // slot-ordered {v, 1/rho if fluid} of every slot for the setup's
+        // neighbour gathers (the surface-tension solve gets the same record
+        // from k_slot_velocity)
+        for (int s = blockIdx.x * BLOCK + threadIdx.x; s < D.n_total; s += gridDim.x * BLOCK) {
+            const int p = D.pid[s];
+            D.vs[s] = make_float4(D.v[3 * p], D.v[3 * p + 1], D.v[3 * p + 2], D.dyn[p] ? D.rflu[s] : 0.0f);
+        }
+    }
     if (!ph.barrier(-1)) return;
     ph.refresh();
     if (!ph.any(K_V_SETUP)) return;
