@@ -19,7 +19,7 @@ no mesh library:
 Particles are appended in the reference's order (fluid blocks, generated
 bodies, boundary walls), with its dtypes at every step, so positions are
 bit-identical to the reference loader's.  `RigidBodies` / `FluidBodies` are
-OBJ meshes voxelised with trimesh, which is not part of this build: an entry
+OBJ meshes voxelised with trimesh, which this package does not use: an entry
 must then carry its points already voxelised (`"voxelizedPoints"`, world
 coordinates) or loading raises.  `SolidBodies` and `ScheduledSpawns` belong to
 the elasticity and spawn systems, which are out of this path's scope.
@@ -78,7 +78,7 @@ def load_scene(src: Union[str, dict], name: str = None) -> Scene:
     conf = data.get("Configuration", {})
     unsupported = [k for k in ("SolidBodies", "ScheduledSpawns") if data.get(k)]
     if unsupported:
-        raise NotImplementedError(f"{', '.join(unsupported)}: elasticity and scheduled spawns are outside this build")
+        raise NotImplementedError(f"{', '.join(unsupported)}: elasticity and scheduled spawns are outside this package")
     radius = float(conf.get("particleRadius", 0.01))
     diameter = 2.0 * radius  # config_builder.py:46-52
     rho0 = float(conf.get("density0", 1000.0))
