@@ -348,12 +348,11 @@ def run_ours(args, rank, world, local_rank):
     prof = eng.profile_step(3)
     pairs = [int(r.neighbour_pairs) for r in eng_stats(eng, len(scenes))]
     if not args.per_phase:
-        # gravity, advection fused with the cell keys, 2 scan passes, place,
-        # order, neighbour build; one persistent kernel per solve that runs
-        # (IP, PRJ, viscosity) and two for surface tension (slot velocities +
-        # solve)
-        n_launch = (7 + int("ip_solve" in prof) + int("prj" in prof) + int("visc" in prof) +
-                    2 * int("surface_tension" in prof)) * args.steps
+        # every step launches the same kernels (gravity unless the viscosity
+        # kernel applies it, one persistent kernel per solve, the slot
+        # velocities of the surface tension, advection + keys, two scan
+        # passes, place, order, neighbour build): the profiled steps' count
+        n_launch = int(round(sum(v[1] for v in prof.values()) * args.steps / 3))
     else:
         so = sum(r.sum_outer_iters for r in raws)
         n_launch = 10 * args.steps + (so + args.steps) + so + 2 * sum(r.sum_pcg_iters for r in raws)

@@ -205,6 +205,9 @@ struct Dev {
     // advect leaves scenes whose last solve raised where they are (the
     // reference raises before advecting, framework.py:483-513)
     int advect_skip_failed;
+    // the viscosity kernel applies the step's gravity in its prologue (set on
+    // step launches whose first force is the viscosity; k_gravity is then skipped)
+    int fold_gravity;
     // the persistent solve runs the viscosity phases (set on step launches)
     int visc_enabled;
     int force;               // implicit non-pressure solve of this launch: 0 viscosity, 1 surface tension

@@ -448,13 +448,14 @@ int emit_advect(ivp_engine* e, Launcher& L) {
     return L.dev(IVP_K_ADVECT, k_advect, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, e->D);
 }
 
-int emit_force_persistent(ivp_engine* e, Launcher& L, int force) {
+int emit_force_persistent(ivp_engine* e, Launcher& L, int force, bool fold_gravity = false) {
     if (e->n_tiles == 0 || !force_any(e, force)) return IVP_OK;
     KernelSet K;
     kernel_set(e->G, e->BLOCK, &K);
     CKS(L.memset0(e->D.bar_count, sizeof(unsigned)));
     Dev copy = e->D;
     copy.force = force;
+    copy.fold_gravity = fold_gravity && force == FORCE_VISC ? 1 : 0;
     if (force == FORCE_ST)
         CKS(L.dev(IVP_K_SURFACE_TENSION, k_slot_velocity, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, copy));
     void* args[] = {&copy};
@@ -475,8 +476,16 @@ int emit_forces(ivp_engine* e, Launcher& L) {
 }
 
 int emit_step(ivp_engine* e, Launcher& L) {
-    CKS(L.dev(IVP_K_GRAVITY, k_gravity, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, e->D));
-    CKS(emit_forces(e, L));
+    // with the viscosity as the step's first force (persistent, no surface
+    // tension), its kernel applies gravity in its prologue, which visits every
+    // slot before anything reads v
+    const bool fold = e->persistent && e->n_tiles > 0 && e->any_visc && !e->any_st;
+    if (fold) {
+        CKS(emit_force_persistent(e, L, FORCE_VISC, true));
+    } else {
+        CKS(L.dev(IVP_K_GRAVITY, k_gravity, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, e->D));
+        CKS(emit_forces(e, L));
+    }
     CKS(emit_solve(e, L, true));
     CKS(emit_prj(e, L));
     CKS(emit_build_impl(e, L, true));  // advection (skipping scenes whose solve failed) + the next build

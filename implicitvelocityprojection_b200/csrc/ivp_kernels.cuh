@@ -2529,7 +2529,20 @@ __global__ void __launch_bounds__(BLOCK, persist_min_blocks<BLOCK>()) k_force_pe
         // from k_slot_velocity)
         for (int s = blockIdx.x * BLOCK + threadIdx.x; s < D.n_total; s += gridDim.x * BLOCK) {
             const int p = D.pid[s];
-            D.vs[s] = make_float4(D.v[3 * p], D.v[3 * p + 1], D.v[3 * p + 2], D.dyn[p] ? D.rflu[s] : 0.0f);
+            const bool dyn = D.dyn[p] != 0;
+            float vx = D.v[3 * p], vy = D.v[3 * p + 1], vz = D.v[3 * p + 2];
+            if (D.fold_gravity && dyn) {
+                // apply_gravity (framework.py:26-41), as k_gravity computes it
+                const SceneParams& P = D.scenes[D.pscene[p]];
+                const float gx = P.gravity[0] * P.dt, gy = P.gravity[1] * P.dt, gz = P.gravity[2] * P.dt;
+                vx = vx + gx;
+                vy = vy + gy;
+                vz = vz + gz;
+                D.v[3 * p] = vx;
+                D.v[3 * p + 1] = vy;
+                D.v[3 * p + 2] = vz;
+            }
+            D.vs[s] = make_float4(vx, vy, vz, dyn ? D.rflu[s] : 0.0f);
         }
     }
     if (!ph.barrier(-1)) return;
