@@ -132,7 +132,8 @@ enum {
 
 typedef struct ivp_engine ivp_engine;
 
-/* Defaults for ivp_options. */
+/* Defaults for ivp_options: engine settings with no counterpart in the
+ * reference (its solver settings are per scene, in ivp_scene_desc). */
 void ivp_default_options(ivp_options* opt);
 
 /* The options an engine over these scenes runs with: a lane count of 0
@@ -141,10 +142,13 @@ void ivp_default_options(ivp_options* opt);
  * lanes x 128 particles (many tiles per CTA: fewer, larger tiles per phase);
  * a particles-per-block of 0 follows the lane count (256 threads).  Other
  * fields are copied.  ivp_workspace_bytes and ivp_engine_create resolve the
- * options the same way. */
+ * options the same way.  No counterpart in the reference (Warp picks its own
+ * launch shapes). */
 int ivp_resolve_options(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_options* opt, ivp_options* out);
 
-/* Workspace bytes for a set of scenes (no allocation). */
+/* Workspace bytes for a set of scenes (no allocation).  Replaces the
+ * solver's own allocations at particle_max_num (ip.py:232-242,
+ * pressure_base.py:290-302) with one caller-owned workspace. */
 int ivp_workspace_bytes(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_options* opt, size_t* bytes);
 
 /* Creates an engine over a caller-owned device workspace of
@@ -221,14 +225,17 @@ int ivp_reset_counters(ivp_engine* e, void* stream);
 /* Runs n_steps of ivp_step with host-driven launches (no graphs) and CUDA
  * events around every kernel; accumulates per-kernel device milliseconds and
  * launch counts into ms[IVP_K_COUNT] and launches[IVP_K_COUNT].  Synchronous.
- * Same results as ivp_step. */
+ * Same results as ivp_step.  The reference times only whole solves
+ * (stats_total_cost_ms, pressure_base.py:331-339); no per-kernel counterpart. */
 int ivp_profile_step(ivp_engine* e, int32_t n_steps, void* stream, double* ms, int32_t* launches);
 
-/* Synchronises the stream and copies one scene's stats of the last solve. */
+/* Synchronises the stream and copies one scene's stats of the last solve:
+ * the statistics attributes of IP / PressureBase (pressure_base.py:331-339). */
 int ivp_read_stats(ivp_engine* e, int32_t scene, void* stream, ivp_solve_stats* out);
 
 /* Copies up to `cap` per-outer-iteration density errors / CG iteration counts
- * of the last solve (stats_density_errors, stats_pcg_iters).  Synchronous. */
+ * of the last solve (stats_density_errors, stats_pcg_iters,
+ * pressure_base.py:331-339).  Synchronous. */
 int ivp_read_history(ivp_engine* e, int32_t scene, void* stream, double* errors, int32_t* pcg_iters, int32_t cap,
                      int32_t* n_errors, int32_t* n_pcg);
 
