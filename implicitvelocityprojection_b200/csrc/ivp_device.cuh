@@ -19,9 +19,12 @@
 //     neighbour sum then streams its row and gathers only the neighbour's
 //     operand: mass-weighted terms use (m_j a_i + m_i a_j) grad W_ij =
 //     (a_i + m_i (a_j / m_j)) J_ij with a_j / m_j stored per particle;
-//   * tiles: (scene, first slot, end slot, first row) -- a CTA never spans
-//     two scenes, so per-scene reductions are per-CTA partials summed in a
-//     fixed order by the scene's last CTA (deterministic FP64).
+//   * tiles: (scene, first slot, end slot, first row) -- a tile never spans
+//     two scenes, so per-scene reductions are per-tile FP64 partials summed
+//     in one fixed association over the scene's tiles (128 logical lanes,
+//     then a fixed tree), whichever CTA or launch produced them: the same
+//     bits in the persistent and per-phase paths and for a scene alone or
+//     in a batch.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -63,8 +66,10 @@ struct SceneParams {
     double tol_opt, tol_pcg;
 };
 
-// Per-scene solver control block, written only by the scene's last CTA of a
-// launch and read by every CTA of the next launch.
+// Per-scene solver control block, written by the CTA that decides a phase
+// (the scene's last CTA of a per-phase launch; in a persistent kernel CTA 0
+// or the last CTA to arrive at the barrier) and read by every CTA of the next
+// phase.
 struct SceneCtl {
     double err;          // last average density error
     double rr_old;

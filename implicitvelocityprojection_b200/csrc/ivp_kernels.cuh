@@ -2,13 +2,16 @@
 //
 // Bandwidth-bound sparse neighbour sums on CUDA cores (no tensor cores: the
 // operator is a gather over ~30 neighbours per particle, ~1 flop/byte).
-// Every neighbour-sum kernel maps G lanes to one particle: lane l takes list
-// entries l, l+G, ... (coalesced 8-byte row reads) and the group reduces
-// with shuffles.  Reductions across particles are FP64 per-CTA partials,
-// summed in a fixed order by the last CTA of each scene, which also runs the
+// Every neighbour-sum kernel maps G lanes to one particle: lane l takes the
+// list entries 2l, 2l+1, then 2l+2G, ... (two entries per 256-bit row read)
+// and the group reduces with shuffles.  Reductions across particles are FP64
+// per-tile partials, summed per scene in one fixed association.  With one
+// launch per phase, the last CTA of each scene sums them and runs the
 // scene's solver control (outer loop / CG decisions of ip.py:346-392 and
-// ip.py:283-329); the last CTA of the launch sets the CUDA-graph conditional
-// variables, so a whole step runs without a host round trip.
+// ip.py:283-329), and the last CTA of the launch sets the CUDA-graph
+// conditional variables, so a whole step runs without a host round trip.  The
+// persistent kernels sum them at each grid barrier (every CTA when there are
+// one or two scenes, else the last CTA to arrive).
 #pragma once
 #include "ivp_device.cuh"
 
