@@ -79,6 +79,38 @@ def test_oversized_request_rejected_and_idle_gaps_skipped():
     assert rep.results[0].admit_s >= 100.0  # virtual clock jumped to the arrival
 
 
+class _Failed:
+    status = 0
+    failed_solves = 1
+    last_failure = 3  # IVP_ERR_NOT_CONVERGED
+
+
+class FailingEngine(FakeEngine):
+    """A scene named "bad" reports a failed solve after every chunk."""
+
+    def raw_stats(self, i):
+        return _Failed() if self.scenes[i].name == "bad" else _Stats()
+
+
+def test_failed_request_leaves_batch_others_continue():
+    """A request whose solve fails finishes at the end of that chunk with the
+    solve's status and leaves the batch; the requests batched with it run to
+    their end with their state carried exactly, as if it had never been
+    there."""
+    reqs = [_req(0.0, 10, 9, "a"), _req(0.0, 5, 20, "bad"), _req(0.0, 8, 6, "c")]
+    FakeEngine.built = []
+    srv = Server(engine_factory=FailingEngine, footprint=lambda sc: sc.n, hbm_budget_bytes=1000, chunk_steps=4)
+    rep = srv.run(reqs)
+    by = {r.rid: r for r in rep.results}
+    assert by[1].status == 3 and by[1].steps == 4
+    for rid in (0, 2):
+        assert by[rid].status == 0 and by[rid].steps == reqs[rid].steps
+        assert np.all(by[rid].x == np.float32(reqs[rid].steps))
+    assert all("bad" not in names for names in FakeEngine.built[1:])  # re-planned without it
+    s = rep.summary()
+    assert s["completed"] == 2 and s["failed"] == 1 and s["rejected"] == 0
+
+
 def test_workspace_footprint_grows_with_particles():
     from implicitvelocityprojection_b200.engine import workspace_bytes
     small = workspace_bytes([S.random_column(3000, 2.0, seed=1)])
