@@ -11,8 +11,13 @@ box, Weiler 2018 implicit viscosity nu = 1e-3 m^2/s, dt = 1 ms.
 One step = one full Framework.forward() of every replica's scene (gravity,
 implicit viscosity where the workload enables it, the IP solve with its CG,
 advect + boundary clamp, neighbour rebuild, density, Aii, divergence).  The
-value counts fluid particles x steps / device time; each timed step must end
-with status OK and its final average density error below densityErrorTol.
+value counts fluid particles x timed steps / device time of those steps.  The
+`--steps K` timed steps are spread evenly over the workload's configured run
+(500 steps for the tall column: a collapsing column needs more iterations per
+step late than early), after `--warmup W` untimed steps; each timed step has
+the L2 flushed before it (outside its CUDA events).  Every step of the run
+must end with status OK and its final average density error below
+densityErrorTol.
 
 Multi-GPU (torchrun): the plain form does not shard a scene, so every rank
 runs an independent replica (weak scaling, no data-path collective); time is
@@ -100,55 +105,135 @@ def workload_config(scenes, name: str) -> dict:
 # ----------------------------------------------------------------- clocks
 
 class ClockSampler:
-    """nvidia-smi samples during the timed region (50 ms period)."""
+    """SM clock, power and clock-event reasons of the benchmarked GPU, read
+    through NVML every 5 ms in a background thread while the timed region
+    runs (reading only; no setting of the GPU is changed).  Falls back to
+    nvidia-smi (50 ms period) when NVML is not importable."""
 
+    REASONS = (("hw_slowdown", "HwSlowdown"), ("hw_thermal_slowdown", "HwThermalSlowdown"),
+               ("sw_thermal_slowdown", "SwThermalSlowdown"), ("sw_power_cap", "SwPowerCap"),
+               ("hw_power_brake", "HwPowerBrakeSlowdown"))
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index: int):
-        self.gpu = gpu_index
-        self.proc = None
-        self.lines = []
+    def __init__(self, cuda_index: int, period_s: float = 0.005):
+        self.cuda_index = cuda_index
+        self.period = period_s
+        self.samples = []  # (sm_mhz, sm_max_mhz, power_w, reason names)
+        self._stop = threading.Event()
+        self._thread = None
+        self._proc = None
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.cuda_index).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.cuda_index)
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-        except Exception:
-            self.proc = None
+            nv, h = self._nvml_handle()
+            bits = []
+            for name, suffix in self.REASONS:
+                v = getattr(nv, "nvmlClocksEventReason" + suffix, getattr(nv, "nvmlClocksThrottleReason" + suffix, 0))
+                bits.append((name, int(v)))
+            get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons",
+                                  getattr(nv, "nvmlDeviceGetCurrentClocksThrottleReasons", None))
+            smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            def loop():
+                while not self._stop.is_set():
+                    try:
+                        sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                        pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+                        r = int(get_reasons(h)) if get_reasons else 0
+                        self.samples.append((sm, smax, pw, [n for n, b in bits if b and (r & b)]))
+                    except Exception:
+                        pass
+                    self._stop.wait(self.period)
+
+            self.source = "nvml (5 ms)"
+            self._thread = threading.Thread(target=loop, daemon=True)
+            self._thread.start()
+            return
+        except Exception:
+            pass
+        try:
+            self._proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.cuda_index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                text=True)
+            self.source = "nvidia-smi (50 ms)"
+
+            def read():
+                names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+                for ln in self._proc.stdout:
+                    f = [x.strip() for x in ln.split(",")]
+                    if len(f) < 9:
+                        continue
+                    try:
+                        self.samples.append((float(f[1]), float(f[2]), float(f[3]),
+                                             [n for n, v in zip(names, f[5:9]) if v.lower().startswith("active")]))
+                    except ValueError:
+                        continue
+
+            self._thread = threading.Thread(target=read, daemon=True)
+            self._thread.start()
+        except Exception:
+            self._proc = None
 
     def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
+        self._stop.set()
+        if self._proc is not None:
+            self._proc.terminate()
             try:
-                sm.append(float(f[1]))
-                smax.append(float(f[2]))
-            except ValueError:
-                continue
-            for nm, val in zip(names, f[5:9]):
-                if val.lower().startswith("active"):
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                self._proc.wait(timeout=5)
+            except Exception:
+                self._proc.kill()
+        if self._thread is not None:
+            self._thread.join(timeout=5)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0, "source": self.source}
+        sm = [x[0] for x in self.samples]
+        reasons = sorted({n for x in self.samples for n in x[3]})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(x[1] for x in self.samples),
+                "sm_mhz_min": min(sm), "power_w_max": max(x[2] for x in self.samples), "reasons": reasons,
+                "samples": len(sm), "source": self.source}
+
+
+# ----------------------------------------------------------------- schedule
+
+# Steps of each workload's configuration: the timed steps are spread evenly
+# over this many steps, so the measurement covers the whole run (a collapsing
+# column needs more iterations per step late than early).
+CONFIG_STEPS = {"tall_column": 500, "tall_column_ip": 500, "tall_column_prj": 500, "small_column": 200,
+                "dam_break": 1000, "dam_break_ip": 1000}
+
+
+def config_steps(workload: str) -> int:
+    if workload.startswith("batch"):
+        return 300
+    return CONFIG_STEPS.get(workload, 0)
+
+
+def timed_schedule(warmup: int, steps: int, run_steps: int):
+    """Indices (0-based, after `warmup` untimed steps) of the `steps` timed
+    steps, spread evenly over a run of `run_steps` steps; the run is extended
+    when it is shorter than warm-up plus timed steps."""
+    span = max(run_steps - warmup, steps)
+    return [warmup + (j * span) // steps + (span // steps) // 2 for j in range(steps)]
+
+
+def schedule_note(warmup: int, steps: int, run_steps: int) -> str:
+    span = max(run_steps - warmup, steps)
+    return (f"{steps} timed steps spread evenly over steps {warmup + 1}-{warmup + span} of a "
+            f"{warmup + span}-step run (every {span / steps:.1f}th step), after {warmup} warm-up steps")
 
 
 # ----------------------------------------------------------------- roofline
@@ -220,13 +305,32 @@ def load_traffic(kernel: str, workload: str):
 
 # ----------------------------------------------------------------- arms
 
-def cpu_baseline(scenes, budget_s: float, max_steps: int):
-    """The oracle (C restatement, OpenMP) stepping the same workload: one
-    scene for up to `budget_s`, or for a batch, two steps of each scene in
-    turn until the budget is spent."""
+def cpu_baseline(scenes, budget_s: float, max_steps: int, states=None):
+    """The oracle (C restatement, OpenMP) stepping the same workload.  With
+    `states` (GPU states (x, v) sampled along the timed run of a single
+    scene), one oracle step from each sampled state, rebuilt first (untimed),
+    so the sample covers the same part of the run as the device-timed steps;
+    else one scene for up to `budget_s`, or for a batch, two steps of each
+    scene in turn until the budget is spent."""
     from oracle import oracle as O
     if not isinstance(scenes, (list, tuple)):
         scenes = [scenes]
+    if states and len(scenes) == 1:
+        sc = scenes[0]
+        t_all, k = 0.0, 0
+        for x, v in states:
+            st = O.State.from_scene(sc, x=np.array(x, np.float32), v=np.array(v, np.float32))
+            st.rebuild()
+            t0 = time.perf_counter()
+            st.step(fast=True)
+            t_all += time.perf_counter() - t0
+            k += 1
+            if t_all >= budget_s:
+                break
+        sample = (f"one step from each of {k} GPU states sampled evenly along the timed run of {sc.name} "
+                  f"({sc.n_dynamic} fluid particles), {t_all:.1f} s")
+        return {"value": sc.n_dynamic * k / t_all, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
+                "sample": sample}
     per_scene = max_steps if len(scenes) == 1 else 2
     t_all, ps, steps, used = 0.0, 0, 0, 0
     for sc in scenes:
@@ -252,8 +356,9 @@ def cpu_baseline(scenes, budget_s: float, max_steps: int):
 
 def run_reference(args, rank, world):
     """The CPU restatement of the reference's step (the oracle, OpenMP on the
-    host cores) on the same workload; for a batch, one step is one step of
-    every scene.  Timed steps stop early once `--ref-budget-s` is spent."""
+    host cores) on the same workload, warm-up and timed-step schedule as the
+    GPU arm; for a batch, one step is one step of every scene.  Timing stops
+    early once `--ref-budget-s` of timed CPU steps is spent."""
     if rank != 0:
         return
     scenes = make_scenes(args.workload)
@@ -264,27 +369,35 @@ def run_reference(args, rank, world):
         st.rebuild()
         states.append(st)
     n_dyn = sum(sc.n_dynamic for sc in scenes)
-    for _ in range(min(args.warmup, 3)):
-        for st in states:
-            st.step(fast=True)
+    run_steps = args.run_steps if args.run_steps > 0 else config_steps(args.workload)
+    sched = timed_schedule(args.warmup, args.steps, run_steps)
     times = []
     t_start = time.perf_counter()
-    for _ in range(args.steps):
+    k = 0
+    for t in sched:
+        while k < t:  # warm-up and the untimed steps between timed ones
+            for st in states:
+                st.step(fast=True)
+            k += 1
         t0 = time.perf_counter()
         for st in states:
             st.step(fast=True)
         times.append(time.perf_counter() - t0)
+        k += 1
         if time.perf_counter() - t_start > args.ref_budget_s:
             break
     tot = sum(times)
     value = n_dyn * len(times) / tot
     name = scenes[0].name if len(scenes) == 1 else f"{len(scenes)} scenes"
+    note = schedule_note(args.warmup, args.steps, run_steps)
+    if len(times) < args.steps:
+        note += f"; stopped after {len(times)} timed steps (budget {args.ref_budget_s:.0f} s)"
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": len(times),
             "warmup": args.warmup, "ms_per_step": 1000 * tot / len(times), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "impl": "reference", "config": workload_config(scenes, args.workload),
+            "impl": "reference", "config": {**workload_config(scenes, args.workload), "timed": note},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": O.num_threads(), "kind": "port",
-                             "sample": f"{len(times)} full steps of {name} on the CPU restatement"},
+                             "sample": f"{len(times)} full steps of {name} on the CPU restatement ({note})"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "p50_ms": 1000 * statistics.median(times), "p99_ms": 1000 * float(np.percentile(times, 99))}
     print(json.dumps(line), flush=True)
@@ -309,6 +422,8 @@ def run_ours(args, rank, world, local_rank):
     eng.build()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream()
+    run_steps = args.run_steps if args.run_steps > 0 else config_steps(args.workload)
+    sched = timed_schedule(args.warmup, args.steps, run_steps)
     for _ in range(args.warmup):
         flush.zero_()
         eng.step(1)
@@ -316,22 +431,33 @@ def run_ours(args, rank, world, local_rank):
     eng.reset_counters()
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    # GPU states at evenly spaced timed steps, for the CPU baseline's sample
+    sample_at = set(sched[:: max(1, len(sched) // 20)]) if (rank == 0 and world == 1 and not args.no_cpu
+                                                            and len(scenes) == 1) else set()
+    sampled = []
     clocks = ClockSampler(local_rank)
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
     clocks.start()
     wall0 = time.perf_counter()
-    for k in range(args.steps):
+    k = args.warmup
+    for j, t in enumerate(sched):
+        if t > k:
+            eng.step(t - k)  # untimed steps between timed ones (the run goes on)
+        if t in sample_at:
+            sampled.append((eng.arrays["x"].cpu().numpy(), eng.arrays["v"].cpu().numpy()))
         flush.zero_()
-        starts[k].record(stream)
+        starts[j].record(stream)
         eng.step(1)
-        ends[k].record(stream)
+        ends[j].record(stream)
+        k = t + 1
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
     wall = time.perf_counter() - wall0
     clk = clocks.stop()
+    run_after_warmup = k - args.warmup  # steps run between the brackets (timed and untimed)
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     total_ms = float(sum(step_ms))
     raws = [eng.raw_stats(i) for i in range(len(scenes))]
@@ -339,42 +465,51 @@ def run_ours(args, rank, world, local_rank):
         t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         total_ms = float(t.item())
-    valid = all(r.failed_solves == 0 and r.solves == args.steps and r.max_final_density_error < sc.density_error_tol
-                for r, sc in zip(raws, scenes))
+    # every step after the warm-up, timed or not, must end converged
+    valid = all(r.failed_solves == 0 and r.solves == run_after_warmup
+                and r.max_final_density_error < sc.density_error_tol for r, sc in zip(raws, scenes))
     value = (n_dyn_job if sharded else world * n_dyn) * args.steps / (total_ms / 1000.0)
 
-    # per-kernel device time of the same workload (host-driven launches with
-    # CUDA events around each kernel, after the timed region)
-    prof = eng.profile_step(3)
-    pairs = [int(r.neighbour_pairs) for r in eng_stats(eng, len(scenes))]
+    # per-kernel device time at the end of the run (host-driven launches with
+    # CUDA events around each kernel), with the iteration counts of exactly
+    # the profiled steps for the roofline's per-launch bytes
+    n_prof = 3
+    eng.reset_counters()
+    prof = eng.profile_step(n_prof)
+    praws = [eng.raw_stats(i) for i in range(len(scenes))]
+    pairs = [int(r.neighbour_pairs) for r in praws]
     if not args.per_phase:
         # every step launches the same kernels (gravity unless the viscosity
         # kernel applies it, one persistent kernel per solve, the slot
         # velocities of the surface tension, advection + keys, two scan
         # passes, place, order, neighbour build): the profiled steps' count
-        n_launch = int(round(sum(v[1] for v in prof.values()) * args.steps / 3))
+        per_step = sum(v[1] for v in prof.values()) / n_prof
+        n_launch = int(round(per_step * run_after_warmup))
+        n_launch_timed = int(round(per_step * args.steps))
     else:
         so = sum(r.sum_outer_iters for r in raws)
-        n_launch = 10 * args.steps + (so + args.steps) + so + 2 * sum(r.sum_pcg_iters for r in raws)
+        n_launch = 10 * run_after_warmup + (so + run_after_warmup) + so + 2 * sum(r.sum_pcg_iters for r in raws)
+        n_launch_timed = int(round(n_launch * args.steps / run_after_warmup))
     dom = max(prof.items(), key=lambda kv: kv[1][0])
     dom_name, (dom_ms, dom_n) = dom
     avg_s = dom_ms / dom_n / 1000.0
+
+    def iters(r, sc, n):
+        return {"outer": r.sum_outer_iters / n, "cg": r.sum_pcg_iters / n, "visc": r.sum_visc_iters / n,
+                "visc_on": sc.viscosity_method == 1, "st": r.sum_st_iters / n}
+
     alg = 0.0
-    for sc, r, pr in zip(scenes, raws, pairs):
-        it = {"outer": r.sum_outer_iters / args.steps, "cg": r.sum_pcg_iters / args.steps,
-              "visc": r.sum_visc_iters / args.steps, "visc_on": sc.viscosity_method == 1,
-              "st": r.sum_st_iters / args.steps}
-        alg += algorithmic_bytes(dom_name, sc.n_dynamic, sc.n, pr, it)
+    for sc, r, pr in zip(scenes, praws, pairs):
+        alg += algorithmic_bytes(dom_name, sc.n_dynamic, sc.n, pr, iters(r, sc, n_prof))
     peak, peak_kind = load_peaks()
     achieved = alg / avg_s / 1e9 if avg_s > 0 else 0.0
     # the whole step: algorithmic bytes of every kernel that runs (neighbour
     # build, each solve, and the glue passes: gravity, advection, 64 B per
-    # fluid particle) over the measured step time
+    # fluid particle) over the measured step time, with the iteration counts
+    # averaged over every step of the timed run (its pair count at the end)
     step_bytes = 0.0
     for sc, r, pr in zip(scenes, raws, pairs):
-        it = {"outer": r.sum_outer_iters / args.steps, "cg": r.sum_pcg_iters / args.steps,
-              "visc": r.sum_visc_iters / args.steps, "visc_on": sc.viscosity_method == 1,
-              "st": r.sum_st_iters / args.steps}
+        it = iters(r, sc, run_after_warmup)
         step_bytes += algorithmic_bytes("nbr_build", sc.n_dynamic, sc.n, pr) + 64 * sc.n_dynamic
         step_bytes += algorithmic_bytes("prj" if sc.pressure_method == 0 else "ip_solve", sc.n_dynamic, sc.n, pr, it)
         if sc.viscosity_method == 1 and sc.viscosity_coeff > 0:
@@ -387,9 +522,10 @@ def run_ours(args, rank, world, local_rank):
             "frac": achieved / peak, "peak_kind": peak_kind, "traffic": load_traffic(dom_name, args.workload),
             "algorithmic_bytes_per_launch": alg, "avg_launch_us": avg_s * 1e6,
             "share_of_step": dom_ms / sum(v[0] for v in prof.values()),
+            "measured_on": f"{n_prof} host-driven steps at the end of the run, CUDA events around each launch",
             "step": {"algorithmic_bytes": step_bytes, "achieved": step_gbs, "frac_of_measured": step_gbs / peak,
                      "frac_of_nominal": step_gbs / 8000.0, "nominal_gbs": 8000.0},
-            "kernels_ms_per_step": {k: round(v[0] / 3, 4) for k, v in prof.items()}}
+            "kernels_ms_per_step": {k: round(v[0] / n_prof, 4) for k, v in prof.items()}}
     lanes, ppb = eng.lanes_per_particle, eng.particles_per_block
     del eng
     torch.cuda.synchronize()
@@ -402,7 +538,7 @@ def run_ours(args, rank, world, local_rank):
         serial = run_serial(args, scenes, dev, opts, value / world)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(scenes, args.cpu_budget_s, 200)
+        cpu = cpu_baseline(scenes, args.cpu_budget_s, 200, states=sampled)
     if rank == 0:
         so = sum(r.sum_outer_iters for r in raws)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -413,15 +549,17 @@ def run_ours(args, rank, world, local_rank):
                            "parallelism": f"scenes sharded over {world} ranks" if sharded else f"replicas x{world}",
                            "lanes_per_particle": lanes, "row_format": args.row_format,
                            "particles_per_block": ppb,
-                           "solve": "per-phase launches" if args.per_phase else "persistent cooperative kernel"},
+                           "solve": "per-phase launches" if args.per_phase else "persistent cooperative kernel",
+                           "timed": schedule_note(args.warmup, args.steps, run_steps)},
                 "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
                 "valid": bool(valid), "max_final_density_error": max(r.max_final_density_error for r in raws),
-                "outer_iters_per_step": so / args.steps / len(scenes),
-                "cg_iters_per_step": sum(r.sum_pcg_iters for r in raws) / args.steps / len(scenes),
-                "visc_cg_iters_per_step": sum(r.sum_visc_iters for r in raws) / args.steps / len(scenes),
-                "st_cg_iters_per_step": sum(r.sum_st_iters for r in raws) / args.steps / len(scenes),
-                "mean_neighbours": sum(pairs) / max(n_dyn, 1),
-                "wall_s": wall, "gpu_launches": int(n_launch), "clocks": clk, "roofline": roof,
+                "outer_iters_per_step": so / run_after_warmup / len(scenes),
+                "cg_iters_per_step": sum(r.sum_pcg_iters for r in raws) / run_after_warmup / len(scenes),
+                "visc_cg_iters_per_step": sum(r.sum_visc_iters for r in raws) / run_after_warmup / len(scenes),
+                "st_cg_iters_per_step": sum(r.sum_st_iters for r in raws) / run_after_warmup / len(scenes),
+                "mean_neighbours": sum(pairs) / max(n_dyn, 1), "steps_run_in_timed_region": run_after_warmup,
+                "wall_s": wall, "gpu_launches": int(n_launch), "gpu_launches_timed_steps": int(n_launch_timed),
+                "clocks": clk, "roofline": roof,
                 "cpu_baseline": cpu, "e2e": e2e}
         if serial is not None:
             line["serial"] = serial
@@ -511,10 +649,15 @@ def run_serial(args, scenes, dev, opts, batched_value):
             "form": "each scene alone in its own engine, device-timed steps summed"}
 
 
+def _e2e_schedule(args):
+    run_steps = args.run_steps if args.run_steps > 0 else config_steps(args.workload)
+    return timed_schedule(args.warmup, args.steps, run_steps)
+
+
 def run_e2e_batch(args, scenes, dev, opts):
     """Batched form end to end through Engine: every step copies all scenes'
     x and v from pinned host memory into the bound arrays, steps, and copies
-    them back."""
+    them back; the steps of the device-timed schedule are timed."""
     import torch
     from implicitvelocityprojection_b200.engine import Engine
     eng = Engine(scenes, device=str(dev), options=opts)
@@ -525,7 +668,6 @@ def run_e2e_batch(args, scenes, dev, opts):
     x_h.copy_(x_d)
     v_h.copy_(v_d)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    steps = args.steps if args.e2e_steps <= 0 else max(1, min(args.steps, args.e2e_steps))
 
     def one():
         x_d.copy_(x_h, non_blocking=True)
@@ -535,26 +677,31 @@ def run_e2e_batch(args, scenes, dev, opts):
         v_h.copy_(v_d, non_blocking=True)
         torch.cuda.synchronize()
 
-    for _ in range(args.warmup):
-        one()
-    tot = 0.0
-    for _ in range(steps):
+    sched = _e2e_schedule(args)
+    k, tot = 0, 0.0
+    for t in sched:
+        while k < t:
+            one()
+            k += 1
         flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         one()
         tot += time.perf_counter() - t0
+        k += 1
     n = int(x_d.shape[0])
     nd = sum(sc.n_dynamic for sc in scenes)
     del eng
-    return {"value": nd * steps / tot, "unit": UNIT, "h2d_bytes_per_step": 2 * n * 12,
-            "d2h_bytes_per_step": 2 * n * 12, "steps": steps,
-            "api": "Engine(scenes).step(1) with every scene's x, v copied from/to pinned host memory every step"}
+    return {"value": nd * len(sched) / tot, "unit": UNIT, "h2d_bytes_per_step": 2 * n * 12,
+            "d2h_bytes_per_step": 2 * n * 12, "steps": len(sched),
+            "api": "Engine(scenes).step(1) with every scene's x, v copied from/to pinned host memory every step "
+                   "(the device-timed schedule's steps timed)"}
 
 
 def run_e2e(args, sc, dev):
     """Same metric through the public API (SimulationData + Framework.forward)
-    with the step's state coming from and going back to pinned host memory."""
+    with every step's state coming from and going back to pinned host memory;
+    the steps of the device-timed schedule are timed (host clock, synchronised)."""
     import torch
     from implicitvelocityprojection_b200.config import SimConfig
     from implicitvelocityprojection_b200.framework import Framework
@@ -571,28 +718,31 @@ def run_e2e(args, sc, dev):
     x_h.copy_(ps.x[:n])
     v_h.copy_(ps.v[:n])
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    steps = args.steps if args.e2e_steps <= 0 else max(1, min(args.steps, args.e2e_steps))
-    for _ in range(args.warmup):
-        ps.x[:n].copy_(x_h, non_blocking=True)
-        ps.v[:n].copy_(v_h, non_blocking=True)
-        fw.forward()
-        x_h.copy_(ps.x[:n])
-        v_h.copy_(ps.v[:n])
-    tot = 0.0
-    for _ in range(steps):
-        flush.zero_()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
+
+    def one():
         ps.x[:n].copy_(x_h, non_blocking=True)
         ps.v[:n].copy_(v_h, non_blocking=True)
         fw.forward()  # raises on a failed solve; reads the stats (one sync)
         x_h.copy_(ps.x[:n], non_blocking=True)
         v_h.copy_(ps.v[:n], non_blocking=True)
         torch.cuda.synchronize()
+
+    sched = _e2e_schedule(args)
+    k, tot = 0, 0.0
+    for t in sched:
+        while k < t:
+            one()
+            k += 1
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        one()
         tot += time.perf_counter() - t0
-    return {"value": sc.n_dynamic * steps / tot, "unit": UNIT, "h2d_bytes_per_step": 2 * n * 12,
-            "d2h_bytes_per_step": 2 * n * 12 + 256, "steps": steps,
-            "api": "Framework.forward() with x, v copied from/to pinned host memory every step"}
+        k += 1
+    return {"value": sc.n_dynamic * len(sched) / tot, "unit": UNIT, "h2d_bytes_per_step": 2 * n * 12,
+            "d2h_bytes_per_step": 2 * n * 12 + 256, "steps": len(sched),
+            "api": "Framework.forward() with x, v copied from/to pinned host memory every step "
+                   "(the device-timed schedule's steps timed)"}
 
 
 def main():
@@ -606,8 +756,9 @@ def main():
     ap.add_argument("--ppb", type=int, default=0, help="particles per CTA (default 256 / lanes)")
     ap.add_argument("--per-phase", action="store_true", help="one launch per solver phase instead of the "
                     "persistent cooperative solve")
-    ap.add_argument("--e2e-steps", type=int, default=0,
-                    help="steps of the end-to-end measurement (default: the same as --steps)")
+    ap.add_argument("--run-steps", type=int, default=0,
+                    help="steps of the run over which the timed steps are spread (default: the workload's "
+                         "configured step count, e.g. 500 for the tall column)")
     ap.add_argument("--cpu-budget-s", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")

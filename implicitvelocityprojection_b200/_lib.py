@@ -92,6 +92,9 @@ class SolveStats(ctypes.Structure):
         ("neighbour_pairs", ctypes.c_int64),
         ("sum_visc_iters", ctypes.c_int64),
         ("sum_st_iters", ctypes.c_int64),
+        ("last_pap", ctypes.c_double),
+        ("last_cg_iter", ctypes.c_int32),
+        ("fixup_entries", ctypes.c_int32),
     ]
 
 
@@ -133,6 +136,9 @@ SIGNATURES = {
     "ivp_read_solve": (_I, [_P, _I, _P, ctypes.POINTER(SolveStats), _P, _P, _I, ctypes.POINTER(_I),
                             ctypes.POINTER(_I)]),
     "ivp_export_neighbours": (_I, [_P, _I, _P, _P, _I, _P]),
+    "ivp_set_wait_limit": (_I, [_P, ctypes.c_int64]),
+    "ivp_prepare": (_I, [_P]),
+    "ivp_read_stats_all": (_I, [_P, _P, ctypes.POINTER(SolveStats)]),
     "ivp_density_aii_noalloc": (_I, [_P, _P, _P, _I, ctypes.c_float, _P, _I, _P, _P, _P]),
     "ivp_status_string": (ctypes.c_char_p, [_I]),
     "ivp_last_error": (ctypes.c_char_p, []),

@@ -17,7 +17,7 @@ REPO = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libivp.so")
 SOURCES = ["ivp_engine.cu", "ivp_noalloc.cu"]
-DEPS = ["ivp_engine.cu", "ivp_noalloc.cu", "ivp_kernels.cuh", "ivp_device.cuh"]
+DEPS = ["ivp_engine.cu", "ivp_noalloc.cu", "ivp_kernels.cuh", "ivp_device.cuh", "ivp_scan.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -158,6 +158,24 @@ struct Dev {
     int* inv;                // particle -> slot
     int* overflow;           // per scene
     unsigned long long* pairs;  // per scene: neighbour pairs of the last build
+    // neighbour-cache overflow (a dynamic particle with more than cache_size
+    // neighbours): its row is rebuilt with the reference's first cache_size
+    // hits, and CG phase B adds the transpose terms the gather form gets
+    // wrong for pairs that appear in only one of the two rows (the
+    // reference's scatter form, ip.py:110-121, is the exact transpose)
+    int* ovf_list;           // [n_dyn] slots whose lists were truncated in the current build
+    int* ovf_ctr;            // [0] truncated particles, [1] dropped dynamic pairs
+    int2* drop;              // [drop_cap] (o, k): dynamic k within h of o, left out of o's row
+    float4* drop_w;          // [drop_cap] J_ko of k's row entry for o, .w = 1; .w = 0 if o is not in k's row
+    int drop_cap;
+    int* fix_cnt;            // [n_total] corrections per target slot (all zero outside the fix-up)
+    int* fix_off;            // [n_total + 1] CSR offsets of the corrections by target slot
+    int* fix_bsums;          // scan block sums of fix_cnt
+    float4* fix_w;           // [2 drop_cap] {w, source slot}: phase B adds -omega y_source w
+    int* fix_fail;           // [n_scenes] 1: more dropped pairs than drop_cap (the IP solve stops
+                             // with IVP_ERR_NBR_OVERFLOW)
+    int* fix_scene;          // [n_scenes] corrections of the scene in the current build
+    unsigned long long h_fix;  // graph conditional: the build sets it when a list was truncated
     // per slot
     float4* xm;
     float* rho0s;
@@ -221,6 +239,7 @@ struct Dev {
     unsigned* bar_count;
     unsigned* bar_gen;
     long long phase_limit;
+    unsigned long long bar_limit_ns;  // longest wait on a grid barrier before giving up (default 2 s)
 };
 
 // ------------------------------------------------------------------ math

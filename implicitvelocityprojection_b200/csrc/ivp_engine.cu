@@ -51,6 +51,10 @@ inline int blocks_for(int n, int b) { return (n + b - 1) / b; }
 
 }  // namespace
 
+namespace ivp {
+void set_last_error(const std::string& msg) { g_err = msg; }
+}  // namespace ivp
+
 struct ivp_engine {
     std::vector<ivp_scene_desc> desc;
     std::vector<SceneParams> hp;
@@ -59,6 +63,9 @@ struct ivp_engine {
     Dev D{};
     int G = 4, BLOCK = 128, T = 32;
     int n_total = 0, n_dyn_total = 0, n_keys = 0, n_tiles = 0, scan_blocks = 0, n_segs = 0;
+    int fix_scan_blocks = 0;
+    int* h_ovf = nullptr;        // pinned: truncated-list count read back by host-driven builds
+    int* h_fix_scene = nullptr;  // pinned, n_scenes: corrections per scene
     int n_scenes = 0;
     bool bound = false;
     bool want_divergence = false;
@@ -224,6 +231,34 @@ bool kernel_set(int G, int B, KernelSet* out) {
     return false;
 }
 
+int add_conditional(cudaGraph_t g, Launcher& L, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type,
+                    cudaGraph_t* body);
+
+// Rows of truncated lists in the reference's order, then the transpose
+// corrections of CG phase B (k_ovf_* in ivp_kernels.cuh).  Runs only after a
+// build that truncated a list.
+int emit_overflow_fix(ivp_engine* e, Launcher& L) {
+    const Dev& D = e->D;
+    int sms = 148, dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaGetLastError();
+    CKS(L.dev(IVP_K_NBR_BUILD, k_ovf_rows, 2 * sms, 256, D));
+    CKS(L.dev(IVP_K_NBR_BUILD, k_ovf_pairs, 4 * sms, 256, D));
+    {
+        int* in = D.fix_cnt;
+        int* out = D.fix_off;
+        int* bs = D.fix_bsums;
+        int n = e->n_total;
+        void* a1[] = {&in, &out, &bs, &n};
+        CKS(L.kernel(IVP_K_NBR_BUILD, (const void*)k_scan_local, dim3(e->fix_scan_blocks), dim3(SCAN_BLOCK), a1));
+        int nb = e->fix_scan_blocks;
+        void* a2[] = {&out, &bs, &n, &nb};
+        CKS(L.kernel(IVP_K_NBR_BUILD, (const void*)k_scan_add, dim3(e->fix_scan_blocks), dim3(SCAN_BLOCK), a2));
+    }
+    CKS(L.dev(IVP_K_NBR_BUILD, k_ovf_fill, 4 * sms, 256, D));
+    return L.dev(IVP_K_NBR_BUILD, k_ovf_sort, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D);
+}
+
 // with_advect: the step's advection runs fused with the key pass
 int emit_build_impl(ivp_engine* e, Launcher& L, bool with_advect) {
     const Dev& D = e->D;
@@ -235,6 +270,9 @@ int emit_build_impl(ivp_engine* e, Launcher& L, bool with_advect) {
         CKS(L.memset0(D.overflow, sizeof(int) * (size_t)e->n_scenes));
         CKS(L.memset0(D.pairs, sizeof(unsigned long long) * (size_t)e->n_scenes));
         CKS(L.memset0(D.seg_ctr, sizeof(int)));
+        CKS(L.memset0(D.ovf_ctr, 4 * sizeof(int)));
+        CKS(L.memset0(D.fix_fail, sizeof(int) * (size_t)e->n_scenes));
+        CKS(L.memset0(D.fix_scene, sizeof(int) * (size_t)e->n_scenes));
         CKS(L.dev(IVP_K_KEYS, k_keys, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D));
     }
     {
@@ -254,9 +292,26 @@ int emit_build_impl(ivp_engine* e, Launcher& L, bool with_advect) {
         // cell-tiled build: one CTA per segment holding dynamic particles
         // (k_place listed them), one warp per cell
         Dev copy = D;
+        cudaGraphConditionalHandle h_fix = 0;
+        if (L.graph) {
+            // the build sets it when a list was truncated; reset every launch
+            CK(cudaGraphConditionalHandleCreate(&h_fix, L.graph, 0, cudaGraphCondAssignDefault));
+            copy.h_fix = (unsigned long long)h_fix;
+        }
         void* args[] = {&copy};
         CKS(L.kernel(IVP_K_NBR_BUILD, (const void*)k_nbr_build<kBuildPP>, dim3(e->n_segs), dim3(256), args,
                      sizeof(float4) * kStageCap));
+        if (L.graph) {
+            cudaGraph_t body;
+            CKS(add_conditional(L.graph, L, h_fix, cudaGraphCondTypeIf, &body));
+            Launcher Lb;
+            Lb.graph = body;
+            CKS(emit_overflow_fix(e, Lb));
+        } else {
+            CK(cudaMemcpyAsync(e->h_ovf, D.ovf_ctr, sizeof(int), cudaMemcpyDeviceToHost, L.stream));
+            CK(cudaStreamSynchronize(L.stream));
+            if (*e->h_ovf > 0) CKS(emit_overflow_fix(e, L));
+        }
     }
     return IVP_OK;
 }
@@ -598,9 +653,16 @@ struct Plan {
     int n_total = 0, n_dyn = 0, n_keys = 0, scan_blocks = 0;
     int row_fmt = 0;       // ROW_FULL (16 B entries), ROW_COMPACT ({j, w}, 8 B), ROW_BF16 (4 B id + 6 B)
     bool any_st = false;   // some scene runs the implicit surface tension
-    size_t off[56];
+    int drop_cap = 0;      // dropped-pair records of the overflow fix-up
+    int fix_scan_blocks = 0;
+    size_t off[64];
     Layout lay;
 };
+
+// Dropped-pair records: two per dynamic particle plus this floor.  A build
+// that drops more pairs stops the affected scenes' IP solves with
+// IVP_ERR_NBR_OVERFLOW rather than solve with an uncorrected operator.
+constexpr int kDropFloor = 65536;
 
 void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
     const int T = o->particles_per_block;
@@ -745,6 +807,19 @@ void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
     P.off[i++] = L.add(sizeof(int) * std::max<size_t>(P.segs.size(), 1));  // 49 live_segs
     P.off[i++] = L.add(sizeof(int));                                         // 50 seg_ctr (live segment count)
     P.off[i++] = L.add(sizeof(float4) * N);                                  // 51 e = d - sol
+    // neighbour-cache overflow fix-up
+    P.drop_cap = 2 * std::max(P.n_dyn, 1) + kDropFloor;
+    P.fix_scan_blocks = std::max(1, (P.n_total + SCAN_TILE - 1) / SCAN_TILE);
+    P.off[i++] = L.add(sizeof(int) * std::max<size_t>((size_t)P.n_dyn, 1));   // 52 ovf_list
+    P.off[i++] = L.add(4 * sizeof(int));                                       // 53 ovf_ctr
+    P.off[i++] = L.add(sizeof(int2) * (size_t)P.drop_cap);                     // 54 drop
+    P.off[i++] = L.add(sizeof(float4) * (size_t)P.drop_cap);                   // 55 drop_w
+    P.off[i++] = L.add(sizeof(int) * N);                                       // 56 fix_cnt
+    P.off[i++] = L.add(sizeof(int) * (N + 1));                                 // 57 fix_off
+    P.off[i++] = L.add(sizeof(int) * (size_t)P.fix_scan_blocks);               // 58 fix_bsums
+    P.off[i++] = L.add(2 * sizeof(float4) * (size_t)P.drop_cap);               // 59 fix_w
+    P.off[i++] = L.add(sizeof(int) * S);                                       // 60 fix_fail
+    P.off[i++] = L.add(sizeof(int) * S);                                       // 61 fix_scene
 }
 
 cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
@@ -757,6 +832,7 @@ int enqueue_stats(ivp_engine* e, int scene, cudaStream_t s) {
     CK(cudaMemcpyAsync(e->h_overflow + scene, e->D.overflow + scene, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(e->h_flags, e->D.flags, sizeof(Flags), cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(e->h_pairs + scene, e->D.pairs + scene, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(e->h_fix_scene + scene, e->D.fix_scene + scene, sizeof(int), cudaMemcpyDeviceToHost, s));
     return IVP_OK;
 }
 
@@ -788,6 +864,11 @@ int fill_stats(ivp_engine* e, int scene, ivp_solve_stats* out) {
     out->neighbour_pairs = (int64_t)e->h_pairs[scene];
     out->sum_visc_iters = C.acc_visc;
     out->sum_st_iters = C.acc_st;
+    out->last_pap = C.pap;
+    out->last_cg_iter = C.cg_it;
+    out->fixup_entries = e->h_fix_scene[scene];
+    if (C.status == IVP_ERR_NBR_OVERFLOW)
+        g_err = "truncated neighbour lists dropped more pairs than the engine's correction storage holds";
     if (e->h_flags->timeout) {
         g_err = "a solve exceeded its iteration budget or a grid barrier timed out";
         out->status = IVP_ERR_TIMEOUT;
@@ -937,6 +1018,18 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
     D.live_segs = reinterpret_cast<int*>(w + P.off[i++]);
     D.seg_ctr = reinterpret_cast<int*>(w + P.off[i++]);
     D.e = reinterpret_cast<float4*>(w + P.off[i++]);
+    D.ovf_list = reinterpret_cast<int*>(w + P.off[i++]);
+    D.ovf_ctr = reinterpret_cast<int*>(w + P.off[i++]);
+    D.drop = reinterpret_cast<int2*>(w + P.off[i++]);
+    D.drop_w = reinterpret_cast<float4*>(w + P.off[i++]);
+    D.fix_cnt = reinterpret_cast<int*>(w + P.off[i++]);
+    D.fix_off = reinterpret_cast<int*>(w + P.off[i++]);
+    D.fix_bsums = reinterpret_cast<int*>(w + P.off[i++]);
+    D.fix_w = reinterpret_cast<float4*>(w + P.off[i++]);
+    D.fix_fail = reinterpret_cast<int*>(w + P.off[i++]);
+    D.fix_scene = reinterpret_cast<int*>(w + P.off[i++]);
+    D.drop_cap = P.drop_cap;
+    e->fix_scan_blocks = P.fix_scan_blocks;
     D.n_segs = (int)P.segs.size();
     e->n_segs = D.n_segs;
     {
@@ -946,6 +1039,7 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
                    2 * 1000 + 4;
         D.phase_limit = lim;
     }
+    D.bar_limit_ns = kBarrierLimitNs;
     D.n_scenes = n_scenes;
     D.n_tiles = e->n_tiles;
     D.n_keys = e->n_keys;
@@ -974,7 +1068,9 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
         cudaHostAlloc((void**)&e->h_overflow, sizeof(int) * n_scenes, cudaHostAllocDefault) != cudaSuccess ||
         cudaHostAlloc((void**)&e->h_pairs, sizeof(unsigned long long) * n_scenes, cudaHostAllocDefault) != cudaSuccess ||
         cudaHostAlloc((void**)&e->h_err, sizeof(double) * opt->max_hist, cudaHostAllocDefault) != cudaSuccess ||
-        cudaHostAlloc((void**)&e->h_pcg, sizeof(int) * opt->max_hist, cudaHostAllocDefault) != cudaSuccess)
+        cudaHostAlloc((void**)&e->h_pcg, sizeof(int) * opt->max_hist, cudaHostAllocDefault) != cudaSuccess ||
+        cudaHostAlloc((void**)&e->h_ovf, sizeof(int), cudaHostAllocDefault) != cudaSuccess ||
+        cudaHostAlloc((void**)&e->h_fix_scene, sizeof(int) * n_scenes, cudaHostAllocDefault) != cudaSuccess)
         return fail(IVP_ERR_CUDA);
     if (cudaMemcpyAsync((void*)D.scenes, P.hp.data(), sizeof(SceneParams) * n_scenes, cudaMemcpyHostToDevice, s) !=
             cudaSuccess ||
@@ -1029,6 +1125,8 @@ int ivp_engine_destroy(ivp_engine* e) {
     if (e->h_pairs) cudaFreeHost(e->h_pairs);
     if (e->h_err) cudaFreeHost(e->h_err);
     if (e->h_pcg) cudaFreeHost(e->h_pcg);
+    if (e->h_ovf) cudaFreeHost(e->h_ovf);
+    if (e->h_fix_scene) cudaFreeHost(e->h_fix_scene);
     delete e;
     return IVP_OK;
 }
@@ -1173,6 +1271,29 @@ int ivp_read_stats(ivp_engine* e, int32_t scene, void* stream, ivp_solve_stats* 
     return fill_stats(e, scene, out);
 }
 
+int ivp_prepare(ivp_engine* e) {
+    if (!e) return IVP_ERR_BAD_ARG;
+    if (!e->bound) return IVP_ERR_NOT_BOUND;
+    if (!e->opt.use_graphs) return IVP_OK;
+    if (!e->exec_build) CKS(make_graph(e, emit_build, &e->graph_build, &e->exec_build));
+    if (!e->exec_step) CKS(make_graph(e, emit_step, &e->graph_step, &e->exec_step));
+    return IVP_OK;
+}
+
+int ivp_read_stats_all(ivp_engine* e, void* stream, ivp_solve_stats* out) {
+    if (!e || !out) return IVP_ERR_BAD_ARG;
+    cudaStream_t s = as_stream(stream);
+    const int ns = e->n_scenes;
+    CK(cudaMemcpyAsync(e->h_ctl, e->D.ctl, sizeof(SceneCtl) * ns, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(e->h_overflow, e->D.overflow, sizeof(int) * ns, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(e->h_flags, e->D.flags, sizeof(Flags), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(e->h_pairs, e->D.pairs, sizeof(unsigned long long) * ns, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(e->h_fix_scene, e->D.fix_scene, sizeof(int) * ns, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (int k = 0; k < ns; ++k) CKS(fill_stats(e, k, out + k));
+    return IVP_OK;
+}
+
 int ivp_read_history(ivp_engine* e, int32_t scene, void* stream, double* errors, int32_t* pcg_iters, int32_t cap,
                      int32_t* n_errors, int32_t* n_pcg) {
     if (!e || scene < 0 || scene >= e->n_scenes || cap < 0) return IVP_ERR_BAD_ARG;
@@ -1203,6 +1324,16 @@ int ivp_export_neighbours(ivp_engine* e, int32_t scene, int32_t* count, int32_t*
     k_export<<<blocks_for(nd, 128), 128, 0, s>>>(e->D, scene, count, ids, cache);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s));
+    return IVP_OK;
+}
+
+int ivp_set_wait_limit(ivp_engine* e, int64_t ns) {
+    if (!e) return IVP_ERR_BAD_ARG;
+    const unsigned long long v = ns > 0 ? (unsigned long long)ns : kBarrierLimitNs;
+    if (v != e->D.bar_limit_ns) {
+        destroy_graphs(e);  // the graphs hold the previous value in their kernel parameters
+        e->D.bar_limit_ns = v;
+    }
     return IVP_OK;
 }
 
@@ -1244,7 +1375,7 @@ const char* ivp_status_string(int32_t status) {
         case IVP_OK: return "ok";
         case IVP_ERR_NOT_SPD: return "non-positive definite matrix (pAp < 0)";
         case IVP_ERR_NOT_CONVERGED: return "outer iteration did not converge";
-        case IVP_ERR_NBR_OVERFLOW: return "neighbour cache overflow";
+        case IVP_ERR_NBR_OVERFLOW: return "neighbour cache overflow: more dropped pairs than the correction storage holds";
         case IVP_ERR_BAD_ARG: return "bad argument";
         case IVP_ERR_CUDA: return "CUDA error";
         case IVP_ERR_TIMEOUT: return "timeout";

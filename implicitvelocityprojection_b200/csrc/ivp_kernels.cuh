@@ -14,6 +14,7 @@
 // one or two scenes, else the last CTA to arrive).
 #pragma once
 #include "ivp_device.cuh"
+#include "ivp_scan.cuh"
 
 namespace ivp {
 
@@ -28,7 +29,7 @@ enum Kind {
 constexpr int FORCE_VISC = 0, FORCE_ST = 1;
 constexpr int MODE_IP = 0, MODE_FORCE = 1, MODE_PRJ = 3;
 
-constexpr int IVP_OK_ = 0, IVP_NOT_SPD_ = 1, IVP_NOT_CONVERGED_ = 2, IVP_TIMEOUT_ = 6;
+constexpr int IVP_OK_ = 0, IVP_NOT_SPD_ = 1, IVP_NOT_CONVERGED_ = 2, IVP_NBR_OVERFLOW_ = 3, IVP_TIMEOUT_ = 6;
 
 __device__ __forceinline__ void set_cond(unsigned long long h, unsigned v) {
     if (h) cudaGraphSetConditional((cudaGraphConditionalHandle)h, v);
@@ -272,6 +273,18 @@ __device__ __forceinline__ void ctl_begin(const SceneParams& P, SceneCtl& C, int
     C.total_cg = 0;
 }
 
+// ctl_begin of an IP scene; a scene whose truncated lists need more
+// corrections than the workspace holds stops at once with
+// IVP_ERR_NBR_OVERFLOW instead of solving with a wrong operator.
+__device__ __forceinline__ void ip_ctl_begin(const Dev& D, int s) {
+    SceneCtl& C = D.ctl[s];
+    ctl_begin(D.scenes[s], C);
+    if (C.outer_active && D.fix_fail[s]) {
+        C.status = IVP_NBR_OVERFLOW_;
+        C.outer_active = 0;
+    }
+}
+
 // Launch-level decision (one thread of the last CTA of the launch).
 __device__ void launch_finalize(const Dev& D, int kind) {
     volatile Flags* F = D.flags;
@@ -376,76 +389,6 @@ __global__ void k_keys(const Dev D) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= D.n_total) return;
     cell_key(D, p, D.pscene[p], D.x[3 * p], D.x[3 * p + 1], D.x[3 * p + 2]);
-}
-
-// Exclusive scan, pass 1: per-block scan of 4 elements per thread.
-constexpr int SCAN_BLOCK = 1024;
-constexpr int SCAN_ITEMS = 4;
-constexpr int SCAN_TILE = SCAN_BLOCK * SCAN_ITEMS;
-
-__global__ void __launch_bounds__(SCAN_BLOCK) k_scan_local(const int* __restrict__ in, int* __restrict__ out,
-                                                          int* __restrict__ block_sums, int n) {
-    __shared__ int warp_tot[SCAN_BLOCK / 32];
-    const int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
-    int v[SCAN_ITEMS];
-    int tsum = 0;
-#pragma unroll
-    for (int k = 0; k < SCAN_ITEMS; ++k) {
-        v[k] = (base + k < n) ? in[base + k] : 0;
-        tsum += v[k];
-    }
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    int incl = tsum;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        int t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += t;
-    }
-    if (lane == 31) warp_tot[w] = incl;
-    __syncthreads();
-    if (w == 0) {
-        int t = warp_tot[lane];
-        int ti = t;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            int u = __shfl_up_sync(0xffffffffu, ti, o);
-            if (lane >= o) ti += u;
-        }
-        warp_tot[lane] = ti - t;  // exclusive warp offsets
-        if (lane == 31) block_sums[blockIdx.x] = ti;
-    }
-    __syncthreads();
-    int run = warp_tot[w] + incl - tsum;
-#pragma unroll
-    for (int k = 0; k < SCAN_ITEMS; ++k) {
-        if (base + k < n) out[base + k] = run;
-        run += v[k];
-    }
-}
-
-// Exclusive scan, pass 2: add the sum of the preceding blocks; block 0 also
-// writes the total at out[n].
-__global__ void __launch_bounds__(SCAN_BLOCK) k_scan_add(int* __restrict__ out, const int* __restrict__ block_sums,
-                                                        int n, int n_blocks) {
-    __shared__ int sh_off;
-    __shared__ int warp_tot[SCAN_BLOCK / 32];
-    int acc = 0;
-    for (int b = threadIdx.x; b < (int)blockIdx.x; b += SCAN_BLOCK) acc += block_sums[b];
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if ((threadIdx.x & 31) == 0) warp_tot[threadIdx.x >> 5] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int t = 0;
-        for (int w = 0; w < SCAN_BLOCK / 32; ++w) t += warp_tot[w];
-        sh_off = t;
-        if (blockIdx.x == n_blocks - 1) out[n] = t + block_sums[blockIdx.x];
-    }
-    __syncthreads();
-    const int off = sh_off;
-    if (off == 0) return;
-    const int base = blockIdx.x * SCAN_TILE;
-    for (int k = threadIdx.x; k < SCAN_TILE; k += SCAN_BLOCK)
-        if (base + k < n) out[base + k] += off;
 }
 
 // Build segments: kSegW cells along x of one (y, z) cell row of a scene.
@@ -769,7 +712,13 @@ __global__ void __launch_bounds__(256, 4) k_nbr_build(const Dev D) {
             D.rflu[i] = D.material[pid] == 1 ? __frcp_rn(dens) : 0.0f;
             D.density_out[pid] = dens;
             D.k_out[pid] = kd;
-            if (found > cap) atomicAdd(&D.overflow[sc], 1);
+            if (found > cap) {
+                // truncated list: the fix-up rebuilds the row in the
+                // reference's candidate order and adds transpose corrections
+                atomicAdd(&D.overflow[sc], 1);
+                D.ovf_list[atomicAdd(&D.ovf_ctr[0], 1)] = i;
+                set_cond(D.h_fix, 1u);
+            }
             my_pairs += n_hit;
         }
         __syncwarp();
@@ -779,6 +728,226 @@ __global__ void __launch_bounds__(256, 4) k_nbr_build(const Dev D) {
     if (lane == 0 && my_pairs) atomicAdd(&sh_pairs, my_pairs);
     __syncthreads();
     if (threadIdx.x == 0 && sh_pairs) atomicAdd(&D.pairs[sc], (unsigned long long)sh_pairs);
+}
+
+// ---- neighbour-cache overflow: rows of truncated lists and the transpose
+// corrections (only when some dynamic particle has more than cache_size
+// neighbours; a graph conditional runs these kernels in that build only)
+
+constexpr int kOvfHits = 256;  // hits one warp ranks per truncated particle
+
+// Rows of the truncated particles in the reference's candidate order.  The
+// reference walks the 3x3x3 cells around x_i with z outermost and x
+// innermost, each cell in increasing particle index (Warp's hash grid,
+// neighbour_search.py:38-51, with cells of size h from the domain origin),
+// and keeps the first cache_size hits: the hits with the smallest
+// (linear cell index, particle index) keys.  One warp per truncated
+// particle re-scans its window, ranks every hit by that key, writes the
+// first cache_size in key order and recomputes density, Aii, k, c and 1/rho
+// over them exactly as the build does.  Dropped dynamic neighbours are
+// recorded for the corrections.
+__global__ void __launch_bounds__(256) k_ovf_rows(const Dev D) {
+    __shared__ unsigned long long hk[8][kOvfHits];
+    __shared__ int hj[8][kOvfHits];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int n_ovf = D.ovf_ctr[0];
+    for (int o = blockIdx.x * 8 + w; o < n_ovf; o += gridDim.x * 8) {
+        const int i = D.ovf_list[o];
+        const int sc = D.pscene[D.pid[i]];
+        const SceneParams& P = D.scenes[sc];
+        const float4 xi4 = D.xm[i];
+        const float3 xi = f3(xi4);
+        const int dimx = P.dims[0];
+        const int cx = cell_coord(xi.x, P.cell_inv, dimx);
+        const int cy = cell_coord(xi.y, P.cell_inv, P.dims[1]);
+        const int cz = cell_coord(xi.z, P.cell_inv, P.dims[2]);
+        const int x0 = cx > 0 ? cx - 1 : 0, x1 = cx < dimx - 1 ? cx + 1 : dimx - 1;
+        int H = 0;
+        for (int dz = -1; dz <= 1; ++dz) {
+            const int z = cz + dz;
+            if (z < 0 || z >= P.dims[2]) continue;
+            for (int dy = -1; dy <= 1; ++dy) {
+                const int y = cy + dy;
+                if (y < 0 || y >= P.dims[1]) continue;
+                const int cb = (z * P.dims[1] + y) * dimx;
+                for (int pass = 0; pass < 2; ++pass) {
+                    const int kb = P.key_base + (pass ? P.ncell : 0) + cb;
+                    const int jb = D.cell_start[kb + x0], je = D.cell_start[kb + x1 + 1];
+                    const int s1 = x0 + 1 <= x1 ? D.cell_start[kb + x0 + 1] : je;
+                    const int s2 = x0 + 2 <= x1 ? D.cell_start[kb + x0 + 2] : je;
+                    for (int base = jb; base < je; base += 32) {
+                        const int j = base + lane;
+                        bool hit = false;
+                        unsigned long long key = 0ull;
+                        if (j < je && j != i) {
+                            hit = norm2_rn(sub3(xi, f3(D.xm[j]))) <= P.r2_max;
+                            if (hit) {
+                                const int c = j >= s2 ? x0 + 2 : (j >= s1 ? x0 + 1 : x0);
+                                key = ((unsigned long long)(unsigned)(cb + c) << 32) | (unsigned)D.pid[j];
+                            }
+                        }
+                        const unsigned ball = __ballot_sync(0xffffffffu, hit);
+                        const int pos = H + __popc(ball & lt);
+                        if (hit && pos < kOvfHits) {
+                            hk[w][pos] = key;
+                            hj[w][pos] = j;
+                        }
+                        H += __popc(ball);
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        if (H > kOvfHits) {
+            // more hits than one warp ranks: stop the scene's IP solve loudly
+            if (lane == 0) D.fix_fail[sc] = 1;
+            continue;
+        }
+        const int cap = min(min(P.cache, D.stride), 64);
+        const int row = P.row_base + (i - P.s_begin);
+        float4* out = D.nbr + (size_t)row * D.stride;
+        float2* out2 = reinterpret_cast<float2*>(D.nbr) + (size_t)row * D.stride;
+        float rho = 0.0f, aii = 0.0f;
+        float3 jii = make_float3(0.0f, 0.0f, 0.0f);
+        for (int h = lane; h < H; h += 32) {
+            const unsigned long long kh = hk[w][h];
+            int r = 0;
+            for (int q = 0; q < H; ++q) r += hk[w][q] < kh ? 1 : 0;
+            const int j = hj[w][h];
+            if (r >= cap) {
+                if (j < P.s_dyn_end) {
+                    const int d = atomicAdd(&D.ovf_ctr[1], 1);
+                    if (d < D.drop_cap) D.drop[d] = make_int2(i, j);
+                    else D.fix_fail[sc] = 1;
+                }
+                continue;
+            }
+            // the build's dense-pass arithmetic for entry r
+            const float4 xj4 = D.xm[j];
+            const float3 rv = sub3(xi, f3(xj4));
+            const float rn = sqrtf(norm2_rn(rv));
+            const float rc = rn < 1e-6f ? 1e-6f : rn;
+            const float t = P.h - rc;
+            const float sg = -P.spiky_k * (t * t);
+            const float ir = __frcp_rn(rc);
+            const float mj = xj4.w;
+            const float wgt = mj * (sg * ir);
+            const float3 J = make_float3(__fmul_rn(wgt, rv.x), __fmul_rn(wgt, rv.y), __fmul_rn(wgt, rv.z));
+            if (D.row_fmt == ROW_FULL) {
+                out[r] = make_float4(J.x, J.y, J.z, __int_as_float(j));
+            } else if (D.row_fmt == ROW_COMPACT) {
+                out2[r] = make_float2(__int_as_float(j), wgt);
+            } else {
+                const size_t e = (size_t)row * D.stride + r;
+                reinterpret_cast<int*>(D.nbr)[e] = j;
+                unsigned short* gb = D.nbr_g + 3 * e;
+                gb[0] = bf16_bits(J.x);
+                gb[1] = bf16_bits(J.y);
+                gb[2] = bf16_bits(J.z);
+            }
+            rho += mj * cubic_Wq(rn * P.inv_h, P.cubic_k);
+            if (j < P.s_dyn_end) aii += dot3(J, J) * __frcp_rn(mj);
+            jii = sub3(jii, J);
+        }
+#pragma unroll
+        for (int q = 16; q > 0; q >>= 1) {
+            rho += __shfl_xor_sync(0xffffffffu, rho, q);
+            aii += __shfl_xor_sync(0xffffffffu, aii, q);
+            jii.x += __shfl_xor_sync(0xffffffffu, jii.x, q);
+            jii.y += __shfl_xor_sync(0xffffffffu, jii.y, q);
+            jii.z += __shfl_xor_sync(0xffffffffu, jii.z, q);
+        }
+        if (lane == 0) {
+            const float mi = xi4.w;
+            float dens = 0.0f;
+            dens = dens + mi * P.W0;
+            dens += rho;
+            aii += dot3(jii, jii) * __frcp_rn(mi);
+            const float kd = __frcp_rn(aii + 1e-3f);
+            D.nbr_cnt[row] = cap;
+            D.dens[i] = dens;
+            D.kd[i] = kd;
+            D.c[i] = dens - D.rho0s[i];
+            const int pid = D.pid[i];
+            D.rflu[i] = D.material[pid] == 1 ? __frcp_rn(dens) : 0.0f;
+            D.density_out[pid] = dens;
+            D.k_out[pid] = kd;
+        }
+        __syncwarp();
+    }
+}
+
+// Each dropped pair (o, k): k is within h of o but not in o's row.  When o
+// is in k's row, the pair appears in one row only: k's gather-form phase B
+// counts a transpose term the reference does not (k is not in o's row), and
+// o's misses the reference's term from k's row.  Both get a correction;
+// counted per target slot here, placed by k_ovf_fill.
+__global__ void k_ovf_pairs(const Dev D) {
+    const int n = min(D.ovf_ctr[1], D.drop_cap);
+    for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < n; d += gridDim.x * blockDim.x) {
+        const int2 pr = D.drop[d];
+        const int o = pr.x, k = pr.y;
+        const int sc = D.pscene[D.pid[k]];
+        const SceneParams& P = D.scenes[sc];
+        const int rowk = P.row_base + (k - P.s_begin);
+        const int cnt = D.nbr_cnt[rowk];
+        int q = -1;
+        for (int e = 0; e < cnt; ++e)
+            if (row_j(D, rowk, e) == o) {
+                q = e;
+                break;
+            }
+        if (q < 0) {
+            D.drop_w[d] = make_float4(0.f, 0.f, 0.f, 0.f);  // in neither row: nothing to correct
+            continue;
+        }
+        int jj;
+        const float3 J = row_J(D, rowk, q, f3(D.xm[k]), &jj);
+        D.drop_w[d] = make_float4(J.x, J.y, J.z, 1.0f);
+        atomicAdd(&D.fix_cnt[o], 1);
+        atomicAdd(&D.fix_cnt[k], 1);
+        atomicAdd(&D.fix_scene[sc], 2);
+    }
+}
+
+// Places the corrections by target slot (fix_off from the scan of fix_cnt,
+// which this pass counts back down to zero for the next build):
+//   target o, source k: the reference's term -omega y_k J_ko, which o's
+//     gather misses (w = J_ko);
+//   target k, source o: the gather's term omega m_k (y_o / m_o) J_ko, which
+//     the reference does not have (w = (m_k / m_o) J_ko, subtracted).
+__global__ void k_ovf_fill(const Dev D) {
+    const int n = min(D.ovf_ctr[1], D.drop_cap);
+    for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < n; d += gridDim.x * blockDim.x) {
+        const float4 w = D.drop_w[d];
+        if (w.w == 0.0f) continue;
+        const int2 pr = D.drop[d];
+        const int o = pr.x, k = pr.y;
+        const int po = D.fix_off[o] + atomicSub(&D.fix_cnt[o], 1) - 1;
+        D.fix_w[po] = make_float4(w.x, w.y, w.z, __int_as_float(k));
+        const float s = D.xm[k].w * D.inv_m[o];
+        const int pk = D.fix_off[k] + atomicSub(&D.fix_cnt[k], 1) - 1;
+        D.fix_w[pk] = make_float4(s * w.x, s * w.y, s * w.z, __int_as_float(o));
+    }
+}
+
+// Corrections of each target in increasing source slot, so phase B adds them
+// in a fixed order (deterministic results).
+__global__ void k_ovf_sort(const Dev D) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= D.n_total) return;
+    const int b = D.fix_off[t], e = D.fix_off[t + 1];
+    for (int a = b + 1; a < e; ++a) {
+        const float4 v = D.fix_w[a];
+        const int key = __float_as_int(v.w);
+        int c = a - 1;
+        while (c >= b && __float_as_int(D.fix_w[c].w) > key) {
+            D.fix_w[c + 1] = D.fix_w[c];
+            --c;
+        }
+        D.fix_w[c + 1] = v;
+    }
 }
 
 // Static particles: the reference zeroes their k (pressure_base.py:65-67) and
@@ -878,7 +1047,7 @@ __global__ void k_solve_begin(const Dev D) {
     const int4 tile = D.tiles[blockIdx.x];
     const SceneParams& P = D.scenes[tile.x];
     if (blockIdx.x == 0 && threadIdx.x == 0) guard_begin(D);
-    if (blockIdx.x == P.tile_begin && threadIdx.x == 0) ctl_begin(P, D.ctl[tile.x]);
+    if (blockIdx.x == P.tile_begin && threadIdx.x == 0) ip_ctl_begin(D, tile.x);
     if (P.solver != SOLVER_IP) return;
     const int i = tile.y + threadIdx.x;
     if (i >= tile.z) return;
@@ -979,8 +1148,14 @@ __global__ void k_advect_keys(const Dev D) {
     if (p < D.n_scenes) {
         D.overflow[p] = 0;
         D.pairs[p] = 0ull;
+        D.fix_fail[p] = 0;
+        D.fix_scene[p] = 0;
     }
-    if (p == 0) D.seg_ctr[0] = 0;
+    if (p == 0) {
+        D.seg_ctr[0] = 0;
+        D.ovf_ctr[0] = 0;
+        D.ovf_ctr[1] = 0;
+    }
     if (p >= D.n_total) return;
     const int sc = D.pscene[p];
     float pos[3];
@@ -1273,6 +1448,23 @@ __device__ __forceinline__ double cga_tile(const Dev& D, const SceneParams& P, c
     return part;
 }
 
+// Sum of y_source w over slot i's transpose corrections (k_ovf_fill), in
+// increasing source slot.  Kept out of line: it runs only in scenes with a
+// truncated list and must not take registers from the pair loop.
+__device__ __noinline__ float3 ovf_correction(const int* __restrict__ fix_off, const float4* __restrict__ fix_w,
+                                               const float* __restrict__ y, int i) {
+    float3 c = make_float3(0.0f, 0.0f, 0.0f);
+    const int fb = fix_off[i], fe = fix_off[i + 1];
+    for (int f = fb; f < fe; ++f) {
+        const float4 w = fix_w[f];
+        const float ys = y[__float_as_int(w.w)];
+        c.x += ys * w.x;
+        c.y += ys * w.y;
+        c.z += ys * w.z;
+    }
+    return c;
+}
+
 // CG phase B: Ap = m p + omega J^T y in gather form (compute_Ax_part1/2,
 // ip.py:63-121, as pressure_base.py:130-166 writes J^T), x += alpha p,
 // r -= alpha Ap (pcg_update_x_r_scalar, math_utils.py:181-195), rr = r.r.
@@ -1307,6 +1499,14 @@ __device__ __forceinline__ double cgb_tile(const Dev& D, const SceneParams& P, c
     az = group_sum<G>(az);
     double part = 0.0;
     if (T.valid && T.lane == 0) {
+        if (D.overflow[T.sc] > 0) {
+            // truncated lists: the transpose terms of pairs held in one row
+            // only (k_ovf_fill), in a fixed order
+            const float3 c = ovf_correction(D.fix_off, D.fix_w, D.y, T.i);
+            ax -= c.x;
+            ay -= c.y;
+            az -= c.z;
+        }
         const float om = P.omega;
         const float4 p4 = cn[2 * T.i + 1];
         const float3 ap = make_float3(mi * p4.x + om * ax, mi * p4.y + om * ay, mi * p4.z + om * az);
@@ -2134,9 +2334,10 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
 // (current: every CTA refreshes them after each barrier), writes them back and
 // only then releases the others.  Every CTA executes a gpu-scope fence after
 // the barrier, which orders its later plain loads (the L1-cached neighbour
-// gathers) after every write of the previous phase.  The wait is bounded: after kBarrierLimitNs a
-// CTA sets the timeout flag and reports failure, so a fault can never keep
-// the kernel spinning.
+// gathers) after every write of the previous phase.  The wait is bounded: after
+// D.bar_limit_ns (kBarrierLimitNs unless a test shortens it) a CTA sets the
+// timeout flag and reports failure, so a fault can never keep the kernel
+// spinning.
 constexpr unsigned long long kBarrierLimitNs = 2000000000ull;
 
 __device__ __forceinline__ bool phase_active(const SceneCtl& C, int kind) {
@@ -2232,7 +2433,7 @@ __device__ bool grid_all_reduce_barrier(const Dev& D, int kind, const double* pa
         const unsigned long long t0 = globaltimer_ns();
         while ((int)(*cnt - target) < 0) {
             __nanosleep(32);
-            if (globaltimer_ns() - t0 > kBarrierLimitNs) {
+            if (globaltimer_ns() - t0 > D.bar_limit_ns) {
                 ok = 0;
                 D.flags->timeout = 1;
                 break;
@@ -2275,7 +2476,7 @@ __device__ bool grid_reduce_barrier(const Dev& D, int kind, const double* partia
         const unsigned long long t0 = globaltimer_ns();
         while (*gen == g) {
             __nanosleep(32);
-            if (globaltimer_ns() - t0 > kBarrierLimitNs) {
+            if (globaltimer_ns() - t0 > D.bar_limit_ns) {
                 sh_flag[1] = 0;
                 D.flags->timeout = 1;
                 break;
@@ -2582,7 +2783,7 @@ __global__ void __launch_bounds__(BLOCK, persist_min_blocks<BLOCK>()) k_ip_persi
     // CTA 0 starts every scene's control block (reset_stats); the first
     // barrier publishes it
     if (blockIdx.x == 0 && threadIdx.x == 0)
-        for (int s = 0; s < D.n_scenes; ++s) ctl_begin(D.scenes[s], D.ctl[s]);
+        for (int s = 0; s < D.n_scenes; ++s) ip_ctl_begin(D, s);
     // d = dt v (ip.py:343) for the owned particles
     for (int t = blockIdx.x; t < D.n_tiles; t += gridDim.x) {
         const int4 tile = __ldg(D.tiles + t);

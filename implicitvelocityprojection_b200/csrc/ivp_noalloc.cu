@@ -31,8 +31,16 @@
 #include <cmath>
 #include <mutex>
 
+#include <string>
+
 #include "../../include/ivp.h"
 #include "ivp_device.cuh"
+#include "ivp_scan.cuh"
+
+namespace ivp {
+// the engine's thread-local error text (ivp_last_error), set in ivp_engine.cu
+void set_last_error(const std::string& msg);
+}  // namespace ivp
 
 namespace {
 
@@ -51,6 +59,7 @@ constexpr int kMaxDevices = 64;
 struct Scratch {
     int cell_count[kMaxKeys];
     int cell_start[kMaxKeys + 64];
+    int block_sums[(kMaxKeys + ivp::SCAN_TILE - 1) / ivp::SCAN_TILE];
     int key[kMaxParticles];
     int rank[kMaxParticles];
     int placed[kMaxParticles];
@@ -80,43 +89,6 @@ __global__ void na_keys(const float* __restrict__ x, const int* __restrict__ dyn
     const int key = (dyn[p] ? 0 : g.ncell) + (cz * g.dims[1] + cy) * g.dims[0] + cx;
     S->key[p] = key;
     S->rank[p] = atomicAdd(&S->cell_count[key], 1);
-}
-
-// Exclusive scan of the cell counts in one CTA (the keys fit in the scratch
-// limit, so one CTA walking 1024-wide chunks is enough for a utility path).
-__global__ void __launch_bounds__(1024) na_scan(Scratch* S, int n_keys) {
-    __shared__ int warp_tot[32];
-    __shared__ int carry;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int base = 0; base < n_keys; base += 1024) {
-        const int i = base + threadIdx.x;
-        const int v = i < n_keys ? S->cell_count[i] : 0;
-        int incl = v;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += t;
-        }
-        if (lane == 31) warp_tot[w] = incl;
-        __syncthreads();
-        if (w == 0) {
-            const int t = warp_tot[lane];
-            int ti = t;
-            for (int o = 1; o < 32; o <<= 1) {
-                const int u = __shfl_up_sync(0xffffffffu, ti, o);
-                if (lane >= o) ti += u;
-            }
-            warp_tot[lane] = ti - t;
-        }
-        __syncthreads();
-        const int off = carry + warp_tot[w];
-        if (i < n_keys) S->cell_start[i] = off + incl - v;
-        __syncthreads();
-        if (threadIdx.x == 1023) carry = off + incl;
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) S->cell_start[n_keys] = carry;
 }
 
 __global__ void na_place(int n, Scratch* S) {
@@ -199,7 +171,22 @@ __global__ void na_density_aii(int n, Grid g, Scratch* S, float* __restrict__ de
     kdiag[p] = 1.0f / (aii + 1e-3f);
 }
 
-int fail(int code, const char*) { return code; }
+// Every failure leaves its reason where ivp_last_error() reads it.
+int fail(int code, const char* msg) {
+    ivp::set_last_error(msg);
+    return code;
+}
+
+// One launch; its own status (cudaLaunchKernel reports this launch's error,
+// not one left pending by earlier work of the caller).
+int launch(const void* fn, int grid, int block, void** args, cudaStream_t s, const char* what) {
+    const cudaError_t e = cudaLaunchKernel(fn, dim3(grid), dim3(block), args, 0, s);
+    if (e != cudaSuccess) {
+        cudaGetLastError();  // this launch's error is now the last error: clear it, it is reported here
+        return fail(IVP_ERR_CUDA, (std::string(what) + ": " + cudaGetErrorString(e)).c_str());
+    }
+    return IVP_OK;
+}
 
 }  // namespace
 
@@ -244,7 +231,11 @@ extern "C" int ivp_density_aii_noalloc(const float* x, const float* m, const int
         if (!g_scratch_addr[dev]) {
             void* addr = nullptr;
             cudaError_t e = cudaGetSymbolAddress(&addr, g_scratch);
-            if (e != cudaSuccess || !addr) return IVP_ERR_CUDA;
+            if (e != cudaSuccess || !addr) {
+                if (e != cudaSuccess) cudaGetLastError();  // reported here
+                return fail(IVP_ERR_CUDA, (std::string("ivp_density_aii_noalloc: cudaGetSymbolAddress: ") +
+                                           cudaGetErrorString(e)).c_str());
+            }
             g_scratch_addr[dev] = static_cast<Scratch*>(addr);
         }
         S = g_scratch_addr[dev];
@@ -252,13 +243,32 @@ extern "C" int ivp_density_aii_noalloc(const float* x, const float* m, const int
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const int n = n_particles, n_keys = 2 * g.ncell;
     const int B = 256, nb = (n + B - 1) / B;
-    if (cudaMemsetAsync(S->cell_count, 0, sizeof(int) * (size_t)n_keys, s) != cudaSuccess)
-        return fail(IVP_ERR_CUDA, "ivp_density_aii_noalloc: memset failed");
-    na_keys<<<nb, B, 0, s>>>(x, is_dynamic, n, g, S);
-    na_scan<<<1, 1024, 0, s>>>(S, n_keys);
-    na_place<<<nb, B, 0, s>>>(n, S);
-    na_order<<<nb, B, 0, s>>>(x, m, n, S);
-    na_density_aii<<<nb, B, 0, s>>>(n, g, S, density, kdiag);
-    if (cudaGetLastError() != cudaSuccess) return IVP_ERR_CUDA;
+    {
+        const cudaError_t e = cudaMemsetAsync(S->cell_count, 0, sizeof(int) * (size_t)n_keys, s);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(IVP_ERR_CUDA, (std::string("ivp_density_aii_noalloc: memset: ") + cudaGetErrorString(e)).c_str());
+        }
+    }
+    int* counts = S->cell_count;
+    int* starts = S->cell_start;
+    int* bsums = S->block_sums;
+    int nk = n_keys, nsb = (n_keys + ivp::SCAN_TILE - 1) / ivp::SCAN_TILE, nn = n;
+    const float* px = x;
+    const float* pm = m;
+    const int* pd = is_dynamic;
+    void* a_keys[] = {&px, &pd, &nn, &g, &S};
+    void* a_scan1[] = {&counts, &starts, &bsums, &nk};
+    void* a_scan2[] = {&starts, &bsums, &nk, &nsb};
+    void* a_place[] = {&nn, &S};
+    void* a_order[] = {&px, &pm, &nn, &S};
+    void* a_dens[] = {&nn, &g, &S, &density, &kdiag};
+    int st = launch((const void*)na_keys, nb, B, a_keys, s, "na_keys");
+    if (st == IVP_OK) st = launch((const void*)ivp::k_scan_local, nsb, ivp::SCAN_BLOCK, a_scan1, s, "scan_local");
+    if (st == IVP_OK) st = launch((const void*)ivp::k_scan_add, nsb, ivp::SCAN_BLOCK, a_scan2, s, "scan_add");
+    if (st == IVP_OK) st = launch((const void*)na_place, nb, B, a_place, s, "na_place");
+    if (st == IVP_OK) st = launch((const void*)na_order, nb, B, a_order, s, "na_order");
+    if (st == IVP_OK) st = launch((const void*)na_density_aii, nb, B, a_dens, s, "na_density_aii");
+    if (st != IVP_OK) return st;
     return IVP_OK;
 }

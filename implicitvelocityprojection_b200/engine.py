@@ -97,6 +97,8 @@ class Stats:
     stats_pcg_iters: list
     overflow_particles: int
     total_pcg_iters: int
+    last_pap: float = 0.0        # p^T A p of the last CG iteration (reported with NOT_SPD)
+    last_cg_iter: int = 0        # CG iterations completed in the last PCG call
 
 
 class Engine:
@@ -245,6 +247,11 @@ class Engine:
         """n Framework.forward() steps of every scene (asynchronous)."""
         check(self.L.ivp_step(self._handle, int(n), ctypes.c_void_p(_stream_ptr(stream))), "ivp_step")
 
+    def set_wait_limit(self, ns: int):
+        """Test hook: longest wait on a grid barrier of the persistent kernels
+        (ns <= 0 restores the default of 2 s)."""
+        check(self.L.ivp_set_wait_limit(self._handle, int(ns)), "ivp_set_wait_limit")
+
     def reset_counters(self, stream=None):
         check(self.L.ivp_reset_counters(self._handle, ctypes.c_void_p(_stream_ptr(stream))), "ivp_reset_counters")
 
@@ -257,6 +264,23 @@ class Engine:
                                       ms.ctypes.data_as(ctypes.c_void_p), cnt.ctypes.data_as(ctypes.c_void_p)),
               "ivp_profile_step")
         return {name: (float(ms[i]), int(cnt[i])) for i, name in enumerate(_lib.KERNEL_NAMES) if cnt[i] > 0}
+
+    def prepare(self):
+        """Instantiates the build and step graphs without launching them
+        (host work only), so the first build() and step() launch at once."""
+        check(self.L.ivp_prepare(self._handle), "ivp_prepare")
+
+    def raw_stats_all(self, stream=None) -> list:
+        """ivp_read_stats of every scene, one stream synchronisation."""
+        out = (_lib.SolveStats * len(self.scenes))()
+        check(self.L.ivp_read_stats_all(self._handle, ctypes.c_void_p(_stream_ptr(stream)), out),
+              "ivp_read_stats_all")
+        return list(out)
+
+    def step_chunk(self, n: int, stream=None) -> "Chunk":
+        """Launches n steps, each between two CUDA events, and returns at once
+        (the per-step device times are read from the returned Chunk)."""
+        return Chunk(self, n, stream)
 
     def raw_stats(self, scene: int = 0, stream=None) -> _lib.SolveStats:
         s = _lib.SolveStats()
@@ -279,7 +303,8 @@ class Engine:
                      stats_final_density_error=float(s.final_density_error),
                      stats_density_errors=[float(e) for e in err[:ne.value]],
                      stats_pcg_iters=[int(q) for q in pcg[:npc.value]],
-                     overflow_particles=int(s.overflow_particles), total_pcg_iters=int(s.total_pcg_iters))
+                     overflow_particles=int(s.overflow_particles), total_pcg_iters=int(s.total_pcg_iters),
+                     last_pap=float(s.last_pap), last_cg_iter=int(s.last_cg_iter))
 
     def neighbours(self, scene: int = 0, cache: Optional[int] = None, stream=None):
         """(count[n], ids[n, cache]) of a scene in the reference layout, local
@@ -300,3 +325,29 @@ class Engine:
 
     def get(self, name: str, scene: int = 0) -> np.ndarray:
         return self.arrays[name][self.scene_slice(scene)].cpu().numpy()
+
+
+class Chunk:
+    """n steps of an engine in flight on a stream, with a CUDA event pair
+    around each step: `done()` polls, `wait()` blocks, `step_ms()` gives the
+    device time of every step once done."""
+
+    def __init__(self, eng: Engine, n: int, stream=None):
+        s = stream if stream is not None else torch.cuda.current_stream()
+        self.n = int(n)
+        self.starts = [torch.cuda.Event(enable_timing=True) for _ in range(self.n)]
+        self.ends = [torch.cuda.Event(enable_timing=True) for _ in range(self.n)]
+        for k in range(self.n):
+            self.starts[k].record(s)
+            eng.step(1, stream=s)
+            self.ends[k].record(s)
+
+    def done(self) -> bool:
+        return self.n == 0 or self.ends[-1].query()
+
+    def wait(self):
+        if self.n:
+            self.ends[-1].synchronize()
+
+    def step_ms(self) -> list:
+        return [a.elapsed_time(b) for a, b in zip(self.starts, self.ends)]

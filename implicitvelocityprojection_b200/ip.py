@@ -37,11 +37,16 @@ class IP(PressureBase):
         n = max(len(self.stats_density_errors), 1)
         self.stats_iter_costs = [cost_ms / n] * len(self.stats_density_errors)
         if st.status == _lib.NOT_SPD:
-            raise RuntimeError(f"[IP] non-positive definite matrix at PCG iter {self.stats_pcg_iters[-1:] or [0]}")
+            # ip.py:308-309: the iteration count of the failing PCG call and p^T A p
+            raise RuntimeError(f"[IP] non-positive definite matrix at PCG iter {st.last_cg_iter} "
+                               f"(pAp={st.last_pap:.2e})")
         if st.status == _lib.NOT_CONVERGED:
             err = self.stats_density_errors[-1] if self.stats_density_errors else self.stats_final_density_error
             raise RuntimeError(f"[IP] does not converge! density err={err:.2e} (tol={self.tol_opt:.2e}) "
                                f"after {self.stats_outer_iters} iters")
+        if st.status == _lib.NBR_OVERFLOW:
+            raise RuntimeError("[IP] neighbour lists truncated at neighborCacheSize dropped more pairs than the "
+                               "engine's transpose-correction storage holds; raise neighborCacheSize")
         if st.status == _lib.TIMEOUT:
             raise RuntimeError("[IP] solve stopped by the device iteration guard")
         if st.status != _lib.OK:

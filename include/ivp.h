@@ -30,7 +30,10 @@ typedef enum {
     IVP_OK = 0,
     IVP_ERR_NOT_SPD = 1,        /* CG saw p^T A p < 0 */
     IVP_ERR_NOT_CONVERGED = 2,  /* outer-iteration cap reached above densityErrorTol */
-    IVP_ERR_NBR_OVERFLOW = 3,   /* a particle had more neighbours than neighborCacheSize (lists truncated, as the reference does) */
+    IVP_ERR_NBR_OVERFLOW = 3,   /* truncated neighbour lists (more neighbours than neighborCacheSize) dropped
+                                   more pairs than the engine's transpose-correction storage holds; lists
+                                   are truncated as the reference does (neighbour_search.py:38-51) and
+                                   solved with its exact transpose otherwise (ip.py:110-121) */
     IVP_ERR_BAD_ARG = 4,
     IVP_ERR_CUDA = 5,
     IVP_ERR_TIMEOUT = 6,
@@ -117,6 +120,11 @@ typedef struct {
     int64_t neighbour_pairs;      /* pairs in the scene's current neighbour lists */
     int64_t sum_visc_iters;       /* implicit-viscosity CG iterations */
     int64_t sum_st_iters;         /* implicit surface-tension CG iterations */
+    double last_pap;              /* p^T A p of the last CG iteration (the value the reference prints
+                                     with its non-positive-definite error, ip.py:308-309) */
+    int32_t last_cg_iter;         /* CG iterations completed in the last PCG call when it stopped */
+    int32_t fixup_entries;        /* transpose corrections of the scene's last build (non-zero only when
+                                     some list was truncated at cache_size) */
 } ivp_solve_stats;
 
 /* Pressure solvers (ivp_scene_desc.pressure_solver). */
@@ -229,6 +237,18 @@ int ivp_reset_counters(ivp_engine* e, void* stream);
  * (stats_total_cost_ms, pressure_base.py:331-339); no per-kernel counterpart. */
 int ivp_profile_step(ivp_engine* e, int32_t n_steps, void* stream, double* ms, int32_t* launches);
 
+/* Builds and instantiates the engine's neighbour-build and step graphs
+ * without launching them, so that the first ivp_neighbour_build / ivp_step
+ * of a new engine spends no host time on graph construction (the served form
+ * prepares the next batch's engine while the current one runs).  Host only;
+ * the particle arrays must be bound.  No counterpart in the reference. */
+int ivp_prepare(ivp_engine* e);
+
+/* ivp_read_stats of every scene (out[n_scenes]) with one stream
+ * synchronisation: the per-scene statistics attributes after a batched step
+ * (pressure_base.py:331-339). */
+int ivp_read_stats_all(ivp_engine* e, void* stream, ivp_solve_stats* out);
+
 /* Synchronises the stream and copies one scene's stats of the last solve:
  * the statistics attributes of IP / PressureBase (pressure_base.py:331-339). */
 int ivp_read_stats(ivp_engine* e, int32_t scene, void* stream, ivp_solve_stats* out);
@@ -250,6 +270,14 @@ int ivp_read_solve(ivp_engine* e, int32_t scene, void* stream, ivp_solve_stats* 
  * (neighbor_count[N], neighbor_ids[N*cache]) with original particle indices,
  * for parity checks.  Synchronous, device pointers. */
 int ivp_export_neighbours(ivp_engine* e, int32_t scene, int32_t* count, int32_t* ids, int32_t cache, void* stream);
+
+/* Test hook, no counterpart in the reference (whose launches never wait on
+ * one another).  Sets how long any wait of the engine's persistent kernels on
+ * a grid barrier may last before the kernel gives up, sets the timeout flag
+ * and returns (default 2 s; ns <= 0 restores it).  A solve cut short this way
+ * reports IVP_ERR_TIMEOUT until ivp_reset_counters clears the flag.  Host
+ * only: rebuilds the engine's graphs at their next launch. */
+int ivp_set_wait_limit(ivp_engine* e, int64_t ns);
 
 /* Limits of ivp_density_aii_noalloc. */
 #define IVP_NOALLOC_MAX_PARTICLES 65536

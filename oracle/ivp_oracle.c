@@ -96,32 +96,38 @@ void orc_spiky_grad(const float* r, float h, float* out) {
 
 /* ------------------------------------------------------- neighbour cache */
 
-static int cell_of(float v, float lo, float inv, int dim) {
-    int c = (int)floorf((v - lo) * inv);
+static int cell_of(float v, float inv, int dim) {
+    int c = (int)floorf(v * inv);
     return c < 0 ? 0 : (c >= dim ? dim - 1 : c);
 }
 
 /*
  * neighbour_search.py:10-51 (build_neighbor_cache) over a uniform grid of cell
- * size h.  Candidate order is cell (z, y, x ascending) then particle index;
- * the reference's order is Warp's hash-grid order, which only matters when a
- * particle has more than cache_size neighbours.  Lists are built for every
- * particle when only_dynamic == 0 (as the reference does) or for dynamic ones
- * only.  Returns the number of particles whose true count exceeded the cap.
+ * size h anchored at the domain origin (neighbour_search.py:105-107: ceil(L/h)
+ * cells per axis; cells of positions outside are clamped to the edge cells).
+ * Candidate order is cell (z outermost, x innermost) then particle index, the
+ * order in which Warp's hash grid query walks a scene whose domain starts at
+ * the origin; it decides which hits a list keeps when a particle has more
+ * than cache_size neighbours.  `domain` may be NULL (cells up to the largest
+ * coordinate).  Lists are built for every particle when only_dynamic == 0 (as
+ * the reference does) or for dynamic ones only.  Returns the number of
+ * particles whose true count exceeded the cap.
  */
 long orc_build_neighbor_cache(int n, const float* x, const int* is_dynamic, int only_dynamic,
-                              float h, int cache, int* count, int* ids, float* gradW) {
+                              float h, int cache, const float* domain, int* count, int* ids, float* gradW) {
     if (n <= 0) return 0;
-    float lo[3] = {x[0], x[1], x[2]}, hi[3] = {x[0], x[1], x[2]};
+    float hi[3] = {x[0], x[1], x[2]};
     for (int i = 1; i < n; ++i)
-        for (int c = 0; c < 3; ++c) {
-            if (x[3 * i + c] < lo[c]) lo[c] = x[3 * i + c];
+        for (int c = 0; c < 3; ++c)
             if (x[3 * i + c] > hi[c]) hi[c] = x[3 * i + c];
-        }
     int dim[3];
     float inv = 1.0f / h;
     for (int c = 0; c < 3; ++c) {
-        dim[c] = (int)floorf((hi[c] - lo[c]) * inv) + 1;
+        if (domain) {
+            dim[c] = (int)ceil((double)domain[c] / (double)h);
+        } else {
+            dim[c] = (int)floorf((hi[c] > 0.0f ? hi[c] : 0.0f) * inv) + 1;
+        }
         if (dim[c] < 1) dim[c] = 1;
     }
     long ncell = (long)dim[0] * dim[1] * dim[2];
@@ -129,9 +135,9 @@ long orc_build_neighbor_cache(int n, const float* x, const int* is_dynamic, int 
     int* cell = (int*)malloc(sizeof(int) * n);
     int* sorted = (int*)malloc(sizeof(int) * n);
     for (int i = 0; i < n; ++i) {
-        int cx = cell_of(x[3 * i], lo[0], inv, dim[0]);
-        int cy = cell_of(x[3 * i + 1], lo[1], inv, dim[1]);
-        int cz = cell_of(x[3 * i + 2], lo[2], inv, dim[2]);
+        int cx = cell_of(x[3 * i], inv, dim[0]);
+        int cy = cell_of(x[3 * i + 1], inv, dim[1]);
+        int cz = cell_of(x[3 * i + 2], inv, dim[2]);
         cell[i] = (int)(((long)cz * dim[1] + cy) * dim[0] + cx);
         cstart[cell[i] + 1]++;
     }
@@ -187,6 +193,15 @@ long orc_build_neighbor_cache(int n, const float* x, const int* is_dynamic, int 
 }
 
 static inline int clamp_cnt(int c, int cache) { return c > cache ? cache : c; }
+
+/* Does any dynamic list hold cache entries?  Only then can a list have been
+ * truncated, and only then may j in N(i) and i in N(j) disagree, so that the
+ * gather form of J^T differs from the reference's scatter form. */
+static int any_full_row(int n, const int* dyn, const int* count, int cache) {
+    for (int i = 0; i < n; ++i)
+        if (dyn[i] && count[i] >= cache) return 1;
+    return 0;
+}
 
 /* pressure_base.py:12-46 */
 void orc_compute_density(int n, const float* x, const float* m, const int* dyn, float h, int cache,
@@ -395,11 +410,14 @@ static int orc_pcg(int n, const orc_params* P, const float* m, const float* dfdt
     memcpy(r, b, sizeof(float) * 3 * (size_t)n);
     double rr_old = dot_dyn(n, r, r, dyn, P->fast);
     int it = 0;
+    /* FAST mode gathers J^T y, which equals the scatter form only while every
+     * pair is in both rows (no truncated list) */
+    const int gather = P->fast && !any_full_row(n, dyn, count, cache);
     if (rr_old > 1e-30) {
         memcpy(p, r, sizeof(float) * 3 * (size_t)n);
         for (;;) {
             jx_pcg(n, p, m, dfdt, kd, dyn, cache, count, ids, gradW, y);
-            if (P->fast)
+            if (gather)
                 ax_gather(n, p, y, m, P->omega, dyn, cache, count, ids, gradW, ap);
             else
                 ax_scatter(n, p, y, m, dfdt, P->omega, dyn, cache, count, ids, gradW, ap);
@@ -1085,7 +1103,7 @@ int orc_step(int n, const orc_params* P, float dt, const float* g, const float* 
                               NULL, NULL, st);
     }
     orc_advect_and_clamp(n, x, v, dyn, dt, domain, P->h);
-    long ov = orc_build_neighbor_cache(n, x, dyn, 1, P->h, P->cache_size, count, ids, gradW);
+    long ov = orc_build_neighbor_cache(n, x, dyn, 1, P->h, P->cache_size, domain, count, ids, gradW);
     if (overflow) *overflow = ov;
     orc_compute_density(n, x, m, dyn, P->h, P->cache_size, count, ids, density);
     orc_compute_aii(n, m, m_inv, dyn, P->cache_size, count, ids, gradW, kd);
@@ -1118,6 +1136,7 @@ int orc_cg_f64(int n, float omega, int cache, const float* m, const float* dfdt,
     }
     double rr = bb;
     int it = 0;
+    const int gather = !any_full_row(n, dyn, count, cache);
     while (it < max_iter && rr > rel_tol * rel_tol * bb && rr > 0.0) {
 #pragma omp parallel for schedule(static)
         for (int i = 0; i < n; ++i) {
@@ -1148,6 +1167,24 @@ int orc_cg_f64(int n, float omega, int cache, const float* m, const float* dfdt,
                 for (int c = 0; c < 3; ++c) acc[c] += w * (double)gradW[3 * b + c];
             }
             for (int c = 0; c < 3; ++c) ap[3 * i + c] = (double)m[i] * p[3 * i + c] + (double)omega * acc[c];
+        }
+        if (!gather) {
+            /* a truncated list: J^T y in the reference's scatter form */
+            for (int i = 0; i < n; ++i)
+                for (int c = 0; c < 3; ++c) ap[3 * i + c] = dyn[i] ? (double)m[i] * p[3 * i + c] : 0.0;
+            for (int i = 0; i < n; ++i) {
+                if (!dyn[i] || y[i] == 0.0) continue;
+                int cnt = clamp_cnt(count[i], cache);
+                for (int k = 0; k < cnt; ++k) {
+                    long b = (long)i * cache + k;
+                    int j = ids[b];
+                    for (int c = 0; c < 3; ++c) {
+                        double contrib = (double)omega * y[i] * (double)m[j] * (double)gradW[3 * b + c];
+                        ap[3 * i + c] += contrib;
+                        if (dyn[j]) ap[3 * j + c] -= contrib;
+                    }
+                }
+            }
         }
         double pap = 0.0;
         for (size_t q = 0; q < n3; ++q) pap += p[q] * ap[q];

@@ -88,7 +88,7 @@ def lib():
         L.orc_cubic_kernel.argtypes = [f, f]
         L.orc_cubic_kernel.restype = f
         L.orc_spiky_grad.argtypes = [P, f, P]
-        L.orc_build_neighbor_cache.argtypes = [i, P, P, i, f, i, P, P, P]
+        L.orc_build_neighbor_cache.argtypes = [i, P, P, i, f, i, P, P, P, P]
         L.orc_build_neighbor_cache.restype = l
         L.orc_compute_density.argtypes = [i, P, P, P, f, i, P, P, P]
         L.orc_compute_aii.argtypes = [i, P, P, P, i, P, P, P, P]
@@ -228,7 +228,8 @@ class State:
             self.k = np.zeros(n, np.float32)
         L = lib()
         self.overflow = int(L.orc_build_neighbor_cache(n, _p(self.x), _p(self.is_dynamic), int(only_dynamic),
-                                                       self.h, c, _p(self.count), _p(self.ids), _p(self.gradW)))
+                                                       self.h, c, _p(_f32(self.domain_size)), _p(self.count),
+                                                       _p(self.ids), _p(self.gradW)))
         L.orc_compute_density(n, _p(self.x), _p(self.m), _p(self.is_dynamic), self.h, c, _p(self.count),
                               _p(self.ids), _p(self.density))
         L.orc_compute_aii(n, _p(self.m), _p(self.m_inv), _p(self.is_dynamic), c, _p(self.count), _p(self.ids),

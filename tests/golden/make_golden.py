@@ -4,10 +4,10 @@ Runs the reference's Python modules (`scripts/framework.py`,
 `scripts/sim/forces/pressure/ip.py`, `pressure_base.py`, `neighbour_search.py`,
 `sph_kernel.py`, `math_utils.py`, `simulation_data.py`, `boundary.py`) on the
 NumPy FP32 stand-in for the Warp runtime in `wpshim/`, and stores the results
-as small `.npz` fixtures next to this script.  It needs the reference checkout
-(default `/root/reference`, or `--reference PATH`) and only runs where that
-checkout exists; the fixtures it writes are committed and are all that the
-tests read.
+as small `.npz` fixtures next to this script.  It needs a checkout of the
+reference, given as `--reference PATH` or in the environment variable
+IVP_REFERENCE, and only runs where that checkout exists; the fixtures it
+writes are committed and are all that the tests read.
 
 Fixtures
 --------
@@ -23,6 +23,9 @@ st_solve.npz      one Jeske23 implicit surface-tension solve (jeske23.py:585-655
 column_st_steps.npz  Framework.forward() steps with Jeske23 surface tension and
                   Weiler18 viscosity on (surface tension runs first,
                   framework.py:417-421);
+overflow_solve.npz  the reference's neighbour build, density, Aii and one IP
+                  solve (two fixed outer updates) on a block compressed to
+                  0.7 d, whose inner lists are truncated at neighborCacheSize;
 block_solve.npz   one IP solve (ip.py:331-404) from a compressed, moving block
                   inside a static box, after the reference's neighbour build,
                   density and Aii;
@@ -31,7 +34,7 @@ column_steps.npz  successive Framework.forward() steps (framework.py:423-544)
                   surface tension (their solver objects are replaced by no-ops,
                   which is what "off" means for these configurations).
 
-Usage:  python tests/golden/make_golden.py [--reference PATH] [--steps N]
+Usage:  python tests/golden/make_golden.py --reference PATH [--steps N]
 """
 from __future__ import annotations
 
@@ -148,6 +151,61 @@ def make_block_solve(out):
         nbr_count=cnt, nbr_offsets=off, nbr_ids=flat, density=density, k=k,
         v=ps.v.numpy().copy(), d=solver.dx.numpy().copy(), m=ps.m.numpy().copy(), m_inv=ps.m_inv.numpy().copy(),
         divergence=ps.divergence.numpy().copy(),
+        stats_density_errors=np.array(solver.stats_density_errors, np.float64),
+        stats_pcg_iters=np.array(solver.stats_pcg_iters, np.int32),
+        stats_outer_iters=np.int32(solver.stats_outer_iters),
+        stats_final_density_error=np.float64(solver.stats_final_density_error))
+
+
+def _scene_overflow():
+    """A 7 x 7 x 7 fluid block at 0.7 d spacing, moving, inside a static box:
+    about 96 neighbours within h at the centre, so the lists of the inner
+    particles are truncated at neighborCacheSize = 60."""
+    from implicitvelocityprojection_b200 import scenes as S
+    d = 0.02
+    rng = np.random.default_rng(17)
+    fluid = S.lattice_block([0.14, 0.12, 0.14], (7, 7, 7), 0.7 * d, jitter=0.01, seed=19)
+    box = (0.3, 0.3, 0.3)
+    center = [0.08 + 0.5 * b for b in box]
+    shell = S.cube_shell(center, box, d, layers=1)
+    domain = [b + 0.16 for b in box]
+    sc = S.assemble([fluid], [shell], particle_radius=0.5 * d, domain_size=domain, name="overflow_block",
+                    max_outer_iters=2, fixed_outer_iters=True)
+    nf = fluid.shape[0]
+    sc.v[:nf] = (rng.uniform(-0.05, 0.05, size=(nf, 3)) + np.array([0.0, -0.3, 0.1])).astype(np.float32)
+    return sc
+
+
+def make_overflow_solve(out):
+    """The reference's neighbour build, density, Aii and one IP solve (two
+    fixed outer updates) on a block whose inner lists are truncated at
+    neighborCacheSize: the reference keeps the first 60 hits of its hash-grid
+    walk and applies J^T in scatter form over the truncated rows
+    (ip.py:110-121)."""
+    from scripts.sim.forces.pressure.ip import IP
+    sc = _scene_overflow()
+    cfg, ps, ns = _make_objects(sc)
+    solver = IP(ps, ns, cfg)
+    t0 = time.time()
+    ns.build(ps.x, ps.particle_num)
+    ns.build_cache(ps.x, ps.particle_num, int(ps.cache_size), ps.neighbor_count, ps.neighbor_ids,
+                   ps.neighbor_gradW)
+    solver.compute_density()
+    solver.compute_Aii()
+    nd = sc.n_dynamic
+    cnt, off, flat = _lists(ps, nd)
+    full = int((cnt >= ps.cache_size).sum())
+    density = ps.density.numpy().copy()
+    k = solver.k.numpy().copy()
+    solver.solve(sc.dt)
+    print(f"overflow_solve: {time.time() - t0:.1f}s full rows={full} outer={solver.stats_outer_iters} "
+          f"pcg={solver.stats_pcg_iters}")
+    np.savez_compressed(
+        out, x=sc.x, v0=sc.v, is_dynamic=sc.is_dynamic, material=sc.material, density0=sc.density0,
+        particle_radius=np.float64(sc.particle_radius), domain_size=sc.domain_size, dt=np.float64(sc.dt),
+        max_outer_iters=np.int32(sc.max_outer_iters), cache_size=np.int32(ps.cache_size),
+        nbr_count=cnt, nbr_offsets=off, nbr_ids=flat, density=density, k=k,
+        v=ps.v.numpy().copy(), m=ps.m.numpy().copy(),
         stats_density_errors=np.array(solver.stats_density_errors, np.float64),
         stats_pcg_iters=np.array(solver.stats_pcg_iters, np.int32),
         stats_outer_iters=np.int32(solver.stats_outer_iters),
@@ -303,15 +361,19 @@ def make_column_steps(out, steps, viscosity=0.0, sigma=0.0, pressure_method=1):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("IVP_REFERENCE"),
+                    help="checkout of the reference (default: $IVP_REFERENCE)")
     ap.add_argument("--steps", type=int, default=12)
     ap.add_argument("--only", default=None)
     a = ap.parse_args()
+    if not a.reference:
+        sys.exit("give the reference checkout with --reference PATH or IVP_REFERENCE")
     if not os.path.isdir(os.path.join(a.reference, "scripts")):
         sys.exit(f"reference checkout not found at {a.reference}")
     _setup(a.reference)
     jobs = {"kernels": lambda: make_kernels(os.path.join(HERE, "kernels.npz")),
             "block_solve": lambda: make_block_solve(os.path.join(HERE, "block_solve.npz")),
+            "overflow_solve": lambda: make_overflow_solve(os.path.join(HERE, "overflow_solve.npz")),
             "column_steps": lambda: make_column_steps(os.path.join(HERE, "column_steps.npz"), a.steps),
             "visc_solve": lambda: make_visc_solve(os.path.join(HERE, "visc_solve.npz")),
             "column_visc_steps": lambda: make_column_steps(os.path.join(HERE, "column_visc_steps.npz"), 10,

@@ -1,22 +1,26 @@
 """CUDA engine vs the CPU oracle and the golden fixtures (through the C ABI).
 
-Tolerances: neighbour sets identical (integer work);
-per-particle density, k and velocity correction within 1e-4 relative in FP32
-(relative to the largest magnitude in the scene); outer-iteration count
-within +-1; CG iteration counts equal when the outer counts agree.
+Tolerances (see _gpu_helpers): neighbour sets identical
+(integer work); per-particle density, k and velocity within 1e-4 relative in
+FP32 (relative to the largest magnitude in the scene); outer-iteration count
+within +-1; results compared whenever the iteration counts agree, with the
+outer count forced to the reference's where it differs, and a floor on the
+compared steps of every multi-step test.
 """
+import dataclasses
 import os
 
 import numpy as np
 import pytest
 import torch
 
+import _gpu_helpers as H
 from oracle import oracle as O
 from implicitvelocityprojection_b200 import scenes as S
 
 pytestmark = pytest.mark.gpu
 
-RTOL = 1e-4
+RTOL = H.RTOL
 
 
 def _engine(scs, **opt):
@@ -64,9 +68,13 @@ def test_neighbour_sets_density_k(small):
 
 
 def test_block_solve_vs_golden(golden_dir):
+    """One IP solve from the reference's compressed, moving block: lists,
+    density, k, outer and CG counts, velocity, density-error history and the
+    divergence output against the reference's own run."""
+    from implicitvelocityprojection_b200.engine import Engine
     g = _load(golden_dir, "block_solve.npz")
     sc = _scene_from_golden(g, g["x"], g["v0"])
-    eng = _engine([sc])
+    eng = Engine([sc], divergence=True)
     eng.build()
     dyn = sc.is_dynamic == 1
     cnt, ids = eng.neighbours(0)
@@ -78,13 +86,24 @@ def test_block_solve_vs_golden(golden_dir):
     eng.solve()
     s = eng.stats(0)
     assert s.status == 0
-    assert abs(s.stats_outer_iters - int(g["stats_outer_iters"])) <= 1
-    if s.stats_outer_iters == int(g["stats_outer_iters"]):
-        assert s.stats_pcg_iters == g["stats_pcg_iters"].tolist()
-        assert _rel(eng.get("v")[dyn], g["v"][dyn]) < RTOL
-        np.testing.assert_allclose(s.stats_density_errors, g["stats_density_errors"], rtol=1e-3)
+    outer = int(g["stats_outer_iters"])
+    assert abs(s.stats_outer_iters - outer) <= 1
     np.testing.assert_allclose(s.stats_final_density_error, float(g["stats_final_density_error"]), rtol=1e-3,
                                atol=1e-7)
+    if s.stats_outer_iters != outer:
+        # an error within rounding of densityErrorTol: the reference's count,
+        # forced (fixedOuterIters), then compared
+        eng = Engine([dataclasses.replace(sc, fixed_outer_iters=True, max_outer_iters=outer)], divergence=True)
+        eng.build()
+        eng.solve()
+        s = eng.stats(0)
+    assert s.stats_outer_iters == outer
+    assert s.stats_pcg_iters == g["stats_pcg_iters"].tolist()
+    assert _rel(eng.get("v")[dyn], g["v"][dyn]) < RTOL
+    np.testing.assert_allclose(s.stats_density_errors, g["stats_density_errors"], rtol=1e-3)
+    # ps.divergence = max(J v, 0) (pressure_base.py:449-457)
+    assert np.abs(g["divergence"][dyn]).max() > 0
+    assert _rel(eng.get("divergence")[dyn], g["divergence"][dyn]) < RTOL
 
 
 def test_column_steps_vs_golden(golden_dir):
@@ -121,21 +140,13 @@ def test_small_column_steps_vs_oracle(small):
     state (strict per-step parity), then a free run of both."""
     st = O.State.from_scene(small)
     st.rebuild()
-    dyn = small.is_dynamic == 1
-    for s in range(12):
-        sc = S.Scene(**{**small.__dict__, "x": st.x.copy(), "v": st.v.copy()})
-        eng = _engine([sc])
-        eng.build()
-        eng.step(1)
-        st.step(fast=True)
-        gs = eng.stats(0)
-        assert gs.status == 0 and st.status == 0
-        assert abs(gs.stats_outer_iters - st.stats_outer_iters) <= 1, s
-        if gs.stats_outer_iters == st.stats_outer_iters and gs.stats_pcg_iters == st.stats_pcg_iters:
-            assert _rel(eng.get("v")[dyn], st.v[dyn]) < RTOL, s
-            assert np.abs(eng.get("x")[dyn] - st.x[dyn]).max() < 1e-6, s
-            np.testing.assert_allclose(eng.get("density")[dyn], st.density[dyn], rtol=RTOL)
-            np.testing.assert_allclose(eng.get("k")[dyn], st.k[dyn], rtol=RTOL)
+    compared = 0
+    steps = 12
+    for s in range(steps):
+        sc = H.with_state(small, st.x, st.v)
+        ok, eng, st = H.compare_step(sc)
+        compared += ok
+    assert compared >= steps - 1, compared
 
 
 def test_small_column_free_run_vs_oracle(small):
@@ -156,57 +167,42 @@ def test_small_column_free_run_vs_oracle(small):
 
 
 def test_solve_matches_oracle_and_fp64(small):
-    """One IP solve from a compressed state: velocity correction vs the oracle
-    (1e-4 relative) and the first linear system's CG solution vs an FP64 CG
-    solve of the same system (error stated, bounded by the absolute tol_pcg)."""
+    """One IP solve from a compressed, moving state: velocity against the
+    oracle (1e-4 relative), and the first linear system's FP64 CG solution
+    exists (the FP32 path's error against it is stated by
+    test_cg_solution_error_vs_fp64_oracle)."""
     sc = S.column_in_box((12, 14, 12), 0.018, (0.4, 0.5, 0.4), seed=5)
     rng = np.random.default_rng(1)
     sc.v[sc.is_dynamic == 1] = rng.normal(0, 0.2, size=(sc.n_dynamic, 3)).astype(np.float32)
-    eng = _engine([sc])
-    eng.build()
-    v0 = eng.get("v").copy()
-    eng.solve()
-    gs = eng.stats(0)
-    st = O.State.from_scene(sc)
-    st.rebuild()
-    d = st.solve(fast=True, return_d=True)
+    ok, eng, st, _ = H.compare_solve(sc)
+    assert ok, "iteration counts differ even with the outer count fixed"
     dyn = sc.is_dynamic == 1
-    assert gs.status == 0 and st.status == 0
-    assert abs(gs.stats_outer_iters - st.stats_outer_iters) <= 1
-    if gs.stats_outer_iters == st.stats_outer_iters and gs.stats_pcg_iters == st.stats_pcg_iters:
-        dv_gpu = eng.get("v")[dyn] - v0[dyn]
-        dv_orc = st.v[dyn] - v0[dyn]
-        assert _rel(dv_gpu, dv_orc) < 1e-3
-        assert _rel(eng.get("v")[dyn], st.v[dyn]) < RTOL
-    # FP64 CG solution of the first outer system
     st2 = O.State.from_scene(sc)
     st2.rebuild()
     d0 = np.zeros((sc.n, 3), np.float32)
     d0[dyn] = np.float32(sc.dt) * sc.v[dyn]
     t, f, dfdt, rhs = st2.system(d0)
     x64, it = st2.cg_f64(dfdt, rhs, rel_tol=1e-12)
-    assert it > 0
-    # the FP32 path stops at ||r||^2 < tol_pcg (absolute); its error vs the
-    # exact solution is bounded through ||A^-1|| ||r||; here it is stated
-    assert np.isfinite(x64).all()
+    assert it > 0 and np.isfinite(x64).all()
 
 
-@pytest.mark.parametrize("row_format,bound", [(1, 1e-3), (3, 0.1)])
-def test_cg_solution_error_vs_fp64_oracle(row_format, bound):
-    """The CG solution of one outer system (a compressed column after 40
-    steps, one fixed outer update) against the oracle's FP64 CG on the same
-    system run for the same number of iterations: the precision error of the
-    FP32 rows (measured 5e-5 here, 1e-3 on the 102,400-particle column) and of
-    the bf16 gradients (3e-2, 1-2e-2).  Against the fully converged FP64
-    solution both are about 0.25 off: the reference's CG stops once
-    |r|^2 < tol_pcg (1e-6, absolute) after two iterations."""
-    import dataclasses
-    sc = S.small_column()
+@pytest.mark.parametrize("workload,row_format,bound", [("small_column", 1, 1e-3), ("small_column", 3, 0.1),
+                                                       ("tall_column_102k", 1, 3e-3),
+                                                       ("tall_column_102k", 3, 0.1)])
+def test_cg_solution_error_vs_fp64_oracle(workload, row_format, bound, record_property):
+    """The CG solution of one outer system (the column after 40 steps, one
+    fixed outer update) against the oracle's FP64 CG on the same system run
+    for the same number of iterations: the precision error of the FP32 rows
+    and of the bf16 gradients, stated per configuration (printed and recorded
+    as a test property).  Against the fully converged FP64 solution both are
+    about 0.25-0.6 off: the reference's CG stops once |r|^2 < tol_pcg (1e-6,
+    absolute, ip.py:319) after two iterations."""
+    sc = S.small_column() if workload == "small_column" else S.tall_column()
     eng = _engine([sc])
     eng.build()
     eng.step(40)
     s1 = dataclasses.replace(sc, x=eng.get("x").copy(), v=eng.get("v").copy(), max_outer_iters=1,
-                             fixed_outer_iters=True)
+                             fixed_outer_iters=True, viscosity_method=0, viscosity_coeff=0.0)
     dyn = sc.is_dynamic == 1
     st = O.State.from_scene(s1)
     st.rebuild()
@@ -222,10 +218,15 @@ def test_cg_solution_error_vs_fp64_oracle(row_format, bound):
     sol = np.float64(sc.dt) * (vb - e.get("v").astype(np.float64))
     xk, _ = st.cg_f64(dfdt, rhs, rel_tol=0.0, max_iter=gs.stats_pcg_iters[0])
     err = np.linalg.norm(sol[dyn] - xk[dyn]) / np.linalg.norm(xk[dyn])
-    assert err < bound, err
     x64, it = st.cg_f64(dfdt, rhs, rel_tol=1e-14)
+    err64 = np.linalg.norm(sol[dyn] - x64[dyn]) / np.linalg.norm(x64[dyn])
+    print(f"{workload} rows={'bf16' if row_format == 3 else 'fp32'}: CG iterations {gs.stats_pcg_iters[0]}, "
+          f"error vs FP64 CG at equal iterations {err:.3e}, vs converged FP64 ({it} iterations) {err64:.3e}")
+    record_property("error_vs_fp64_equal_iterations", float(err))
+    record_property("error_vs_fp64_converged", float(err64))
+    assert err < bound, err
     assert it > gs.stats_pcg_iters[0]
-    assert np.linalg.norm(sol[dyn] - x64[dyn]) / np.linalg.norm(x64[dyn]) < 0.5
+    assert err64 < 0.8
 
 
 def test_multi_scene_bitwise_equal_to_alone():
@@ -391,7 +392,9 @@ def test_viscosity_solve_vs_golden(golden_dir):
 def test_column_visc_steps_vs_golden(golden_dir, persistent):
     g = _load(golden_dir, "column_visc_steps.npz")
     dyn = g["is_dynamic"] == 1
-    for s in range(g["x"].shape[0]):
+    steps = g["x"].shape[0]
+    compared = 0
+    for s in range(steps):
         x_prev = g["x0"] if s == 0 else g["x"][s - 1]
         v_prev = g["v0"] if s == 0 else g["v"][s - 1]
         sc = _visc_scene(g, x_prev, v_prev, g["viscosity"])
@@ -401,10 +404,13 @@ def test_column_visc_steps_vs_golden(golden_dir, persistent):
         eng.step(1)
         st = eng.stats(0)
         assert st.status == 0
+        assert abs(st.stats_outer_iters - int(g["outer"][s])) <= 1
         if st.stats_outer_iters != int(g["outer"][s]):
             continue
+        compared += 1
         assert _rel(eng.get("v")[dyn], g["v"][s][dyn]) < RTOL, s
         assert np.abs(eng.get("x")[dyn] - g["x"][s][dyn]).max() < 1e-6, s
+    assert compared >= steps - 1, compared
 
 
 def test_viscous_column_vs_oracle_and_paths():
@@ -414,20 +420,18 @@ def test_viscous_column_vs_oracle_and_paths():
     sc = S.column_in_box((12, 24, 12), 0.02, (0.4, 1.0, 0.4), seed=4, viscosity_method=1, viscosity_coeff=1e-3)
     st = O.State.from_scene(sc)
     st.rebuild()
-    dyn = sc.is_dynamic == 1
-    for s in range(6):
-        cur = S.Scene(**{**sc.__dict__, "x": st.x.copy(), "v": st.v.copy()})
-        a = _engine([cur], persistent=True)
+    compared = 0
+    steps = 6
+    for s in range(steps):
+        cur = H.with_state(sc, st.x, st.v)
         b = _engine([cur], persistent=False)
-        for e in (a, b):
-            e.build()
-            e.step(1)
-        st.step(fast=True)
-        assert np.array_equal(a.get("v"), b.get("v"))
-        ga = a.stats(0)
-        assert ga.status == 0 and st.status == 0
-        if ga.stats_outer_iters == st.stats_outer_iters and ga.stats_pcg_iters == st.stats_pcg_iters:
-            assert _rel(a.get("v")[dyn], st.v[dyn]) < RTOL, s
+        b.build()
+        b.step(1)
+        ok, a, st = H.compare_step(cur, persistent=True)
+        compared += ok
+        if ok:  # the same (unforced) solve on both paths
+            assert np.array_equal(a.get("v"), b.get("v"))
+    assert compared >= steps - 1, compared
 
 
 @pytest.mark.parametrize("persistent", [True, False])
@@ -586,11 +590,19 @@ def test_prj_solve_vs_golden(golden_dir, persistent):
     eng.prj_solve()
     st = eng.stats(0)
     dyn = sc.is_dynamic == 1
+    passes = int(g["stats_outer_iters"])
     assert st.status == 0
-    assert abs(st.stats_outer_iters - int(g["stats_outer_iters"])) <= 1
-    if st.stats_outer_iters == int(g["stats_outer_iters"]):
-        assert _rel(eng.get("v")[dyn], g["v"][dyn]) < RTOL
-        np.testing.assert_allclose(st.stats_density_errors, g["stats_density_errors"], rtol=1e-3, atol=1e-8)
+    assert abs(st.stats_outer_iters - passes) <= 1
+    if st.stats_outer_iters != passes:
+        # the reference's pass count, forced (fixedOuterIters), then compared
+        eng = _engine([dataclasses.replace(sc, fixed_outer_iters=True, max_outer_iters=passes)],
+                      persistent=persistent)
+        eng.build()
+        eng.prj_solve()
+        st = eng.stats(0)
+    assert st.stats_outer_iters == passes
+    assert _rel(eng.get("v")[dyn], g["v"][dyn]) < RTOL
+    np.testing.assert_allclose(st.stats_density_errors, g["stats_density_errors"], rtol=1e-3, atol=1e-8)
 
 
 @pytest.mark.parametrize("persistent", [True, False])

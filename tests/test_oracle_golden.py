@@ -114,6 +114,63 @@ def test_column_trajectory(golden_dir):
 
 # ---------------------------------------------------------------- analytic KATs
 
+def _overflow_state(g):
+    sc = S.Scene(x=g["x"].copy(), v=g["v0"].copy(), is_dynamic=g["is_dynamic"], material=g["material"],
+                 density0=g["density0"], particle_radius=float(g["particle_radius"]),
+                 domain_size=g["domain_size"], dt=float(g["dt"]), max_outer_iters=int(g["max_outer_iters"]),
+                 fixed_outer_iters=True)
+    return O.State.from_scene(sc)
+
+
+@pytest.mark.parametrize("fast", [False, True])
+def test_overflow_solve(golden_dir, fast):
+    """Truncated lists (neighbour_search.py:38-51: the first neighborCacheSize
+    hits of the hash-grid walk) and the IP solve whose J^T is the scatter form
+    over the truncated rows (ip.py:110-121), against the reference's own run.
+    FAST mode switches to the scatter form when a list is full."""
+    g = _load(golden_dir, "overflow_solve.npz")
+    st = _overflow_state(g)
+    st.rebuild(only_dynamic=True)
+    dyn = st.is_dynamic == 1
+    nd = int(dyn.sum())
+    assert st.overflow > 0 and int((g["nbr_count"] >= int(g["cache_size"])).sum()) > 0
+    off, ids = g["nbr_offsets"], g["nbr_ids"]
+    for i in range(nd):
+        assert st.neighbour_sets(i) == set(ids[off[i]:off[i + 1]].tolist()), i
+    np.testing.assert_allclose(st.density[dyn], g["density"][dyn], rtol=RTOL)
+    np.testing.assert_allclose(st.k[dyn], g["k"][dyn], rtol=RTOL)
+    st.solve(fast=fast)
+    assert st.status == O.OK
+    assert st.stats_outer_iters == int(g["stats_outer_iters"])
+    assert st.stats_pcg_iters == g["stats_pcg_iters"].tolist()
+    assert _rel(st.v[dyn], g["v"][dyn]) < RTOL
+
+
+def test_overflow_truncation_order():
+    """The kept hits of a truncated list are the neighborCacheSize smallest
+    (linear cell index with x fastest, particle index) keys over cells of size
+    h from the domain origin, the order of the reference's hash-grid walk."""
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "overflow_solve.npz"))
+    st = _overflow_state(g)
+    st.rebuild(only_dynamic=True)
+    x = st.x.astype(np.float32)
+    h = np.float32(st.h)
+    inv = np.float32(1.0) / h
+    dims = np.ceil(st.domain_size.astype(np.float64) / np.float64(h)).astype(np.int64)
+    cell = np.clip(np.floor(x * inv).astype(np.int64), 0, dims - 1)
+    lin = (cell[:, 2] * dims[1] + cell[:, 1]) * dims[0] + cell[:, 0]
+    full = np.where((st.count >= st.cache_size) & (st.is_dynamic == 1))[0]
+    assert len(full) > 0
+    for i in full[:40]:
+        r = x[i] - x
+        d2 = ((r[:, 0] * r[:, 0]).astype(np.float32) + (r[:, 1] * r[:, 1]).astype(np.float32)).astype(np.float32)
+        d2 = (d2 + (r[:, 2] * r[:, 2]).astype(np.float32)).astype(np.float32)
+        hits = np.where((np.sqrt(d2) < h) & (np.arange(st.n) != i))[0]
+        assert len(hits) > st.cache_size
+        order = np.lexsort((hits, lin[hits]))
+        assert set(hits[order][:st.cache_size].tolist()) == st.neighbour_sets(i), i
+
+
 def test_rest_lattice_density_and_counts():
     """Exact lattice, h = 2d: interior density is 800 kg/m^3 (sum W d^3 = 1 and
     m = 0.8 d^3 rho0).  Lattice offsets with |o|^2 in {1, 2, 3} (6 + 12 + 8 = 26)

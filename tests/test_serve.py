@@ -1,6 +1,7 @@
 """Served form: the request loop's scheduling on CPU with a stand-in engine,
 and on the GPU bit-identity of a served request with the scene run alone."""
 import dataclasses
+import time
 
 import numpy as np
 import pytest
@@ -81,6 +82,7 @@ def test_oversized_request_rejected_and_idle_gaps_skipped():
 
 class _Failed:
     status = 0
+    solves = 4        # the chunk's four steps, one of which failed
     failed_solves = 1
     last_failure = 3  # IVP_ERR_NOT_CONVERGED
 
@@ -94,21 +96,83 @@ class FailingEngine(FakeEngine):
 
 def test_failed_request_leaves_batch_others_continue():
     """A request whose solve fails finishes at the end of that chunk with the
-    solve's status and leaves the batch; the requests batched with it run to
-    their end with their state carried exactly, as if it had never been
-    there."""
+    solve's status and leaves the batch, credited only with the steps whose
+    solve succeeded; the requests batched with it run to their end with their
+    state carried exactly, as if it had never been there."""
     reqs = [_req(0.0, 10, 9, "a"), _req(0.0, 5, 20, "bad"), _req(0.0, 8, 6, "c")]
     FakeEngine.built = []
     srv = Server(engine_factory=FailingEngine, footprint=lambda sc: sc.n, hbm_budget_bytes=1000, chunk_steps=4)
     rep = srv.run(reqs)
     by = {r.rid: r for r in rep.results}
-    assert by[1].status == 3 and by[1].steps == 4
+    assert by[1].status == 3 and by[1].steps == 3
     for rid in (0, 2):
         assert by[rid].status == 0 and by[rid].steps == reqs[rid].steps
         assert np.all(by[rid].x == np.float32(reqs[rid].steps))
     assert all("bad" not in names for names in FakeEngine.built[1:])  # re-planned without it
     s = rep.summary()
     assert s["completed"] == 2 and s["failed"] == 1 and s["rejected"] == 0
+    assert s["particle_steps"] == 10 * 9 + 8 * 6 + 5 * 3  # the failed step is not counted
+
+
+class _FakeChunk:
+    """n steps that take `step_s` each on a pretend device."""
+
+    def __init__(self, n, step_s):
+        self.n, self.step_s = n, step_s
+        self.t_end = time.perf_counter() + n * step_s
+
+    def done(self):
+        return time.perf_counter() >= self.t_end
+
+    def wait(self):
+        time.sleep(max(0.0, self.t_end - time.perf_counter()))
+
+    def step_ms(self):
+        return [1000.0 * self.step_s] * self.n
+
+
+class ChunkedFakeEngine(FakeEngine):
+    """FakeEngine whose chunks run asynchronously for n * step_s of wall time
+    (the state is final at launch, as a device's would be at the boundary);
+    records when each engine was created."""
+    step_s = 0.01
+    created = []
+
+    def __init__(self, scenes):
+        super().__init__(scenes)
+        ChunkedFakeEngine.created.append((time.perf_counter(), [s.name for s in scenes]))
+
+    def step_chunk(self, n):
+        self.step(n)
+        return _FakeChunk(n, self.step_s)
+
+    def raw_stats_all(self):
+        return [_Stats() for _ in self.scenes]
+
+
+def test_realtime_admits_while_a_chunk_is_in_flight():
+    """On the wall clock: b arrives while a's first chunk (20 steps, 0.2 s)
+    runs; it is admitted at once and the next batch's engine is created
+    before that chunk ends, so b joins at the first boundary.  State is
+    carried exactly and per-step latencies are reported."""
+    reqs = [_req(0.0, 10, 40, "a"), _req(0.05, 5, 10, "b")]
+    FakeEngine.built = []
+    ChunkedFakeEngine.created = []
+    srv = Server(engine_factory=ChunkedFakeEngine, footprint=lambda sc: sc.n, hbm_budget_bytes=100, chunk_steps=20)
+    rep = srv.run_realtime(reqs)
+    by = {r.rid: r for r in rep.results}
+    assert by[0].status == 0 and by[1].status == 0
+    assert np.all(by[0].x == np.float32(40)) and np.all(by[1].x == np.float32(10))
+    assert by[1].admit_s < 0.2  # admitted during the first chunk
+    c0 = ChunkedFakeEngine.created[0][0]  # a's engine: its first chunk starts right after
+    made = [(t - c0, names) for t, names in ChunkedFakeEngine.created]
+    ab = [t for t, names in made if names == ["a", "b"]]
+    assert ab and ab[0] < 0.2, made  # the next batch was prepared while the chunk ran
+    assert by[1].finish_s < 0.45  # joined at the first boundary (0.2 s) and ran 10 steps
+    s = rep.summary()
+    # batched steps: 20 of a alone, 10 of the pair (b's remaining steps), 10 of a alone
+    assert s["steps"] == 40 and abs(s["step_p50_ms"] - 10.0) < 1e-9
+    assert s["particle_steps"] == 10 * 40 + 5 * 10
 
 
 def test_workspace_footprint_grows_with_particles():

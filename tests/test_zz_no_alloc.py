@@ -57,6 +57,31 @@ def test_noalloc_matches_engine_twice():
             assert np.all(d[~dmask] == -1.0)  # static densities are left untouched
 
 
+def test_noalloc_matches_reference_fixture(golden_dir):
+    """Density and k against the reference's own neighbour build, density and
+    Aii (tests/golden/block_solve.npz), on two calls in a row."""
+    import os
+    g = np.load(os.path.join(golden_dir, "block_solve.npz"))
+    L = _lib.load()
+    dev = torch.device("cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    n = g["x"].shape[0]
+    sc = S.Scene(x=np.array(g["x"], np.float32), v=np.array(g["v0"], np.float32), is_dynamic=g["is_dynamic"],
+                 material=g["material"], density0=g["density0"], particle_radius=float(g["particle_radius"]),
+                 domain_size=g["domain_size"], dt=float(g["dt"]))
+    x = torch.from_numpy(sc.x).to(dev)
+    m = torch.from_numpy(np.array(g["m"], np.float32)).to(dev)
+    dyn = torch.from_numpy(np.array(g["is_dynamic"], np.int32)).to(dev)
+    dmask = g["is_dynamic"] == 1
+    for _ in range(2):
+        density = torch.full((n,), -1.0, dtype=torch.float32, device=dev)
+        k = torch.full((n,), -1.0, dtype=torch.float32, device=dev)
+        assert _call(L, sc, x, m, dyn, density, k, stream) == _lib.OK
+        torch.cuda.synchronize()
+        np.testing.assert_allclose(density.cpu().numpy()[dmask], g["density"][dmask], rtol=RTOL)
+        np.testing.assert_allclose(k.cpu().numpy()[dmask], g["k"][dmask], rtol=RTOL)
+
+
 def test_noalloc_rejects_oversized_inputs():
     L = _lib.load()
     dev = torch.device("cuda")
@@ -76,3 +101,4 @@ def test_noalloc_rejects_oversized_inputs():
     ds = torch.from_numpy(small.is_dynamic).to(dev)
     o = torch.zeros(small.n, dtype=torch.float32, device=dev)
     assert _call(L, small, xs, ms, ds, o, o.clone(), stream) == _lib.BAD_ARG
+    assert "IVP_NOALLOC_MAX_CELLS" in L.ivp_last_error().decode()  # the reason, for the caller
