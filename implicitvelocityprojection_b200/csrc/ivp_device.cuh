@@ -194,6 +194,12 @@ struct Dev {
     // cg[(k + 1) & 1], so a neighbour gather takes one sector.
     float4* cg0;
     float4* cg1;
+    // IP CG, per slot: the residual r (gathered by phase A), the direction p
+    // (own slot) and J p of the last phase A (own slot, for the recurrence
+    // J p_k = J r_k + beta J p_(k-1))
+    float4* rip;
+    float4* pip;
+    float* jp;
     float* y;
     float* s;
     float* fk;
@@ -361,6 +367,17 @@ __device__ __forceinline__ void ld_rec(const float4* p, float4& a, float4& b) {
     asm volatile("ld.global.L1::evict_last.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
                  : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
                  : "l"(p));
+}
+
+// One 16-byte per-slot vector written in an earlier phase of the same
+// launch, gathered for a neighbour (kept in L1 ahead of streamed data; the
+// fence after each grid barrier orders it after the writes).
+__device__ __forceinline__ float4 ld_vec(const float4* p) {
+    float4 a;
+    asm volatile("ld.global.L1::evict_last.v4.f32 {%0, %1, %2, %3}, [%4];"
+                 : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w)
+                 : "l"(p));
+    return a;
 }
 
 // Two consecutive neighbour-list entries (32-byte aligned, read-only for the

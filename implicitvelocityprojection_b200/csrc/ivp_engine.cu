@@ -655,7 +655,7 @@ struct Plan {
     bool any_st = false;   // some scene runs the implicit surface tension
     int drop_cap = 0;      // dropped-pair records of the overflow fix-up
     int fix_scan_blocks = 0;
-    size_t off[64];
+    size_t off[72];
     Layout lay;
 };
 
@@ -820,6 +820,9 @@ void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
     P.off[i++] = L.add(2 * sizeof(float4) * (size_t)P.drop_cap);               // 59 fix_w
     P.off[i++] = L.add(sizeof(int) * S);                                       // 60 fix_fail
     P.off[i++] = L.add(sizeof(int) * S);                                       // 61 fix_scene
+    P.off[i++] = L.add(sizeof(float4) * N);                                    // 62 rip
+    P.off[i++] = L.add(sizeof(float4) * N);                                    // 63 pip
+    P.off[i++] = L.add(sizeof(float) * N);                                     // 64 jp
 }
 
 cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
@@ -1028,6 +1031,9 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
     D.fix_w = reinterpret_cast<float4*>(w + P.off[i++]);
     D.fix_fail = reinterpret_cast<int*>(w + P.off[i++]);
     D.fix_scene = reinterpret_cast<int*>(w + P.off[i++]);
+    D.rip = reinterpret_cast<float4*>(w + P.off[i++]);
+    D.pip = reinterpret_cast<float4*>(w + P.off[i++]);
+    D.jp = reinterpret_cast<float*>(w + P.off[i++]);
     D.drop_cap = P.drop_cap;
     e->fix_scan_blocks = P.fix_scan_blocks;
     D.n_segs = (int)P.segs.size();

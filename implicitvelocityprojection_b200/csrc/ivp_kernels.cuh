@@ -1394,8 +1394,9 @@ __device__ __forceinline__ double rhs_tile(const Dev& D, const SceneParams& P, c
     if (T.valid && T.lane == 0) {
         const float om = P.omega;
         const float4 rhs = make_float4(om * ax, om * ay, om * az, 0.0f);
-        D.cg0[2 * T.i] = rhs;
-        D.cg0[2 * T.i + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+        D.rip[T.i] = rhs;
+        D.pip[T.i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        D.jp[T.i] = 0.0f;
         D.sol[T.i] = make_float4(0.f, 0.f, 0.f, 0.f);
         D.e[T.i] = dcur[T.i];  // d - 0
         part = (double)dot3(f3(rhs), f3(rhs));
@@ -1403,47 +1404,46 @@ __device__ __forceinline__ double rhs_tile(const Dev& D, const SceneParams& P, c
     return part;
 }
 
-// CG phase A: p = r + beta p_prev (ip.py:323-327, formed on the fly for the
-// neighbours too), y = dfdt k (J p) (compute_Jx_pcg, ip.py:19-60), and the
-// FP64 partials of p^T A p = sum m |p|^2 + omega sum y (J p) (the value
-// dot(p, A p) of ip.py:307: the gather-form transpose is the exact transpose
-// of J for symmetric lists).
+// CG phase A: p = r + beta p_prev (ip.py:323-327) for the own slot, and
+// J p (compute_Jx_pcg, ip.py:19-60) by the recurrence
+//   J p_k = J r_k + beta J p_(k-1),
+// exact for the linear J, so the neighbour pass gathers only r_j (16 B from a
+// dense array) instead of r_j and p_prev_j; J p of the own slot is kept for
+// the next iteration.  y = dfdt k (J p), and the FP64 partials of
+// p^T A p = sum m |p|^2 + omega sum y (J p) (the value dot(p, A p) of
+// ip.py:307: phase B applies the exact transpose of J).
 template <int G>
 __device__ __forceinline__ double cga_tile(const Dev& D, const SceneParams& P, const TileCtx& T, float beta,
                                            int cg_it) {
-    const float4* cc = (cg_it & 1) ? D.cg1 : D.cg0;  // {r, p_prev}
-    float4* cn = (cg_it & 1) ? D.cg0 : D.cg1;
     const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
-    float3 xi = make_float3(0.f, 0.f, 0.f), pi = xi;
-    float mi = 0.0f;
+    float3 xi = make_float3(0.f, 0.f, 0.f), ri = xi;
     if (T.valid) {
-        const float4 a = D.xm[T.i];
-        xi = f3(a);
-        mi = a.w;
-        const float4 ri = cc[2 * T.i], qi = cc[2 * T.i + 1];
-        pi = make_float3(ri.x + beta * qi.x, ri.y + beta * qi.y, ri.z + beta * qi.z);
+        xi = f3(D.xm[T.i]);
+        ri = f3(D.rip[T.i]);
     }
     float acc = 0.0f;
     const int self = T.valid ? T.i : P.s_begin;
     const bool bad = pair_loop<G>(D, T.row, xi, cnt, T.lane, self, P.s_begin, P.s_end, [&](const PairBatch& b) {
 #pragma unroll
         for (int u = 0; u < PU; ++u) {
-            const int j = b.j[u];
-            float4 rj, qj;
-            ld_rec(cc + 2 * j, rj, qj);
-            const float3 pj = make_float3(rj.x + beta * qj.x, rj.y + beta * qj.y, rj.z + beta * qj.z);
-            acc += dot3(sub3(pi, pj), b.J[u]);
+            const float3 rj = f3(ld_vec(D.rip + b.j[u]));
+            acc += dot3(sub3(ri, rj), b.J[u]);
         }
     });
     if (bad) flag_bad(D, T.i, 3);
     acc = group_sum<G>(acc);
     double part = 0.0;
     if (T.valid && T.lane == 0) {
-        const float yi = acc * D.s[T.i];
+        const float mi = D.xm[T.i].w;
+        const float4 qi = D.pip[T.i];
+        const float3 pi = make_float3(ri.x + beta * qi.x, ri.y + beta * qi.y, ri.z + beta * qi.z);
+        const float jp = cg_it > 0 ? acc + beta * D.jp[T.i] : acc;
+        D.jp[T.i] = jp;
+        const float yi = jp * D.s[T.i];
         D.y[T.i] = yi;
         D.z[T.i] = yi * D.inv_m[T.i];
-        cn[2 * T.i + 1] = make_float4(pi.x, pi.y, pi.z, 0.0f);
-        part = (double)(mi * dot3(pi, pi)) + (double)P.omega * (double)yi * (double)acc;
+        D.pip[T.i] = make_float4(pi.x, pi.y, pi.z, 0.0f);
+        part = (double)(mi * dot3(pi, pi)) + (double)P.omega * (double)yi * (double)jp;
     }
     return part;
 }
@@ -1471,8 +1471,6 @@ __device__ __noinline__ float3 ovf_correction(const int* __restrict__ fix_off, c
 template <int G>
 __device__ __forceinline__ double cgb_tile(const Dev& D, const SceneParams& P, const TileCtx& T, float alpha,
                                            int cg_it, const float4* __restrict__ dcur) {
-    const float4* cc = (cg_it & 1) ? D.cg1 : D.cg0;  // own r
-    float4* cn = (cg_it & 1) ? D.cg0 : D.cg1;        // own p; receives the new r
     const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
     float3 xi = make_float3(0.f, 0.f, 0.f);
     float mi = 0.0f, yi = 0.0f;
@@ -1508,9 +1506,9 @@ __device__ __forceinline__ double cgb_tile(const Dev& D, const SceneParams& P, c
             az -= c.z;
         }
         const float om = P.omega;
-        const float4 p4 = cn[2 * T.i + 1];
+        const float4 p4 = D.pip[T.i];
         const float3 ap = make_float3(mi * p4.x + om * ax, mi * p4.y + om * ay, mi * p4.z + om * az);
-        float4 xs = D.sol[T.i], rs = cc[2 * T.i];
+        float4 xs = D.sol[T.i], rs = D.rip[T.i];
         xs.x = xs.x + alpha * p4.x;
         xs.y = xs.y + alpha * p4.y;
         xs.z = xs.z + alpha * p4.z;
@@ -1520,7 +1518,7 @@ __device__ __forceinline__ double cgb_tile(const Dev& D, const SceneParams& P, c
         D.sol[T.i] = xs;
         const float4 dd = dcur[T.i];
         D.e[T.i] = make_float4(dd.x - xs.x, dd.y - xs.y, dd.z - xs.z, 0.0f);
-        cn[2 * T.i] = rs;
+        D.rip[T.i] = rs;
         part = (double)dot3(f3(rs), f3(rs));
     }
     return part;

@@ -10,6 +10,18 @@ with the outer-iteration count fixed at the engine's (the reference's
 fixedOuterIters, ip.py:364-370) and compared if their CG counts then agree.
 Every caller puts a floor on the number of compared steps, so a test can
 never pass while comparing nothing.
+
+A step is compared in two parts.  The build (neighbour sets, density, k) is
+checked against the oracle's rebuild of the same positions; the solve then
+starts, on both sides, from the engine's density and k.  The reason: the
+constraint t = rho - rho0 + J d is a small difference of large numbers
+(rho ~ 1000 kg/m^3 carries about 4e-4 kg/m^3 of FP32 rounding that depends on
+the summation order), and the reference's derivative switch
+dfdt = (t >= 1e-6) (ip.py:166) is discontinuous.  On a column of 102,400
+particles a few constraints sit within that rounding of the switch, so two
+valid FP32 evaluations of the reference's own algorithm can disagree on them
+and change their operator rows; handing both sides the same density removes
+that ambiguity while every other quantity is still computed independently.
 """
 from __future__ import annotations
 
@@ -73,13 +85,23 @@ def _counts(gs, raw, st) -> bool:
             and int(raw.sum_visc_iters) == st.visc_iters and int(raw.sum_st_iters) == st.st_iters)
 
 
+def same_build_inputs(st, density, k, dyn):
+    """The oracle state continues from the engine's density and k (checked
+    against the oracle's own by check_build)."""
+    st.density[dyn] = density[dyn]
+    st.k[dyn] = k[dyn]
+
+
 def _step_both(sc, opts):
     eng = engine([sc], **opts)
     eng.build()
-    eng.step(1)
-    gs, raw = eng.stats(0), eng.raw_stats(0)
     st = O.State.from_scene(sc)
     st.rebuild()
+    check_build(eng, st, sc)
+    dyn = sc.is_dynamic == 1
+    same_build_inputs(st, eng.get("density"), eng.get("k"), dyn)
+    eng.step(1)
+    gs, raw = eng.stats(0), eng.raw_stats(0)
     st.step(fast=True)
     return eng, gs, raw, st
 
@@ -104,8 +126,10 @@ def compare_step(sc, check_x=True, **opts):
         tol = XTOL + float(sc.dt) * RTOL * float(np.abs(st.v[dyn]).max())
         ex = float(np.abs(eng.get("x")[dyn] - st.x[dyn]).max())
         assert ex < tol, f"positions off by {ex:.3e} m (tolerance {tol:.3e})"
-    np.testing.assert_allclose(eng.get("density")[dyn], st.density[dyn], rtol=RTOL)
-    np.testing.assert_allclose(eng.get("k")[dyn], st.k[dyn], rtol=RTOL)
+    # the step's own rebuild (density, k) ran on the two sides' slightly
+    # different new positions; the build is compared from identical positions
+    # at the start of every restarted step (check_build), where a truncated
+    # list's kept hits do not depend on which cell a particle just moved into
     return True, eng, st
 
 
@@ -117,9 +141,11 @@ def compare_solve(sc, divergence=False, **opts):
         from implicitvelocityprojection_b200.engine import Engine, EngineOptions
         e = Engine([s], options=EngineOptions(**opts) if opts else None, divergence=divergence)
         e.build()
-        e.solve()
         o = O.State.from_scene(s)
         o.rebuild()
+        check_build(e, o, s)
+        same_build_inputs(o, e.get("density"), e.get("k"), s.is_dynamic == 1)
+        e.solve()
         div = o.solve(fast=True, divergence=divergence)
         return e, e.stats(0), o, div
 

@@ -325,12 +325,14 @@ def test_multi_scene_persistent_equals_per_phase():
         assert a.stats(i).stats_pcg_iters == b.stats(i).stats_pcg_iters
 
 
-@pytest.mark.parametrize("lanes", [1, 2, 8])
-def test_lane_variants_agree(small, lanes):
+@pytest.mark.parametrize("lanes,ppb", [(1, 128), (2, 128), (4, 64), (8, 32), (2, 64), (4, 32), (8, 16)])
+def test_lane_variants_agree(small, lanes, ppb):
+    """Every launch shape the autotuner can pick (and one lane per particle)
+    gives the same steps within the FP32 tolerance."""
     ref = _engine([small])
     ref.build()
     ref.step(3)
-    eng = _engine([small], lanes_per_particle=lanes, particles_per_block=128 // lanes)
+    eng = _engine([small], lanes_per_particle=lanes, particles_per_block=ppb)
     eng.build()
     eng.step(3)
     dyn = small.is_dynamic == 1
@@ -670,3 +672,27 @@ def test_prj_framework_dropin():
         fw.forward()
     assert fw.pressure.stats_outer_iters >= 1
     assert fw.pressure.stats_final_density_error < cfg.get_cfg("densityErrorTol", 1e-3)
+
+
+def test_autotuner_picks_a_candidate_and_caches():
+    """The autotuner times every candidate on the actual scenes, picks the
+    fastest, and answers the same scene set again from its cache; the engine
+    built with the choice steps to the same result as the default shape
+    within the FP32 tolerance."""
+    from implicitvelocityprojection_b200 import autotune
+    scs = [S.random_column(6000, 2.0, seed=101), S.random_column(3000, 1.5, seed=102)]
+    opts, res = autotune.tuned_options(scs, force=True)
+    assert not res["cached"] and len(res["table"]) == len(autotune.candidates())
+    best = min(res["table"], key=lambda r: r["ms_per_step"])
+    assert best["shape"].startswith(f"{opts.lanes_per_particle}x{opts.particles_per_block}/")
+    again = autotune.tune(scs)
+    assert again["cached"] and again["choice"] == res["choice"]
+    a = _engine(scs, lanes_per_particle=opts.lanes_per_particle, particles_per_block=opts.particles_per_block,
+                persistent=opts.persistent)
+    b = _engine(scs)
+    for e in (a, b):
+        e.build()
+        e.step(3)
+    for i in range(len(scs)):
+        dyn = scs[i].is_dynamic == 1
+        assert _rel(a.get("v", i)[dyn], b.get("v", i)[dyn]) < 1e-4

@@ -199,3 +199,24 @@ def test_served_request_equals_scene_alone():
         alone.step(n)
         assert np.array_equal(r.x, alone.get("x")), r.rid
         assert np.array_equal(r.v, alone.get("v")), r.rid
+
+
+@pytest.mark.gpu
+def test_realtime_served_request_equals_scene_alone():
+    """The wall-clock loop on the GPU: requests arriving while a chunk runs
+    join at the next boundary through an engine prepared on a side stream
+    (continuing scenes' state copied on the device); each result equals its
+    scene stepped alone, bit for bit, and per-step latencies are reported."""
+    from implicitvelocityprojection_b200.engine import Engine
+    scs = [S.random_column(2500, 1.5, seed=51), S.small_dam_break(3000, seed=52), S.random_column(4000, 3.0, seed=53)]
+    steps = [30, 12, 20]
+    reqs = [S.Request(arrival_s=t, scene=sc, steps=n) for t, sc, n in zip((0.0, 0.005, 0.01), scs, steps)]
+    rep = Server(chunk_steps=8).run_realtime(reqs)
+    assert rep.rebuilds >= 2 and rep.summary()["steps"] >= 30
+    for r, sc, n in zip(rep.results, scs, steps):
+        assert r.status == 0 and r.steps == n
+        alone = Engine([sc])
+        alone.build()
+        alone.step(n)
+        assert np.array_equal(r.x, alone.get("x")), r.rid
+        assert np.array_equal(r.v, alone.get("v")), r.rid
