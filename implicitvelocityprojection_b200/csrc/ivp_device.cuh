@@ -200,6 +200,12 @@ struct Dev {
     float4* rip;
     float4* pip;
     float* jp;
+    // viscosity and surface-tension CG, per slot (own): the direction p and
+    // the neighbour sum of the last phase A (L(p) or S(p), carried by the
+    // recurrence L(p_k) = L(z_k) + beta L(p_(k-1)))
+    float4* vpp;
+    float4* vlp;
+    float4* stz;             // surface-tension CG: z per slot (gathered by phase A)
     float* y;
     float* s;
     float* fk;

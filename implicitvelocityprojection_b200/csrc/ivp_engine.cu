@@ -823,6 +823,9 @@ void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
     P.off[i++] = L.add(sizeof(float4) * N);                                    // 62 rip
     P.off[i++] = L.add(sizeof(float4) * N);                                    // 63 pip
     P.off[i++] = L.add(sizeof(float) * N);                                     // 64 jp
+    P.off[i++] = L.add(sizeof(float4) * N);                                    // 65 vpp
+    P.off[i++] = L.add(sizeof(float4) * N);                                    // 66 vlp
+    P.off[i++] = L.add(P.any_st ? sizeof(float4) * N : 0);                     // 67 stz
 }
 
 cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
@@ -1034,6 +1037,9 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
     D.rip = reinterpret_cast<float4*>(w + P.off[i++]);
     D.pip = reinterpret_cast<float4*>(w + P.off[i++]);
     D.jp = reinterpret_cast<float*>(w + P.off[i++]);
+    D.vpp = reinterpret_cast<float4*>(w + P.off[i++]);
+    D.vlp = reinterpret_cast<float4*>(w + P.off[i++]);
+    D.stz = reinterpret_cast<float4*>(w + P.off[i++]);
     D.drop_cap = P.drop_cap;
     e->fix_scan_blocks = P.fix_scan_blocks;
     D.n_segs = (int)P.segs.size();

@@ -1631,28 +1631,34 @@ __device__ __forceinline__ double visc_setup_tile(const Dev& D, const SceneParam
         const float3 rh = make_float3(vi.x + (-1.0f) * av.x, vi.y + (-1.0f) * av.y, vi.z + (-1.0f) * av.z);
         const float3 z = make_float3(dot3(f3(r0), rh), dot3(f3(r1), rh), dot3(f3(r2), rh));
         D.r[T.i] = make_float4(rh.x, rh.y, rh.z, 0.f);
+        // the record a neighbour gathers: {z | 1/rho} and {x}; the position
+        // half is the same in both ping-pong buffers for the whole solve
         D.cg0[2 * T.i] = make_float4(z.x, z.y, z.z, D.rflu[T.i]);
-        D.cg0[2 * T.i + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+        D.cg0[2 * T.i + 1] = make_float4(xi.x, xi.y, xi.z, 0.f);
+        D.cg1[2 * T.i + 1] = make_float4(xi.x, xi.y, xi.z, 0.f);
+        D.vpp[T.i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        D.vlp[T.i] = make_float4(0.f, 0.f, 0.f, 0.f);
         D.sol[T.i] = make_float4(0.f, 0.f, 0.f, 0.f);
         part = (double)dot3(rh, z);
     }
     return part;
 }
 
-// CG phase A (weiler18.py:332-333, 361-364): p = z + beta p_prev (formed on
-// the fly for the neighbours), A p = p - dt mu/rho L(p); partial p.Ap.
+// CG phase A (weiler18.py:332-333, 361-364): p = z + beta p_prev for the own
+// slot, A p = p - dt mu/rho L(p) with L(p) by the recurrence
+//   L(p_k) = L(z_k) + beta L(p_(k-1))
+// (exact for the linear L), so a neighbour contributes one 32-byte record
+// {z_j | 1/rho_j, x_j}; partial p.Ap.
 template <int G>
 __device__ __forceinline__ double visc_a_tile(const Dev& D, const SceneParams& P, const TileCtx& T, float beta,
                                               int it) {
-    const float4* cc = (it & 1) ? D.cg1 : D.cg0;  // {z | 1/rho, p_prev}
-    float4* cn = (it & 1) ? D.cg0 : D.cg1;
+    const float4* cc = (it & 1) ? D.cg1 : D.cg0;  // {z | 1/rho, x}
     const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
     const bool fluid = T.valid && D.rflu[T.i] != 0.0f;
-    float3 xi = make_float3(0.f, 0.f, 0.f), pi = xi;
+    float3 xi = make_float3(0.f, 0.f, 0.f), zi = xi;
     if (T.valid) {
         xi = f3(D.xm[T.i]);
-        const float4 zi = cc[2 * T.i], qi = cc[2 * T.i + 1];
-        pi = make_float3(zi.x + beta * qi.x, zi.y + beta * qi.y, zi.z + beta * qi.z);
+        zi = f3(cc[2 * T.i]);
     }
     const float eps2 = 0.01f * P.h * P.h;
     float lx = 0.0f, ly = 0.0f, lz = 0.0f;
@@ -1663,13 +1669,11 @@ __device__ __forceinline__ double visc_a_tile(const Dev& D, const SceneParams& P
         bad |= load_pairs<G>(D, T.row, xi, k0, cnt, self, P.s_begin, P.s_end, b);
 #pragma unroll
         for (int u = 0; u < PU; ++u) {
-            const int j = b.j[u];
-            const float3 xij = sub3(xi, f3(__ldg(D.xm + j)));
-            float4 zj, qj;
-            ld_rec(cc + 2 * j, zj, qj);
-            const float3 pj = make_float3(zj.x + beta * qj.x, zj.y + beta * qj.y, zj.z + beta * qj.z);
+            float4 zj, xj;
+            ld_rec(cc + 2 * b.j[u], zj, xj);
+            const float3 xij = sub3(xi, f3(xj));
             const float rsq = dot3(xij, xij);
-            const float s = (10.0f * zj.w) * __frcp_rn(rsq + eps2) * dot3(sub3(pi, pj), xij);
+            const float s = (10.0f * zj.w) * __frcp_rn(rsq + eps2) * dot3(sub3(zi, f3(zj)), xij);
             lx += s * b.J[u].x;
             ly += s * b.J[u].y;
             lz += s * b.J[u].z;
@@ -1681,12 +1685,21 @@ __device__ __forceinline__ double visc_a_tile(const Dev& D, const SceneParams& P
     lz = group_sum<G>(lz);
     double part = 0.0;
     if (T.valid && T.lane == 0) {
+        const float4 qi = D.vpp[T.i];
+        const float3 pi = make_float3(zi.x + beta * qi.x, zi.y + beta * qi.y, zi.z + beta * qi.z);
         float3 ap = pi;
         if (fluid) {
+            if (it > 0) {
+                const float4 lp = D.vlp[T.i];
+                lx = lx + beta * lp.x;
+                ly = ly + beta * lp.y;
+                lz = lz + beta * lp.z;
+            }
+            D.vlp[T.i] = make_float4(lx, ly, lz, 0.f);
             const float f = visc_factor(D, P, T.i);
             ap = make_float3(pi.x - f * lx, pi.y - f * ly, pi.z - f * lz);
         }
-        cn[2 * T.i + 1] = make_float4(pi.x, pi.y, pi.z, 0.f);
+        D.vpp[T.i] = make_float4(pi.x, pi.y, pi.z, 0.f);
         D.vap[T.i] = make_float4(ap.x, ap.y, ap.z, 0.f);
         part = (double)dot3(pi, ap);
     }
@@ -1701,8 +1714,8 @@ __device__ __forceinline__ void visc_b_tile(const Dev& D, const TileCtx& T, floa
     *part = 0.0;
     *part2 = 0.0;
     if (!(T.valid && T.lane == 0)) return;
-    float4* cn = (it & 1) ? D.cg0 : D.cg1;  // own p; receives the new z
-    const float4 p4 = cn[2 * T.i + 1], ap = D.vap[T.i];
+    float4* cn = (it & 1) ? D.cg0 : D.cg1;  // receives the new z
+    const float4 p4 = D.vpp[T.i], ap = D.vap[T.i];
     float4 x = D.sol[T.i], r = D.r[T.i];
     x.x = x.x + alpha * p4.x;
     x.y = x.y + alpha * p4.y;
@@ -1908,30 +1921,30 @@ __device__ __forceinline__ double st_setup_tile(const Dev& D, const SceneParams&
         const float3 z = make_float3(inv * rh.x, inv * rh.y, inv * rh.z);
         D.st_inv[T.i] = inv;
         D.r[T.i] = make_float4(rh.x, rh.y, rh.z, 0.f);
-        D.cg0[2 * T.i] = make_float4(z.x, z.y, z.z, 0.f);
-        D.cg0[2 * T.i + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+        D.stz[T.i] = make_float4(z.x, z.y, z.z, 0.f);
+        D.vpp[T.i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        D.vlp[T.i] = make_float4(0.f, 0.f, 0.f, 0.f);
         D.sol[T.i] = make_float4(0.f, 0.f, 0.f, 0.f);
         part = (double)dot3(rh, z);
     }
     return part;
 }
 
-// CG phase A (jeske23.py:540-545, 570-577): p = z + beta p_prev (formed on
-// the fly for the neighbours), (M p)_i = p_i + dt^2 sigma / m_i sum w_ij p_ij
-// (compute_Av_jeske23, jeske23.py:240-292); partial p.Mp.
+// CG phase A (jeske23.py:540-545, 570-577): p = z + beta p_prev for the own
+// slot, (M p)_i = p_i + dt^2 sigma / m_i S_i(p) with S_i(p) = sum w_ij p_ij
+// (compute_Av_jeske23, jeske23.py:240-292) by the recurrence
+// S(p_k) = S(z_k) + beta S(p_(k-1)) (exact for the linear S), so a neighbour
+// contributes one 16-byte z_j from a dense array; partial p.Mp.
 template <int G>
 __device__ __forceinline__ double st_a_tile(const Dev& D, const SceneParams& P, const TileCtx& T, float beta,
                                             int it) {
-    const float4* cc = (it & 1) ? D.cg1 : D.cg0;  // {z, p_prev}
-    float4* cn = (it & 1) ? D.cg0 : D.cg1;
     const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
     const bool fluid = T.valid && D.rflu[T.i] != 0.0f;
-    float3 pi = make_float3(0.f, 0.f, 0.f);
+    float3 zi = make_float3(0.f, 0.f, 0.f);
     float mi = 1.0f;
     if (T.valid) {
         mi = D.xm[T.i].w;
-        const float4 zi = cc[2 * T.i], qi = cc[2 * T.i + 1];
-        pi = make_float3(zi.x + beta * qi.x, zi.y + beta * qi.y, zi.z + beta * qi.z);
+        zi = f3(D.stz[T.i]);
     }
     float sx = 0.f, sy = 0.f, sz = 0.f;
     const int self = T.valid ? T.i : P.s_begin;
@@ -1955,14 +1968,12 @@ __device__ __forceinline__ double st_a_tile(const Dev& D, const SceneParams& P, 
 #pragma unroll
         for (int u = 0; u < PU; ++u) {
             const int j = (jj[u] >= P.s_begin && jj[u] < P.s_end) ? jj[u] : self;
-            float4 zj, qj;
-            ld_rec(cc + 2 * j, zj, qj);
-            const float3 pj = make_float3(zj.x + beta * qj.x, zj.y + beta * qj.y, zj.z + beta * qj.z);
+            const float3 zj = f3(ld_vec(D.stz + j));
             const float w = ww[u];
             if (w != 0.0f) {
-                sx += w * (pi.x - pj.x);
-                sy += w * (pi.y - pj.y);
-                sz += w * (pi.z - pj.z);
+                sx += w * (zi.x - zj.x);
+                sy += w * (zi.y - zj.y);
+                sz += w * (zi.z - zj.z);
             }
         }
     }
@@ -1971,12 +1982,21 @@ __device__ __forceinline__ double st_a_tile(const Dev& D, const SceneParams& P, 
     sz = group_sum<G>(sz);
     double part = 0.0;
     if (T.valid && T.lane == 0) {
+        const float4 qi = D.vpp[T.i];
+        const float3 pi = make_float3(zi.x + beta * qi.x, zi.y + beta * qi.y, zi.z + beta * qi.z);
         float3 ap = pi;
         if (fluid) {
+            if (it > 0) {
+                const float4 sp = D.vlp[T.i];
+                sx = sx + beta * sp.x;
+                sy = sy + beta * sp.y;
+                sz = sz + beta * sp.z;
+            }
+            D.vlp[T.i] = make_float4(sx, sy, sz, 0.f);
             const float f = P.dt * P.dt * P.st_coeff / mi;
             ap = make_float3(pi.x + f * sx, pi.y + f * sy, pi.z + f * sz);
         }
-        cn[2 * T.i + 1] = make_float4(pi.x, pi.y, pi.z, 0.f);
+        D.vpp[T.i] = make_float4(pi.x, pi.y, pi.z, 0.f);
         D.vap[T.i] = make_float4(ap.x, ap.y, ap.z, 0.f);
         part = (double)dot3(pi, ap);
     }
@@ -1991,8 +2011,7 @@ __device__ __forceinline__ void st_b_tile(const Dev& D, const TileCtx& T, float 
     *part = 0.0;
     *part2 = 0.0;
     if (!(T.valid && T.lane == 0)) return;
-    float4* cn = (it & 1) ? D.cg0 : D.cg1;  // own p; receives the new z
-    const float4 p4 = cn[2 * T.i + 1], ap = D.vap[T.i];
+    const float4 p4 = D.vpp[T.i], ap = D.vap[T.i];
     float4 x = D.sol[T.i], r = D.r[T.i];
     x.x = x.x + alpha * p4.x;
     x.y = x.y + alpha * p4.y;
@@ -2006,7 +2025,7 @@ __device__ __forceinline__ void st_b_tile(const Dev& D, const TileCtx& T, float 
     const float inv = D.st_inv[T.i];
     const float3 rr = f3(r);
     const float3 z = make_float3(inv * rr.x, inv * rr.y, inv * rr.z);
-    cn[2 * T.i] = make_float4(z.x, z.y, z.z, 0.f);
+    D.stz[T.i] = make_float4(z.x, z.y, z.z, 0.f);
     *part = (double)dot3(rr, rr);
     *part2 = (double)dot3(rr, z);
 }
