@@ -418,7 +418,7 @@ def run_ours(args, rank, world, local_rank):
     n_dyn = sum(sc.n_dynamic for sc in scenes)
     opts = EngineOptions(lanes_per_particle=args.lanes,
                          particles_per_block=args.ppb, persistent=not args.per_phase,
-                         row_format=ROW_FORMATS[args.row_format])
+                         row_format=ROW_FORMATS[args.row_format], build_kernel=args.build_kernel)
     tuning = None
     if not args.no_autotune and args.lanes == 0 and not args.per_phase:
         # launch shape timed on the actual scenes (outside the timed region)
@@ -553,10 +553,13 @@ def run_ours(args, rank, world, local_rank):
                 "dtype": "f32 (bf16 gradients)" if args.row_format == "bf16" else "f32", "data": "synthetic",
                 "config": {**workload_config(scenes, args.workload),
                            "parallelism": f"scenes sharded over {world} ranks" if sharded else f"replicas x{world}",
-                           "lanes_per_particle": lanes, "row_format": args.row_format,
+                           "lanes_per_particle": lanes,
+                           "row_format": {0: "full", 1: "full", 2: "compact", 3: "bf16"}[opts.row_format],
                            "particles_per_block": ppb,
                            "solve": "persistent cooperative kernel" if opts.persistent else "per-phase launches",
                            "launch_shape": "autotuned" if tuning else ("fixed" if args.lanes else "heuristic"),
+                           "build_kernel": {0: "thread per particle", 1: "thread per particle",
+                                            2: "warp per cell"}[args.build_kernel],
                            "timed": schedule_note(args.warmup, args.steps, run_steps)},
                 "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
                 "valid": bool(valid), "max_final_density_error": max(r.max_final_density_error for r in raws),
@@ -838,6 +841,8 @@ def main():
     ap.add_argument("--hbm-budget-gb", type=float, default=150.0, help="served: admission budget")
     ap.add_argument("--row-format", default="full", choices=sorted(ROW_FORMATS),
                     help="neighbour rows: full FP32 gradients (default), compact {j, w}, or bf16 gradients")
+    ap.add_argument("--build-kernel", type=int, default=0, choices=[0, 1, 2],
+                    help="neighbour build: 0 default, 1 one thread per particle, 2 one warp per cell")
     ap.add_argument("--no-autotune", action="store_true",
                     help="skip the launch-shape autotuner (use the engine's tile-count heuristic)")
     ap.add_argument("--shard", action="store_true",

@@ -55,7 +55,7 @@ class Options(ctypes.Structure):
         ("use_graphs", ctypes.c_int32),
         ("persistent", ctypes.c_int32),
         ("row_format", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 1),
+        ("build_kernel", ctypes.c_int32),
     ]
 
 

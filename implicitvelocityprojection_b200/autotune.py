@@ -2,7 +2,8 @@
 
 The engine's neighbour sums run G lanes per particle in CTAs of G x T
 threads (T particles per tile), either as persistent cooperative solves or as
-one launch per phase.  Which shape is fastest depends on how many tiles the
+one launch per phase, over full {J_ij, j} or compact {j, w_ij} neighbour rows
+(identical bits).  Which shape is fastest depends on how many tiles the
 scenes make per SM and on their neighbour counts, so the tuner times every
 candidate on copies of the scenes the caller will run (a few warm-up steps,
 then a few CUDA-event-timed steps each) and keeps the fastest.  Choices are
@@ -28,6 +29,10 @@ from typing import Dict, List, Optional, Sequence, Tuple
 
 # (lanes per particle, particles per CTA): 256- and 128-thread CTAs
 SHAPES: Tuple[Tuple[int, int], ...] = ((2, 128), (4, 64), (8, 32), (2, 64), (4, 32), (8, 16))
+# neighbour-row formats that give identical bits: full {J_ij, j} (16 B) and
+# compact {j, w_ij} (8 B, J rebuilt from the positions).  Full rows win while
+# the rows stay in L2; compact rows halve the row stream once they do not.
+ROW_FORMATS: Tuple[int, ...] = (1, 2)
 
 _CACHE: Dict[str, dict] = {}
 
@@ -37,10 +42,12 @@ class Trial:
     lanes_per_particle: int
     particles_per_block: int
     persistent: bool
+    row_format: int
     ms_per_step: float
 
     def label(self) -> str:
-        return f"{self.lanes_per_particle}x{self.particles_per_block}/{'persistent' if self.persistent else 'per-phase'}"
+        return (f"{self.lanes_per_particle}x{self.particles_per_block}/"
+                f"{'persistent' if self.persistent else 'per-phase'}/{'full' if self.row_format == 1 else 'compact'}")
 
 
 def signature(scenes: Sequence) -> str:
@@ -54,18 +61,20 @@ def signature(scenes: Sequence) -> str:
     return f"n{len(scenes)}-t{b(sum(nd))}-m{b(max(nd) if nd else 1)}-f{forces}"
 
 
-def candidates(persistent_too: bool = True) -> List[Tuple[int, int, bool]]:
-    out = [(g, t, True) for g, t in SHAPES]
-    if persistent_too:
-        out += [(g, t, False) for g, t in SHAPES]
+def candidates(per_phase: bool = True, row_formats: Sequence[int] = ROW_FORMATS) -> List[Tuple[int, int, bool, int]]:
+    out = []
+    for rf in row_formats:
+        out += [(g, t, True, rf) for g, t in SHAPES]
+        if per_phase:
+            out += [(g, t, False, rf) for g, t in SHAPES]
     return out
 
 
-def _time_candidate(scenes, lanes, ppb, persistent, device, warmup, steps, base_options) -> float:
+def _time_candidate(scenes, lanes, ppb, persistent, row_format, device, warmup, steps, base_options) -> float:
     import torch
     from .engine import Engine
     opts = dataclasses.replace(base_options, lanes_per_particle=lanes, particles_per_block=ppb,
-                               persistent=persistent)
+                               persistent=persistent, row_format=row_format)
     copies = [dataclasses.replace(sc, x=sc.x.copy(), v=sc.v.copy()) for sc in scenes]
     eng = Engine(copies, device=device, options=opts)
     try:
@@ -105,13 +114,15 @@ def tune(scenes: Sequence, device: str = "cuda", base_options=None, warmup: int 
                 pass
     trials: List[Trial] = []
     t0 = time.perf_counter()
-    for g, t, pers in candidates(per_phase):
-        ms = _time_candidate(scenes, g, t, pers, device, warmup, steps, base)
-        trials.append(Trial(g, t, pers, ms))
+    # a caller that fixed the row format (e.g. the bf16 variant) keeps it
+    rfs = ROW_FORMATS if base.row_format in (0, 1, 2) else (base.row_format,)
+    for g, t, pers, rf in candidates(per_phase, rfs):
+        ms = _time_candidate(scenes, g, t, pers, rf, device, warmup, steps, base)
+        trials.append(Trial(g, t, pers, rf, ms))
     best = min(trials, key=lambda tr: tr.ms_per_step)
     res = {"signature": key,
            "choice": {"lanes_per_particle": best.lanes_per_particle, "particles_per_block": best.particles_per_block,
-                      "persistent": best.persistent},
+                      "persistent": best.persistent, "row_format": best.row_format},
            "table": [{"shape": tr.label(), "ms_per_step": round(tr.ms_per_step, 4)} for tr in trials],
            "tuning_s": round(time.perf_counter() - t0, 2), "steps_timed": steps}
     _CACHE[key] = res
@@ -136,4 +147,5 @@ def tuned_options(scenes: Sequence, device: str = "cuda", base_options=None, **k
     res = tune(scenes, device=device, base_options=base, **kw)
     c = res["choice"]
     return dataclasses.replace(base, lanes_per_particle=c["lanes_per_particle"],
-                               particles_per_block=c["particles_per_block"], persistent=c["persistent"]), res
+                               particles_per_block=c["particles_per_block"], persistent=c["persistent"],
+                               row_format=c.get("row_format", base.row_format)), res

@@ -288,9 +288,7 @@ int emit_build_impl(ivp_engine* e, Launcher& L, bool with_advect) {
     }
     CKS(L.dev(IVP_K_PLACE, k_place, blocks_for(std::max(e->n_total, e->n_segs), ELEM_BLOCK), ELEM_BLOCK, D));
     CKS(L.dev(IVP_K_ORDER, k_order, blocks_for(e->n_total, ELEM_BLOCK), ELEM_BLOCK, D));
-    if (e->n_segs > 0) {
-        // cell-tiled build: one CTA per segment holding dynamic particles
-        // (k_place listed them), one warp per cell
+    if (e->n_segs > 0 && e->n_tiles > 0) {
         Dev copy = D;
         cudaGraphConditionalHandle h_fix = 0;
         if (L.graph) {
@@ -299,8 +297,16 @@ int emit_build_impl(ivp_engine* e, Launcher& L, bool with_advect) {
             copy.h_fix = (unsigned long long)h_fix;
         }
         void* args[] = {&copy};
-        CKS(L.kernel(IVP_K_NBR_BUILD, (const void*)k_nbr_build<kBuildPP>, dim3(e->n_segs), dim3(256), args,
-                     sizeof(float4) * kStageCap));
+        if (e->opt.build_kernel == 2) {
+            // cell-tiled build: one CTA per segment holding dynamic particles
+            // (k_place listed them), one warp per cell
+            CKS(L.kernel(IVP_K_NBR_BUILD, (const void*)k_nbr_build<kBuildPP>, dim3(e->n_segs), dim3(256), args,
+                         sizeof(float4) * kStageCap));
+        } else {
+            // one thread per dynamic particle, one CTA per tile
+            CKS(L.kernel(IVP_K_NBR_BUILD, (const void*)k_nbr_build_tpp, dim3(e->n_tiles), dim3(std::max(e->T, 32)),
+                         args));
+        }
         if (L.graph) {
             cudaGraph_t body;
             CKS(add_conditional(L.graph, L, h_fix, cudaGraphCondTypeIf, &body));
@@ -625,6 +631,7 @@ int validate(const ivp_scene_desc* sc, int n, const ivp_options* o) {
     }
     if (o->list_stride <= 0 || (o->list_stride & 1) || o->max_hist <= 0) return IVP_ERR_BAD_ARG;
     if (o->row_format < 0 || o->row_format > 3) return IVP_ERR_BAD_ARG;
+    if (o->build_kernel < 0 || o->build_kernel > 2) return IVP_ERR_BAD_ARG;
     long expect = 0;
     for (int s = 0; s < n; ++s) {
         const ivp_scene_desc& d = sc[s];

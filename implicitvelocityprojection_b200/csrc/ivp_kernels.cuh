@@ -730,6 +730,139 @@ __global__ void __launch_bounds__(256, 4) k_nbr_build(const Dev D) {
     if (threadIdx.x == 0 && sh_pairs) atomicAdd(&D.pairs[sc], (unsigned long long)sh_pairs);
 }
 
+// Neighbour lists, density, Aii, k, c and 1/rho of every dynamic particle,
+// one thread per particle (one CTA per tile of dynamic slots).  The thread
+// walks its 27-cell window in the same sequential candidate order as
+// k_nbr_build -- (y, z) rows with dz outer and dy inner, in each row the
+// dynamic then the static slots of the x-adjacent cells, slots ascending --
+// so it keeps the same first cache_size hits.  Two passes: the filter loop
+// only writes each kept hit's slot into the id field of its row entry, then a
+// dense pass reads them back and computes each entry's vector, density and
+// Aii terms; the filter, which runs for every candidate, stays short even
+// though the lanes of a warp hit on different iterations, and no shared
+// memory is used, which leaves L1 to the candidate positions (neighbouring
+// threads hold neighbouring slots, whose windows overlap).
+constexpr int kTppMaxThreads = 128;
+constexpr int kTppHits = 64;  // >= every cache_size (the row stride caps it)
+
+// the id field of row entry k (every row format holds one)
+__device__ __forceinline__ int* row_id_slot(const Dev& D, int row, int k) {
+    const size_t e = (size_t)row * D.stride + k;
+    if (D.row_fmt == ROW_FULL) return reinterpret_cast<int*>(D.nbr + e) + 3;
+    if (D.row_fmt == ROW_COMPACT) return reinterpret_cast<int*>(reinterpret_cast<float2*>(D.nbr) + e);
+    return reinterpret_cast<int*>(D.nbr) + e;
+}
+
+__global__ void __launch_bounds__(kTppMaxThreads) k_nbr_build_tpp(const Dev D) {
+    const int4 tile = __ldg(D.tiles + blockIdx.x);
+    const int sc = tile.x;
+    const SceneParams& P = D.scenes[sc];
+    const int i = tile.y + threadIdx.x;
+    const bool act = i < tile.z;
+    int n_hit = 0;
+    if (act) {
+        const int row = P.row_base + (i - P.s_begin);
+        const float4 xi4 = D.xm[i];
+        const float3 xi = f3(xi4);
+        const int dimx = P.dims[0];
+        const int cx = cell_coord(xi.x, P.cell_inv, dimx);
+        const int cy = cell_coord(xi.y, P.cell_inv, P.dims[1]);
+        const int cz = cell_coord(xi.z, P.cell_inv, P.dims[2]);
+        const int x0 = cx > 0 ? cx - 1 : 0, x1 = cx < dimx - 1 ? cx + 1 : dimx - 1;
+        const float r2max = P.r2_max;
+        const int cap = min(min(P.cache, D.stride), kTppHits);
+        int found = 0;
+        // filter
+        for (int dz = -1; dz <= 1; ++dz) {
+            const int z = cz + dz;
+            if (z < 0 || z >= P.dims[2]) continue;
+            for (int dy = -1; dy <= 1; ++dy) {
+                const int y = cy + dy;
+                if (y < 0 || y >= P.dims[1]) continue;
+                const int cb = (z * P.dims[1] + y) * dimx;
+#pragma unroll
+                for (int pass = 0; pass < 2; ++pass) {
+                    const int kb = P.key_base + (pass ? P.ncell : 0) + cb;
+                    const int jb = __ldg(D.cell_start + kb + x0), je = __ldg(D.cell_start + kb + x1 + 1);
+#pragma unroll 4
+                    for (int j = jb; j < je; ++j) {
+                        const float3 r = sub3(xi, f3(__ldg(D.xm + j)));
+                        if (j != i && norm2_rn(r) <= r2max) {
+                            if (found < cap) *row_id_slot(D, row, found) = j;
+                            ++found;
+                        }
+                    }
+                }
+            }
+        }
+        n_hit = min(found, cap);
+        // dense pass: the build's arithmetic for every kept hit, in order
+        const float h = P.h, inv_h = P.inv_h, spk = P.spiky_k, ck = P.cubic_k;
+        const int dyn_end = P.s_dyn_end;
+        float4* out = D.nbr + (size_t)row * D.stride;
+        float2* out2 = reinterpret_cast<float2*>(D.nbr) + (size_t)row * D.stride;
+        float rho = 0.0f, aii = 0.0f;
+        float3 jii = make_float3(0.0f, 0.0f, 0.0f);
+        for (int k = 0; k < n_hit; ++k) {
+            const int j = *row_id_slot(D, row, k);
+            const float4 xj4 = __ldg(D.xm + j);
+            const float3 r = sub3(xi, f3(xj4));
+            const float rn = sqrtf(norm2_rn(r));
+            const float rc = rn < 1e-6f ? 1e-6f : rn;
+            const float t = h - rc;
+            const float sg = -spk * (t * t);
+            const float ir = __frcp_rn(rc);
+            const float mj = xj4.w;
+            const float wgt = mj * (sg * ir);
+            const float3 J = make_float3(__fmul_rn(wgt, r.x), __fmul_rn(wgt, r.y), __fmul_rn(wgt, r.z));
+            if (D.row_fmt == ROW_FULL) {
+                out[k] = make_float4(J.x, J.y, J.z, __int_as_float(j));
+            } else if (D.row_fmt == ROW_COMPACT) {
+                out2[k] = make_float2(__int_as_float(j), wgt);
+            } else {
+                const size_t e = (size_t)row * D.stride + k;
+                reinterpret_cast<int*>(D.nbr)[e] = j;
+                unsigned short* gb = D.nbr_g + 3 * e;
+                gb[0] = bf16_bits(J.x);
+                gb[1] = bf16_bits(J.y);
+                gb[2] = bf16_bits(J.z);
+            }
+            rho += mj * cubic_Wq(rn * inv_h, ck);
+            if (j < dyn_end) aii += dot3(J, J) * __frcp_rn(mj);
+            jii = sub3(jii, J);
+        }
+        const float mi = xi4.w;
+        float dens = 0.0f;
+        dens = dens + mi * P.W0;
+        dens += rho;
+        aii += dot3(jii, jii) * __frcp_rn(mi);
+        const float kd = __frcp_rn(aii + 1e-3f);
+        D.nbr_cnt[row] = n_hit;
+        D.dens[i] = dens;
+        D.kd[i] = kd;
+        D.c[i] = dens - D.rho0s[i];
+        const int pid = D.pid[i];
+        D.rflu[i] = D.material[pid] == 1 ? __frcp_rn(dens) : 0.0f;
+        D.density_out[pid] = dens;
+        D.k_out[pid] = kd;
+        if (found > cap) {
+            atomicAdd(&D.overflow[sc], 1);
+            D.ovf_list[atomicAdd(&D.ovf_ctr[0], 1)] = i;
+            set_cond(D.h_fix, 1u);
+        }
+    }
+    // pair count of the scene (a tile never spans scenes): one atomic per CTA
+    int pairs = n_hit;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
+    __shared__ int sh_pairs;
+    if (threadIdx.x == 0) sh_pairs = 0;
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0 && pairs) atomicAdd(&sh_pairs, pairs);
+    __syncthreads();
+    if (threadIdx.x == 0 && sh_pairs) atomicAdd(&D.pairs[sc], (unsigned long long)sh_pairs);
+}
+
 // ---- neighbour-cache overflow: rows of truncated lists and the transpose
 // corrections (only when some dynamic particle has more than cache_size
 // neighbours; a graph conditional runs these kernels in that build only)

@@ -32,6 +32,7 @@ class EngineOptions:
     use_graphs: bool = True
     persistent: bool = True
     row_format: int = 0  # 0 default (full), 1 full {J, j}, 2 compact {j, w}, 3 bf16 gradients
+    build_kernel: int = 0  # 0 default (= 1), 1 thread per particle, 2 warp per cell
 
     def to_c(self) -> _lib.Options:
         o = _lib.Options()
@@ -42,6 +43,7 @@ class EngineOptions:
         o.use_graphs = int(self.use_graphs)
         o.persistent = int(self.persistent)
         o.row_format = int(self.row_format)
+        o.build_kernel = int(self.build_kernel)
         return o
 
 
