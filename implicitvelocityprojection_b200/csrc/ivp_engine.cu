@@ -304,8 +304,9 @@ int emit_build_impl(ivp_engine* e, Launcher& L, bool with_advect) {
                          sizeof(float4) * kStageCap));
         } else {
             // one thread per dynamic particle, one CTA per tile
-            CKS(L.kernel(IVP_K_NBR_BUILD, (const void*)k_nbr_build_tpp, dim3(e->n_tiles), dim3(std::max(e->T, 32)),
-                         args));
+            const int nt = std::max(e->T, 32);
+            CKS(L.kernel(IVP_K_NBR_BUILD, (const void*)k_nbr_build_tpp, dim3(e->n_tiles), dim3(nt), args,
+                         sizeof(unsigned short) * kTppHits * nt));
         }
         if (L.graph) {
             cudaGraph_t body;

@@ -736,32 +736,31 @@ __global__ void __launch_bounds__(256, 4) k_nbr_build(const Dev D) {
 // k_nbr_build -- (y, z) rows with dz outer and dy inner, in each row the
 // dynamic then the static slots of the x-adjacent cells, slots ascending --
 // so it keeps the same first cache_size hits.  Two passes: the filter loop
-// only writes each kept hit's slot into the id field of its row entry, then a
-// dense pass reads them back and computes each entry's vector, density and
-// Aii terms; the filter, which runs for every candidate, stays short even
-// though the lanes of a warp hit on different iterations, and no shared
-// memory is used, which leaves L1 to the candidate positions (neighbouring
-// threads hold neighbouring slots, whose windows overlap).
+// only appends each kept hit to the thread's list in shared memory as 16 bits
+// (which of the 18 slot ranges, and the offset in it; hit k of thread t at
+// [k * blockDim + t], conflict-free), then a dense pass rebuilds each hit's
+// slot and computes its row entry, density and Aii terms.  The filter, which
+// runs for every candidate, stays short even though the lanes of a warp hit
+// on different iterations; the small list leaves most of L1 to the candidate
+// positions that neighbouring threads (neighbouring slots) share.  A range
+// offset that does not fit the 10 bits (more than 1,023 slots in three cells
+// of one row) sets the scene's fix-up failure flag, so its IP solve stops
+// with IVP_ERR_NBR_OVERFLOW instead of using a wrong list.
 constexpr int kTppMaxThreads = 128;
 constexpr int kTppHits = 64;  // >= every cache_size (the row stride caps it)
-
-// the id field of row entry k (every row format holds one)
-__device__ __forceinline__ int* row_id_slot(const Dev& D, int row, int k) {
-    const size_t e = (size_t)row * D.stride + k;
-    if (D.row_fmt == ROW_FULL) return reinterpret_cast<int*>(D.nbr + e) + 3;
-    if (D.row_fmt == ROW_COMPACT) return reinterpret_cast<int*>(reinterpret_cast<float2*>(D.nbr) + e);
-    return reinterpret_cast<int*>(D.nbr) + e;
-}
+constexpr int kTppOffBits = 10;
 
 __global__ void __launch_bounds__(kTppMaxThreads) k_nbr_build_tpp(const Dev D) {
+    extern __shared__ unsigned short hit_q[];
+    const int nt = blockDim.x;
     const int4 tile = __ldg(D.tiles + blockIdx.x);
     const int sc = tile.x;
     const SceneParams& P = D.scenes[sc];
-    const int i = tile.y + threadIdx.x;
+    const int tid = threadIdx.x;
+    const int i = tile.y + tid;
     const bool act = i < tile.z;
     int n_hit = 0;
     if (act) {
-        const int row = P.row_base + (i - P.s_begin);
         const float4 xi4 = D.xm[i];
         const float3 xi = f3(xi4);
         const int dimx = P.dims[0];
@@ -772,39 +771,46 @@ __global__ void __launch_bounds__(kTppMaxThreads) k_nbr_build_tpp(const Dev D) {
         const float r2max = P.r2_max;
         const int cap = min(min(P.cache, D.stride), kTppHits);
         int found = 0;
+        bool too_wide = false;
         // filter
-        for (int dz = -1; dz <= 1; ++dz) {
-            const int z = cz + dz;
-            if (z < 0 || z >= P.dims[2]) continue;
-            for (int dy = -1; dy <= 1; ++dy) {
-                const int y = cy + dy;
-                if (y < 0 || y >= P.dims[1]) continue;
-                const int cb = (z * P.dims[1] + y) * dimx;
-#pragma unroll
-                for (int pass = 0; pass < 2; ++pass) {
-                    const int kb = P.key_base + (pass ? P.ncell : 0) + cb;
-                    const int jb = __ldg(D.cell_start + kb + x0), je = __ldg(D.cell_start + kb + x1 + 1);
+        for (int q = 0; q < 18; ++q) {
+            const int rr = q >> 1, pass = q & 1;
+            const int z = cz + rr / 3 - 1, y = cy + rr % 3 - 1;
+            if (z < 0 || z >= P.dims[2] || y < 0 || y >= P.dims[1]) continue;
+            const int kb = P.key_base + (pass ? P.ncell : 0) + (z * P.dims[1] + y) * dimx;
+            const int jb = __ldg(D.cell_start + kb + x0), je = __ldg(D.cell_start + kb + x1 + 1);
 #pragma unroll 4
-                    for (int j = jb; j < je; ++j) {
-                        const float3 r = sub3(xi, f3(__ldg(D.xm + j)));
-                        if (j != i && norm2_rn(r) <= r2max) {
-                            if (found < cap) *row_id_slot(D, row, found) = j;
-                            ++found;
-                        }
-                    }
+            for (int j = jb; j < je; ++j) {
+                const float3 r = sub3(xi, f3(__ldg(D.xm + j)));
+                if (j != i && norm2_rn(r) <= r2max) {
+                    const int off = j - jb;
+                    too_wide |= off >= (1 << kTppOffBits);
+                    if (found < cap) hit_q[found * nt + tid] = (unsigned short)((q << kTppOffBits) | (off & 1023));
+                    ++found;
                 }
             }
         }
         n_hit = min(found, cap);
+        if (too_wide) D.fix_fail[sc] = 1;
         // dense pass: the build's arithmetic for every kept hit, in order
         const float h = P.h, inv_h = P.inv_h, spk = P.spiky_k, ck = P.cubic_k;
         const int dyn_end = P.s_dyn_end;
+        const int row = P.row_base + (i - P.s_begin);
         float4* out = D.nbr + (size_t)row * D.stride;
         float2* out2 = reinterpret_cast<float2*>(D.nbr) + (size_t)row * D.stride;
         float rho = 0.0f, aii = 0.0f;
         float3 jii = make_float3(0.0f, 0.0f, 0.0f);
+        int q_cur = -1, jb_cur = 0;
         for (int k = 0; k < n_hit; ++k) {
-            const int j = *row_id_slot(D, row, k);
+            const unsigned hq = hit_q[k * nt + tid];
+            const int q = (int)(hq >> kTppOffBits);
+            if (q != q_cur) {  // hits come in range order: one cell-start load per range
+                q_cur = q;
+                const int rr = q >> 1, pass = q & 1;
+                const int z = cz + rr / 3 - 1, y = cy + rr % 3 - 1;
+                jb_cur = __ldg(D.cell_start + P.key_base + (pass ? P.ncell : 0) + (z * P.dims[1] + y) * dimx + x0);
+            }
+            const int j = jb_cur + (int)(hq & 1023u);
             const float4 xj4 = __ldg(D.xm + j);
             const float3 r = sub3(xi, f3(xj4));
             const float rn = sqrtf(norm2_rn(r));
