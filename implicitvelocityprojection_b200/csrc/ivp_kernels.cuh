@@ -772,27 +772,42 @@ __global__ void __launch_bounds__(kTppMaxThreads) k_nbr_build_tpp(const Dev D) {
         const int cap = min(min(P.cache, D.stride), kTppHits);
         int found = 0;
         bool too_wide = false;
-        // filter
-        for (int q = 0; q < 18; ++q) {
-            const int rr = q >> 1, pass = q & 1;
-            const int z = cz + rr / 3 - 1, y = cy + rr % 3 - 1;
-            if (z < 0 || z >= P.dims[2] || y < 0 || y >= P.dims[1]) continue;
-            const int kb = P.key_base + (pass ? P.ncell : 0) + (z * P.dims[1] + y) * dimx;
-            const int jb = __ldg(D.cell_start + kb + x0), je = __ldg(D.cell_start + kb + x1 + 1);
+        // filter, one dz plane (six slot ranges) at a time: the twelve range
+        // bounds of a plane load together, so a thread waits on three rounds
+        // of cell-start loads instead of eighteen
+        for (int dz = 0; dz < 3; ++dz) {
+            const int z = cz + dz - 1;
+            int rb[6], re[6];
+#pragma unroll
+            for (int u = 0; u < 6; ++u) {
+                const int y = cy + (u >> 1) - 1, pass = u & 1;
+                rb[u] = re[u] = 0;
+                if (z >= 0 && z < P.dims[2] && y >= 0 && y < P.dims[1]) {
+                    const int kb = P.key_base + (pass ? P.ncell : 0) + (z * P.dims[1] + y) * dimx;
+                    rb[u] = __ldg(D.cell_start + kb + x0);
+                    re[u] = __ldg(D.cell_start + kb + x1 + 1);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 6; ++u) {
+                const int q = dz * 6 + u, jb = rb[u], je = re[u];
 #pragma unroll 4
-            for (int j = jb; j < je; ++j) {
-                const float3 r = sub3(xi, f3(__ldg(D.xm + j)));
-                if (j != i && norm2_rn(r) <= r2max) {
-                    const int off = j - jb;
-                    too_wide |= off >= (1 << kTppOffBits);
-                    if (found < cap) hit_q[found * nt + tid] = (unsigned short)((q << kTppOffBits) | (off & 1023));
-                    ++found;
+                for (int j = jb; j < je; ++j) {
+                    const float3 r = sub3(xi, f3(__ldg(D.xm + j)));
+                    if (j != i && norm2_rn(r) <= r2max) {
+                        const int off = j - jb;
+                        too_wide |= off >= (1 << kTppOffBits);
+                        if (found < cap) hit_q[found * nt + tid] = (unsigned short)((q << kTppOffBits) | (off & 1023));
+                        ++found;
+                    }
                 }
             }
         }
         n_hit = min(found, cap);
         if (too_wide) D.fix_fail[sc] = 1;
-        // dense pass: the build's arithmetic for every kept hit, in order
+        // dense pass: the build's arithmetic for every kept hit, in order;
+        // two hits at a time, so their position loads are in flight together
+        // (four: 80 registers, slower on the larger scenes)
         const float h = P.h, inv_h = P.inv_h, spk = P.spiky_k, ck = P.cubic_k;
         const int dyn_end = P.s_dyn_end;
         const int row = P.row_base + (i - P.s_begin);
@@ -801,41 +816,57 @@ __global__ void __launch_bounds__(kTppMaxThreads) k_nbr_build_tpp(const Dev D) {
         float rho = 0.0f, aii = 0.0f;
         float3 jii = make_float3(0.0f, 0.0f, 0.0f);
         int q_cur = -1, jb_cur = 0;
-        for (int k = 0; k < n_hit; ++k) {
-            const unsigned hq = hit_q[k * nt + tid];
-            const int q = (int)(hq >> kTppOffBits);
-            if (q != q_cur) {  // hits come in range order: one cell-start load per range
-                q_cur = q;
-                const int rr = q >> 1, pass = q & 1;
-                const int z = cz + rr / 3 - 1, y = cy + rr % 3 - 1;
-                jb_cur = __ldg(D.cell_start + P.key_base + (pass ? P.ncell : 0) + (z * P.dims[1] + y) * dimx + x0);
+        for (int k0 = 0; k0 < n_hit; k0 += 2) {
+            int jj[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                jj[u] = i;
+                if (k0 + u < n_hit) {
+                    const unsigned hq = hit_q[(k0 + u) * nt + tid];
+                    const int q = (int)(hq >> kTppOffBits);
+                    if (q != q_cur) {  // hits come in range order: one cell-start load per range
+                        q_cur = q;
+                        const int rr = q >> 1, pass = q & 1;
+                        const int z = cz + rr / 3 - 1, y = cy + rr % 3 - 1;
+                        jb_cur = __ldg(D.cell_start + P.key_base + (pass ? P.ncell : 0) + (z * P.dims[1] + y) * dimx + x0);
+                    }
+                    jj[u] = jb_cur + (int)(hq & 1023u);
+                }
             }
-            const int j = jb_cur + (int)(hq & 1023u);
-            const float4 xj4 = __ldg(D.xm + j);
-            const float3 r = sub3(xi, f3(xj4));
-            const float rn = sqrtf(norm2_rn(r));
-            const float rc = rn < 1e-6f ? 1e-6f : rn;
-            const float t = h - rc;
-            const float sg = -spk * (t * t);
-            const float ir = __frcp_rn(rc);
-            const float mj = xj4.w;
-            const float wgt = mj * (sg * ir);
-            const float3 J = make_float3(__fmul_rn(wgt, r.x), __fmul_rn(wgt, r.y), __fmul_rn(wgt, r.z));
-            if (D.row_fmt == ROW_FULL) {
-                out[k] = make_float4(J.x, J.y, J.z, __int_as_float(j));
-            } else if (D.row_fmt == ROW_COMPACT) {
-                out2[k] = make_float2(__int_as_float(j), wgt);
-            } else {
-                const size_t e = (size_t)row * D.stride + k;
-                reinterpret_cast<int*>(D.nbr)[e] = j;
-                unsigned short* gb = D.nbr_g + 3 * e;
-                gb[0] = bf16_bits(J.x);
-                gb[1] = bf16_bits(J.y);
-                gb[2] = bf16_bits(J.z);
+            float4 xq[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) xq[u] = __ldg(D.xm + jj[u]);
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const int k = k0 + u;
+                if (k >= n_hit) break;
+                const int j = jj[u];
+                const float4 xj4 = xq[u];
+                const float3 r = sub3(xi, f3(xj4));
+                const float rn = sqrtf(norm2_rn(r));
+                const float rc = rn < 1e-6f ? 1e-6f : rn;
+                const float t = h - rc;
+                const float sg = -spk * (t * t);
+                const float ir = __frcp_rn(rc);
+                const float mj = xj4.w;
+                const float wgt = mj * (sg * ir);
+                const float3 J = make_float3(__fmul_rn(wgt, r.x), __fmul_rn(wgt, r.y), __fmul_rn(wgt, r.z));
+                if (D.row_fmt == ROW_FULL) {
+                    out[k] = make_float4(J.x, J.y, J.z, __int_as_float(j));
+                } else if (D.row_fmt == ROW_COMPACT) {
+                    out2[k] = make_float2(__int_as_float(j), wgt);
+                } else {
+                    const size_t e = (size_t)row * D.stride + k;
+                    reinterpret_cast<int*>(D.nbr)[e] = j;
+                    unsigned short* gb = D.nbr_g + 3 * e;
+                    gb[0] = bf16_bits(J.x);
+                    gb[1] = bf16_bits(J.y);
+                    gb[2] = bf16_bits(J.z);
+                }
+                rho += mj * cubic_Wq(rn * inv_h, ck);
+                if (j < dyn_end) aii += dot3(J, J) * __frcp_rn(mj);
+                jii = sub3(jii, J);
             }
-            rho += mj * cubic_Wq(rn * inv_h, ck);
-            if (j < dyn_end) aii += dot3(J, J) * __frcp_rn(mj);
-            jii = sub3(jii, J);
         }
         const float mi = xi4.w;
         float dens = 0.0f;

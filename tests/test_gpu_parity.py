@@ -186,23 +186,38 @@ def test_solve_matches_oracle_and_fp64(small):
     assert it > 0 and np.isfinite(x64).all()
 
 
+def _error_scene(workload):
+    if workload == "small_column":
+        return S.small_column()
+    if workload == "tall_column_102k":
+        return S.tall_column()
+    if workload == "dam_break_524k":
+        return S.dam_break()
+    # the largest scene of the 64-scene batch (a scene's result in the batch
+    # is bit-identical to the scene alone)
+    return max(S.batch_mix(64), key=lambda sc: sc.n_dynamic)
+
+
 @pytest.mark.parametrize("workload,row_format,bound", [("small_column", 1, 1e-3), ("small_column", 3, 0.1),
                                                        ("tall_column_102k", 1, 3e-3),
-                                                       ("tall_column_102k", 3, 0.1)])
+                                                       ("tall_column_102k", 3, 0.1),
+                                                       ("dam_break_524k", 1, 3e-3),
+                                                       ("batch64_largest", 1, 3e-3)])
 def test_cg_solution_error_vs_fp64_oracle(workload, row_format, bound, record_property):
-    """The CG solution of one outer system (the column after 40 steps, one
+    """The CG solution of one outer system (the scene after 40 steps, one
     fixed outer update) against the oracle's FP64 CG on the same system run
     for the same number of iterations: the precision error of the FP32 rows
     and of the bf16 gradients, stated per configuration (printed and recorded
     as a test property).  Against the fully converged FP64 solution both are
     about 0.25-0.6 off: the reference's CG stops once |r|^2 < tol_pcg (1e-6,
     absolute, ip.py:319) after two iterations."""
-    sc = S.small_column() if workload == "small_column" else S.tall_column()
+    sc = _error_scene(workload)
     eng = _engine([sc])
     eng.build()
     eng.step(40)
     s1 = dataclasses.replace(sc, x=eng.get("x").copy(), v=eng.get("v").copy(), max_outer_iters=1,
-                             fixed_outer_iters=True, viscosity_method=0, viscosity_coeff=0.0)
+                             fixed_outer_iters=True, viscosity_method=0, viscosity_coeff=0.0,
+                             surface_tension_method=0, surface_tension_coeff=0.0)
     dyn = sc.is_dynamic == 1
     st = O.State.from_scene(s1)
     st.rebuild()
