@@ -532,7 +532,7 @@ def run_ours(args, rank, world, local_rank):
             "step": {"algorithmic_bytes": step_bytes, "achieved": step_gbs, "frac_of_measured": step_gbs / peak,
                      "frac_of_nominal": step_gbs / 8000.0, "nominal_gbs": 8000.0},
             "kernels_ms_per_step": {k: round(v[0] / n_prof, 4) for k, v in prof.items()}}
-    lanes, ppb = eng.lanes_per_particle, eng.particles_per_block
+    lanes, ppb, build_kernel = eng.lanes_per_particle, eng.particles_per_block, eng.build_kernel
     del eng
     torch.cuda.synchronize()
 
@@ -558,8 +558,7 @@ def run_ours(args, rank, world, local_rank):
                            "particles_per_block": ppb,
                            "solve": "persistent cooperative kernel" if opts.persistent else "per-phase launches",
                            "launch_shape": "autotuned" if tuning else ("fixed" if args.lanes else "heuristic"),
-                           "build_kernel": {0: "thread per particle", 1: "thread per particle",
-                                            2: "warp per cell"}[args.build_kernel],
+                           "build_kernel": {1: "thread per particle", 2: "warp per cell"}[build_kernel],
                            "timed": schedule_note(args.warmup, args.steps, run_steps)},
                 "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
                 "valid": bool(valid), "max_final_density_error": max(r.max_final_density_error for r in raws),
@@ -671,14 +670,16 @@ def bf16_verdict(line, fp32_ms) -> dict:
     """The bf16-gradient variant is accepted only where it meets the FP32
     form's tolerances and is not slower: every step valid (density error below
     densityErrorTol, as `valid` checks), its CG solution within the FP32 rows'
-    bound of 1e-3 of the FP64 CG oracle at equal iterations
-    (test_cg_solution_error_vs_fp64_oracle measures 1-3e-2 for bf16
-    gradients), and a step time at most the FP32 rows' on the same schedule
-    (timed here)."""
+    bound of the FP64 CG oracle at equal iterations (1e-3 on the 8,192-particle
+    column, 3e-3 on the 102,400-particle column), and a step time at most the
+    FP32 rows' on the same schedule (timed here).
+    test_cg_solution_error_vs_fp64_oracle measures 1.4e-2 and 7.6e-3 for bf16
+    gradients on the two columns (FP32 rows: 2.9e-4 and 2.5e-5)."""
     slower = line["ms_per_step"] > fp32_ms
-    error_within_fp32_bound = False  # 1-3e-2 measured by the test, against 1e-3
+    error_within_fp32_bound = False  # measured by the test, see above
     accepted = bool(line.get("valid")) and error_within_fp32_bound and not slower
-    reasons = ["CG solution error vs the FP64 oracle 1-3e-2 against the FP32 bound 1e-3"]
+    reasons = ["CG solution error vs the FP64 oracle 7.6e-3 (102,400-particle column) and 1.4e-2 "
+               "(8,192) against the FP32 rows' bounds 3e-3 and 1e-3 (FP32 rows: 2.5e-5 and 2.9e-4)"]
     if slower:
         reasons.append(f"slower than FP32 rows ({line['ms_per_step']:.3f} vs {fp32_ms:.3f} ms/step)")
     return {"accepted": accepted, "verdict": "accepted" if accepted else "rejected", "reasons": reasons,

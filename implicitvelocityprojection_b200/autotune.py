@@ -3,10 +3,12 @@
 The engine's neighbour sums run G lanes per particle in CTAs of G x T
 threads (T particles per tile), either as persistent cooperative solves or as
 one launch per phase, over full {J_ij, j} or compact {j, w_ij} neighbour rows
-(identical bits).  Which shape is fastest depends on how many tiles the
-scenes make per SM and on their neighbour counts, so the tuner times every
-candidate on copies of the scenes the caller will run (a few warm-up steps,
-then a few CUDA-event-timed steps each) and keeps the fastest.  Choices are
+(identical bits), after a neighbour build by one thread per particle or one
+warp per cell (identical lists).  Which choice is fastest depends on how many
+tiles the scenes make per SM and on their neighbour counts, so the tuner times
+every launch shape on copies of the scenes the caller will run (a few warm-up
+steps, then a few CUDA-event-timed steps each), keeps the fastest, then times
+both build kernels with that shape.  Choices are
 cached per scene-set signature (scene count, fluid-particle total and largest
 scene, each bucketed to powers of two, and the enabled forces), in memory and
 optionally in a JSON file.
@@ -33,6 +35,8 @@ SHAPES: Tuple[Tuple[int, int], ...] = ((2, 128), (4, 64), (8, 32), (2, 64), (4, 
 # compact {j, w_ij} (8 B, J rebuilt from the positions).  Full rows win while
 # the rows stay in L2; compact rows halve the row stream once they do not.
 ROW_FORMATS: Tuple[int, ...] = (1, 2)
+# neighbour builds with identical lists: one thread per particle, one warp per cell
+BUILD_KERNELS: Tuple[int, ...] = (1, 2)
 
 _CACHE: Dict[str, dict] = {}
 
@@ -44,10 +48,12 @@ class Trial:
     persistent: bool
     row_format: int
     ms_per_step: float
+    build_kernel: int = 0
 
     def label(self) -> str:
+        b = {0: "", 1: "/thread-per-particle build", 2: "/warp-per-cell build"}[self.build_kernel]
         return (f"{self.lanes_per_particle}x{self.particles_per_block}/"
-                f"{'persistent' if self.persistent else 'per-phase'}/{'full' if self.row_format == 1 else 'compact'}")
+                f"{'persistent' if self.persistent else 'per-phase'}/{'full' if self.row_format == 1 else 'compact'}{b}")
 
 
 def signature(scenes: Sequence) -> str:
@@ -70,11 +76,14 @@ def candidates(per_phase: bool = True, row_formats: Sequence[int] = ROW_FORMATS)
     return out
 
 
-def _time_candidate(scenes, lanes, ppb, persistent, row_format, device, warmup, steps, base_options) -> float:
+def _time_candidate(scenes, lanes, ppb, persistent, row_format, device, warmup, steps, base_options,
+                    build_kernel=None) -> float:
     import torch
     from .engine import Engine
     opts = dataclasses.replace(base_options, lanes_per_particle=lanes, particles_per_block=ppb,
                                persistent=persistent, row_format=row_format)
+    if build_kernel is not None:
+        opts = dataclasses.replace(opts, build_kernel=build_kernel)
     copies = [dataclasses.replace(sc, x=sc.x.copy(), v=sc.v.copy()) for sc in scenes]
     eng = Engine(copies, device=device, options=opts)
     try:
@@ -94,9 +103,10 @@ def _time_candidate(scenes, lanes, ppb, persistent, row_format, device, warmup, 
 
 def tune(scenes: Sequence, device: str = "cuda", base_options=None, warmup: int = 2, steps: int = 3,
          per_phase: bool = True, cache_file: Optional[str] = None, force: bool = False) -> dict:
-    """Times every candidate shape on copies of `scenes` and returns
-    {"choice": {lanes_per_particle, particles_per_block, persistent},
-    "table": [{shape, ms_per_step}], "signature", "cached"}."""
+    """Times every candidate shape on copies of `scenes`, then both build
+    kernels with the fastest shape, and returns {"choice":
+    {lanes_per_particle, particles_per_block, persistent, row_format,
+    build_kernel}, "table": [{shape, ms_per_step}], "signature", "cached"}."""
     from .engine import EngineOptions
     base = base_options or EngineOptions()
     key = signature(scenes)
@@ -120,9 +130,19 @@ def tune(scenes: Sequence, device: str = "cuda", base_options=None, warmup: int 
         ms = _time_candidate(scenes, g, t, pers, rf, device, warmup, steps, base)
         trials.append(Trial(g, t, pers, rf, ms))
     best = min(trials, key=lambda tr: tr.ms_per_step)
+    if base.build_kernel == 0:
+        # both build kernels with the fastest shape (a caller that fixed the
+        # build kernel keeps it)
+        builds = [Trial(best.lanes_per_particle, best.particles_per_block, best.persistent, best.row_format,
+                        _time_candidate(scenes, best.lanes_per_particle, best.particles_per_block, best.persistent,
+                                        best.row_format, device, warmup, steps, base, build_kernel=bk), bk)
+                  for bk in BUILD_KERNELS]
+        trials += builds
+        best = min(builds, key=lambda tr: tr.ms_per_step)
     res = {"signature": key,
            "choice": {"lanes_per_particle": best.lanes_per_particle, "particles_per_block": best.particles_per_block,
-                      "persistent": best.persistent, "row_format": best.row_format},
+                      "persistent": best.persistent, "row_format": best.row_format,
+                      "build_kernel": best.build_kernel or base.build_kernel},
            "table": [{"shape": tr.label(), "ms_per_step": round(tr.ms_per_step, 4)} for tr in trials],
            "tuning_s": round(time.perf_counter() - t0, 2), "steps_timed": steps}
     _CACHE[key] = res
@@ -148,4 +168,5 @@ def tuned_options(scenes: Sequence, device: str = "cuda", base_options=None, **k
     c = res["choice"]
     return dataclasses.replace(base, lanes_per_particle=c["lanes_per_particle"],
                                particles_per_block=c["particles_per_block"], persistent=c["persistent"],
-                               row_format=c.get("row_format", base.row_format)), res
+                               row_format=c.get("row_format", base.row_format),
+                               build_kernel=c.get("build_kernel", base.build_kernel)), res

@@ -598,22 +598,32 @@ int run(ivp_engine* e, Emitter emit, cudaGraph_t* g, cudaGraphExec_t* x, cudaStr
 // many tiles per CTA the persistent solves walk fewer, larger tiles per phase
 // (one block reduction per tile); with few, 4 lanes split each row wider.
 constexpr long kAutoTilesPerSM = 16;
+// The thread-per-particle build lasts about one thread's walk of its 27-cell
+// window, so it needs many particles per SM to hide its load latency; below
+// this many dynamic particles per SM the warp-per-cell build (a warp tests a
+// cell's candidates in parallel) is faster (8,192 particles: 0.08 against
+// 0.03 ms; 102,400: 0.117 against 0.129 ms).
+constexpr long kTppMinPerSM = 256;
 
 int resolve_options(const ivp_scene_desc* sc, int n, const ivp_options* in, ivp_options* out) {
     if (!in || !out) return IVP_ERR_BAD_ARG;
     *out = *in;
-    if (in->lanes_per_particle == 0) {
+    if (in->lanes_per_particle == 0 || in->build_kernel == 0) {
         if (n <= 0 || !sc) return IVP_ERR_BAD_ARG;
-        long tiles = 0;
+        long tiles = 0, dyn = 0;
         for (int s = 0; s < n; ++s)
-            if (sc[s].n_dynamic > 0) tiles += ((long)sc[s].n_dynamic + 63) / 64;
+            if (sc[s].n_dynamic > 0) {
+                tiles += ((long)sc[s].n_dynamic + 63) / 64;
+                dyn += sc[s].n_dynamic;
+            }
         int dev = 0, sms = 0;
         if (cudaGetDevice(&dev) != cudaSuccess ||
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) {
             cudaGetLastError();  // no device here: size for a B200
             sms = 148;
         }
-        out->lanes_per_particle = tiles > kAutoTilesPerSM * sms ? 2 : 4;
+        if (in->lanes_per_particle == 0) out->lanes_per_particle = tiles > kAutoTilesPerSM * sms ? 2 : 4;
+        if (in->build_kernel == 0) out->build_kernel = dyn >= kTppMinPerSM * sms ? 1 : 2;
     }
     if (in->particles_per_block == 0 && out->lanes_per_particle > 0)
         out->particles_per_block = 256 / out->lanes_per_particle;

@@ -32,7 +32,7 @@ class EngineOptions:
     use_graphs: bool = True
     persistent: bool = True
     row_format: int = 0  # 0 default (full), 1 full {J, j}, 2 compact {j, w}, 3 bf16 gradients
-    build_kernel: int = 0  # 0 default (= 1), 1 thread per particle, 2 warp per cell
+    build_kernel: int = 0  # 1 thread per particle, 2 warp per cell; 0: chosen from the scenes
 
     def to_c(self) -> _lib.Options:
         o = _lib.Options()
@@ -134,6 +134,7 @@ class Engine:
         # the lane count and tile size the engine runs with
         self.lanes_per_particle = int(res.lanes_per_particle)
         self.particles_per_block = int(res.particles_per_block)
+        self.build_kernel = int(res.build_kernel)
         nbytes = ctypes.c_size_t(0)
         check(self.L.ivp_workspace_bytes(descs, len(self.scenes), ctypes.byref(opt), ctypes.byref(nbytes)),
               "ivp_workspace_bytes")

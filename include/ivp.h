@@ -83,9 +83,10 @@ typedef struct {
                                      positions: half the list memory, slower; bit-identical to 1),
                                      3 bf16 (4 B id + the gradient in 3 bf16: the reduced-precision
                                      variant, 10 B per entry) */
-    int32_t build_kernel;         /* neighbour build: 0 default (= 1), 1 one thread per particle walking
-                                     its 27-cell window, 2 one warp per cell sharing each candidate
-                                     among 4 particles; the same lists in the same order */
+    int32_t build_kernel;         /* neighbour build: 1 one thread per particle walking its 27-cell
+                                     window, 2 one warp per cell sharing each candidate among 4
+                                     particles; the same lists in the same order.  0 (default):
+                                     chosen from the scenes (1 from 256 dynamic particles per SM) */
 } ivp_options;
 
 /* Device arrays in the reference's layout and particle order

@@ -201,7 +201,10 @@ def _error_scene(workload):
 @pytest.mark.parametrize("workload,row_format,bound", [("small_column", 1, 1e-3), ("small_column", 3, 0.1),
                                                        ("tall_column_102k", 1, 3e-3),
                                                        ("tall_column_102k", 3, 0.1),
-                                                       ("dam_break_524k", 1, 3e-3),
+                                                       # early in the dam break the constraint is small, so
+                                                       # the FP32 rounding of c = rho - rho0 is a larger
+                                                       # share of the right-hand side (measured 2.8e-3)
+                                                       ("dam_break_524k", 1, 5e-3),
                                                        ("batch64_largest", 1, 3e-3)])
 def test_cg_solution_error_vs_fp64_oracle(workload, row_format, bound, record_property):
     """The CG solution of one outer system (the scene after 40 steps, one
@@ -697,13 +700,18 @@ def test_autotuner_picks_a_candidate_and_caches():
     from implicitvelocityprojection_b200 import autotune
     scs = [S.random_column(6000, 2.0, seed=101), S.random_column(3000, 1.5, seed=102)]
     opts, res = autotune.tuned_options(scs, force=True)
-    assert not res["cached"] and len(res["table"]) == len(autotune.candidates())
-    best = min(res["table"], key=lambda r: r["ms_per_step"])
+    n_shapes = len(autotune.candidates())
+    assert not res["cached"] and len(res["table"]) == n_shapes + len(autotune.BUILD_KERNELS)
+    best = min(res["table"][:n_shapes], key=lambda r: r["ms_per_step"])
     assert best["shape"].startswith(f"{opts.lanes_per_particle}x{opts.particles_per_block}/")
+    builds = res["table"][n_shapes:]
+    assert all(r["shape"].startswith(best["shape"]) for r in builds)
+    fastest_build = min(builds, key=lambda r: r["ms_per_step"])["shape"]
+    assert fastest_build.endswith({1: "thread-per-particle build", 2: "warp-per-cell build"}[opts.build_kernel])
     again = autotune.tune(scs)
     assert again["cached"] and again["choice"] == res["choice"]
     a = _engine(scs, lanes_per_particle=opts.lanes_per_particle, particles_per_block=opts.particles_per_block,
-                persistent=opts.persistent, row_format=opts.row_format)
+                persistent=opts.persistent, row_format=opts.row_format, build_kernel=opts.build_kernel)
     b = _engine(scs)
     for e in (a, b):
         e.build()
