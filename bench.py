@@ -843,7 +843,7 @@ def main():
     ap.add_argument("--row-format", default="full", choices=sorted(ROW_FORMATS),
                     help="neighbour rows: full FP32 gradients (default), compact {j, w}, or bf16 gradients")
     ap.add_argument("--build-kernel", type=int, default=0, choices=[0, 1, 2],
-                    help="neighbour build: 0 default, 1 one thread per particle, 2 one warp per cell")
+                    help="neighbour build: 0 chosen from the scenes, 1 one thread per particle, 2 one warp per cell")
     ap.add_argument("--no-autotune", action="store_true",
                     help="skip the launch-shape autotuner (use the engine's tile-count heuristic)")
     ap.add_argument("--shard", action="store_true",

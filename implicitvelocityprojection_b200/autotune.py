@@ -8,7 +8,7 @@ warp per cell (identical lists).  Which choice is fastest depends on how many
 tiles the scenes make per SM and on their neighbour counts, so the tuner times
 every launch shape on copies of the scenes the caller will run (a few warm-up
 steps, then a few CUDA-event-timed steps each), keeps the fastest, then times
-both build kernels with that shape.  Choices are
+both build kernels with that shape over ten builds each.  Choices are
 cached per scene-set signature (scene count, fluid-particle total and largest
 scene, each bucketed to powers of two, and the enabled forces), in memory and
 optionally in a JSON file.
@@ -37,6 +37,7 @@ SHAPES: Tuple[Tuple[int, int], ...] = ((2, 128), (4, 64), (8, 32), (2, 64), (4, 
 ROW_FORMATS: Tuple[int, ...] = (1, 2)
 # neighbour builds with identical lists: one thread per particle, one warp per cell
 BUILD_KERNELS: Tuple[int, ...] = (1, 2)
+BUILD_REPS = 10
 
 _CACHE: Dict[str, dict] = {}
 
@@ -101,12 +102,41 @@ def _time_candidate(scenes, lanes, ppb, persistent, row_format, device, warmup, 
         eng.close()
 
 
+def _time_build(scenes, lanes, ppb, persistent, row_format, build_kernel, device, warmup, reps,
+                base_options) -> float:
+    """Milliseconds per neighbour build (ivp_neighbour_build: cell sort, lists,
+    density and Aii) of copies of `scenes` with the given build kernel.  The
+    two build kernels differ by a few percent of a step, less than the noise
+    of a few timed steps, so the builds are timed on their own."""
+    import torch
+    from .engine import Engine
+    opts = dataclasses.replace(base_options, lanes_per_particle=lanes, particles_per_block=ppb,
+                               persistent=persistent, row_format=row_format, build_kernel=build_kernel)
+    copies = [dataclasses.replace(sc, x=sc.x.copy(), v=sc.v.copy()) for sc in scenes]
+    eng = Engine(copies, device=device, options=opts)
+    try:
+        for _ in range(max(warmup, 1)):
+            eng.build()
+        stream = torch.cuda.current_stream()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        for _ in range(reps):
+            eng.build()
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b) / reps
+    finally:
+        eng.close()
+
+
 def tune(scenes: Sequence, device: str = "cuda", base_options=None, warmup: int = 2, steps: int = 3,
          per_phase: bool = True, cache_file: Optional[str] = None, force: bool = False) -> dict:
     """Times every candidate shape on copies of `scenes`, then both build
     kernels with the fastest shape, and returns {"choice":
     {lanes_per_particle, particles_per_block, persistent, row_format,
-    build_kernel}, "table": [{shape, ms_per_step}], "signature", "cached"}."""
+    build_kernel}, "table": [{shape, ms_per_step}], "build_ms", "signature",
+    "cached"}."""
     from .engine import EngineOptions
     base = base_options or EngineOptions()
     key = signature(scenes)
@@ -130,20 +160,21 @@ def tune(scenes: Sequence, device: str = "cuda", base_options=None, warmup: int 
         ms = _time_candidate(scenes, g, t, pers, rf, device, warmup, steps, base)
         trials.append(Trial(g, t, pers, rf, ms))
     best = min(trials, key=lambda tr: tr.ms_per_step)
+    build_ms = None
     if base.build_kernel == 0:
-        # both build kernels with the fastest shape (a caller that fixed the
-        # build kernel keeps it)
-        builds = [Trial(best.lanes_per_particle, best.particles_per_block, best.persistent, best.row_format,
-                        _time_candidate(scenes, best.lanes_per_particle, best.particles_per_block, best.persistent,
-                                        best.row_format, device, warmup, steps, base, build_kernel=bk), bk)
-                  for bk in BUILD_KERNELS]
-        trials += builds
-        best = min(builds, key=lambda tr: tr.ms_per_step)
+        # both build kernels with the fastest shape, timed as builds (a caller
+        # that fixed the build kernel keeps it)
+        build_ms = {bk: _time_build(scenes, best.lanes_per_particle, best.particles_per_block, best.persistent,
+                                    best.row_format, bk, device, warmup, BUILD_REPS, base)
+                    for bk in BUILD_KERNELS}
+        best = dataclasses.replace(best, build_kernel=min(build_ms, key=build_ms.get))
     res = {"signature": key,
            "choice": {"lanes_per_particle": best.lanes_per_particle, "particles_per_block": best.particles_per_block,
                       "persistent": best.persistent, "row_format": best.row_format,
                       "build_kernel": best.build_kernel or base.build_kernel},
            "table": [{"shape": tr.label(), "ms_per_step": round(tr.ms_per_step, 4)} for tr in trials],
+           "build_ms": None if build_ms is None else
+           {{1: "thread per particle", 2: "warp per cell"}[bk]: round(ms, 4) for bk, ms in build_ms.items()},
            "tuning_s": round(time.perf_counter() - t0, 2), "steps_timed": steps}
     _CACHE[key] = res
     if cache_file:

@@ -1477,6 +1477,10 @@ __device__ __forceinline__ TileCtx tile_ctx(const Dev& D, int t) {
     return c;
 }
 
+// L1 prefetch of a slot's own values that a tile body reads only after its
+// neighbour sum, so that read finds them in L1 instead of waiting on L2.
+__device__ __forceinline__ void pf_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
 // ---- per-tile bodies (return this thread's contribution to the FP64 partial)
 
 // ip_pack_fused (ip.py:124-171) + coef_wise_div + the average density error
@@ -1491,6 +1495,12 @@ __device__ __forceinline__ double pack_tile(const Dev& D, const SceneParams& P, 
     // after an update the displacement is d - sol, which rhs and every CG-B
     // stored per slot in D.e (one gather per neighbour instead of two)
     const float4* dsrc = upd ? D.e : src;
+    if (T.valid && T.lane == 0) {
+        pf_l1(D.c + T.i);
+        pf_l1(D.kd + T.i);
+        pf_l1(D.inv_m + T.i);
+        pf_l1(D.rho0s + T.i);
+    }
     const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
     float3 xi = make_float3(0.f, 0.f, 0.f), di = xi;
     if (T.valid) {
@@ -1585,6 +1595,12 @@ __device__ __forceinline__ double rhs_tile(const Dev& D, const SceneParams& P, c
 template <int G>
 __device__ __forceinline__ double cga_tile(const Dev& D, const SceneParams& P, const TileCtx& T, float beta,
                                            int cg_it) {
+    if (T.valid && T.lane == 0) {
+        pf_l1(D.pip + T.i);
+        pf_l1(D.jp + T.i);
+        pf_l1(D.s + T.i);
+        pf_l1(D.inv_m + T.i);
+    }
     const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
     float3 xi = make_float3(0.f, 0.f, 0.f), ri = xi;
     if (T.valid) {
@@ -1641,6 +1657,12 @@ __device__ __noinline__ float3 ovf_correction(const int* __restrict__ fix_off, c
 template <int G>
 __device__ __forceinline__ double cgb_tile(const Dev& D, const SceneParams& P, const TileCtx& T, float alpha,
                                            int cg_it, const float4* __restrict__ dcur) {
+    if (T.valid && T.lane == 0) {
+        pf_l1(D.pip + T.i);
+        pf_l1(D.sol + T.i);
+        pf_l1(D.rip + T.i);
+        pf_l1(dcur + T.i);
+    }
     const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
     float3 xi = make_float3(0.f, 0.f, 0.f);
     float mi = 0.0f, yi = 0.0f;
@@ -2826,9 +2848,25 @@ struct Phaser {
         for (int a = blockIdx.x; a < A; a += gridDim.x) {
             while (a >= act_sh[sc + 1]) ++sc;
             const int t = tb_sh[sc] + (a - act_sh[sc]);
-            const TileCtx T = tile_ctx<G>(D, t);
+            const SceneParams& P = D.scenes[sc];
+            TileCtx T;
+            {
+                // the context computed from the scene's layout instead of
+                // loaded (one dependent load less per tile): the engine cuts
+                // each scene's dynamic slots into tiles of TS particles in
+                // order, tile k holding slots s_begin + k TS .. min(s_begin +
+                // (k + 1) TS, s_dyn_end) and rows row_base + k TS ..
+                constexpr int TS = BLOCK / G;
+                const int b = (t - tb_sh[sc]) * TS;
+                T.tile = make_int4(sc, P.s_begin + b, min(P.s_begin + b + TS, P.s_dyn_end), P.row_base + b);
+                T.sc = sc;
+                T.g = threadIdx.x / G;
+                T.lane = threadIdx.x % G;
+                T.i = T.tile.y + T.g;
+                T.row = T.tile.w + T.g;
+                T.valid = T.i < T.tile.z;
+            }
             const SceneCtl& C = sc_sh[T.sc];
-            const SceneParams& P = D.scenes[T.sc];
             double part = 0.0, part2 = 0.0;
             if constexpr (MODE == MODE_FORCE + FORCE_ST) {
                 if (kind == K_ST_DIV) {

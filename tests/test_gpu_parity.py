@@ -700,14 +700,12 @@ def test_autotuner_picks_a_candidate_and_caches():
     from implicitvelocityprojection_b200 import autotune
     scs = [S.random_column(6000, 2.0, seed=101), S.random_column(3000, 1.5, seed=102)]
     opts, res = autotune.tuned_options(scs, force=True)
-    n_shapes = len(autotune.candidates())
-    assert not res["cached"] and len(res["table"]) == n_shapes + len(autotune.BUILD_KERNELS)
-    best = min(res["table"][:n_shapes], key=lambda r: r["ms_per_step"])
+    assert not res["cached"] and len(res["table"]) == len(autotune.candidates())
+    best = min(res["table"], key=lambda r: r["ms_per_step"])
     assert best["shape"].startswith(f"{opts.lanes_per_particle}x{opts.particles_per_block}/")
-    builds = res["table"][n_shapes:]
-    assert all(r["shape"].startswith(best["shape"]) for r in builds)
-    fastest_build = min(builds, key=lambda r: r["ms_per_step"])["shape"]
-    assert fastest_build.endswith({1: "thread-per-particle build", 2: "warp-per-cell build"}[opts.build_kernel])
+    bm = res["build_ms"]
+    assert set(bm) == {"thread per particle", "warp per cell"} and all(v > 0 for v in bm.values())
+    assert {1: "thread per particle", 2: "warp per cell"}[opts.build_kernel] == min(bm, key=bm.get)
     again = autotune.tune(scs)
     assert again["cached"] and again["choice"] == res["choice"]
     a = _engine(scs, lanes_per_particle=opts.lanes_per_particle, particles_per_block=opts.particles_per_block,
