@@ -287,12 +287,14 @@ def load_peaks():
 
 
 def load_traffic(kernel: str, workload: str):
-    """DRAM bytes per launch of `kernel` on `workload`, from the ncu summaries
-    under profiles/ (a line `traffic kernel=K workload=W dram_bytes_per_launch=B`)."""
+    """DRAM bytes per launch of `kernel` on `workload` from the ncu summaries
+    under profiles/ (a line `traffic kernel=K workload=W
+    dram_bytes_per_launch=B [algorithmic_bytes=A]`), and the algorithmic
+    bytes of the captured launch when the line states them."""
     d = os.path.join(REPO, "profiles")
     if not os.path.isdir(d):
-        return None
-    pat = re.compile(r"traffic kernel=(\S+) workload=(\S+) dram_bytes_per_launch=(\d+)")
+        return None, None
+    pat = re.compile(r"traffic kernel=(\S+) workload=(\S+) dram_bytes_per_launch=(\d+)(?: algorithmic_bytes=(\d+))?")
     for name in sorted(os.listdir(d)):
         if not name.endswith(".md"):
             continue
@@ -300,8 +302,25 @@ def load_traffic(kernel: str, workload: str):
             for line in f:
                 m = pat.search(line)
                 if m and m.group(1) == kernel and m.group(2) == workload:
-                    return float(m.group(3))
-    return None
+                    return float(m.group(3)), (float(m.group(4)) if m.group(4) else None)
+    return None, None
+
+
+def traffic_for(kernel: str, workload: str, alg_bytes: float) -> dict:
+    """`roofline.traffic` for a launch of `alg_bytes` algorithmic bytes: the
+    captured launch's DRAM bytes, scaled by alg_bytes / (its algorithmic
+    bytes) when the summary states them.  A summary states them only where
+    the rows exceed L2, so that every pass streams them from DRAM and DRAM
+    bytes grow with the passes as the algorithmic bytes do; where the rows
+    stay in L2 the DRAM bytes of a launch hardly depend on its iteration
+    counts and are reported unscaled."""
+    dram, alg = load_traffic(kernel, workload)
+    if dram is None:
+        return {"traffic": None}
+    if not alg:
+        return {"traffic": dram, "traffic_note": "DRAM bytes of the captured launch, unscaled"}
+    return {"traffic": dram * alg_bytes / alg, "traffic_captured": dram, "traffic_captured_algorithmic": alg,
+            "traffic_note": "DRAM bytes of the captured launch scaled by this launch's algorithmic bytes"}
 
 
 # ----------------------------------------------------------------- arms
@@ -525,7 +544,7 @@ def run_ours(args, rank, world, local_rank):
     step_s = total_ms / args.steps / 1000.0
     step_gbs = step_bytes / step_s / 1e9 if step_s > 0 else 0.0
     roof = {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_kind": peak_kind, "traffic": load_traffic(dom_name, args.workload),
+            "frac": achieved / peak, "peak_kind": peak_kind, **traffic_for(dom_name, args.workload, alg),
             "algorithmic_bytes_per_launch": alg, "avg_launch_us": avg_s * 1e6,
             "share_of_step": dom_ms / sum(v[0] for v in prof.values()),
             "measured_on": f"{n_prof} host-driven steps at the end of the run, CUDA events around each launch",

@@ -107,7 +107,8 @@ def _time_build(scenes, lanes, ppb, persistent, row_format, build_kernel, device
     """Milliseconds per neighbour build (ivp_neighbour_build: cell sort, lists,
     density and Aii) of copies of `scenes` with the given build kernel.  The
     two build kernels differ by a few percent of a step, less than the noise
-    of a few timed steps, so the builds are timed on their own."""
+    of a few timed steps, so the builds are timed on their own, each after an
+    L2 flush (as a build inside a step finds little of its data in L2)."""
     import torch
     from .engine import Engine
     opts = dataclasses.replace(base_options, lanes_per_particle=lanes, particles_per_block=ppb,
@@ -118,14 +119,16 @@ def _time_build(scenes, lanes, ppb, persistent, row_format, build_kernel, device
         for _ in range(max(warmup, 1)):
             eng.build()
         stream = torch.cuda.current_stream()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
         torch.cuda.synchronize()
-        a.record(stream)
-        for _ in range(reps):
+        for a, b in ev:
+            flush.fill_(1)
+            a.record(stream)
             eng.build()
-        b.record(stream)
-        b.synchronize()
-        return a.elapsed_time(b) / reps
+            b.record(stream)
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in ev) / reps
     finally:
         eng.close()
 
