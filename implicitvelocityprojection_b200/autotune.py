@@ -8,7 +8,8 @@ warp per cell (identical lists).  Which choice is fastest depends on how many
 tiles the scenes make per SM and on their neighbour counts, so the tuner times
 every launch shape on copies of the scenes the caller will run (a few warm-up
 steps, then a few CUDA-event-timed steps each), keeps the fastest, then times
-both build kernels with that shape over ten builds each.  Choices are
+both build kernels with that shape, each build launch timed on its own
+inside five host-driven steps.  Choices are
 cached per scene-set signature (scene count, fluid-particle total and largest
 scene, each bucketed to powers of two, and the enabled forces), in memory and
 optionally in a JSON file.
@@ -37,7 +38,7 @@ SHAPES: Tuple[Tuple[int, int], ...] = ((2, 128), (4, 64), (8, 32), (2, 64), (4, 
 ROW_FORMATS: Tuple[int, ...] = (1, 2)
 # neighbour builds with identical lists: one thread per particle, one warp per cell
 BUILD_KERNELS: Tuple[int, ...] = (1, 2)
-BUILD_REPS = 10
+BUILD_REPS = 5
 
 _CACHE: Dict[str, dict] = {}
 
@@ -104,31 +105,22 @@ def _time_candidate(scenes, lanes, ppb, persistent, row_format, device, warmup, 
 
 def _time_build(scenes, lanes, ppb, persistent, row_format, build_kernel, device, warmup, reps,
                 base_options) -> float:
-    """Milliseconds per neighbour build (ivp_neighbour_build: cell sort, lists,
-    density and Aii) of copies of `scenes` with the given build kernel.  The
-    two build kernels differ by a few percent of a step, less than the noise
-    of a few timed steps, so the builds are timed on their own, each after an
-    L2 flush (as a build inside a step finds little of its data in L2)."""
-    import torch
+    """Milliseconds per neighbour-build kernel launch of copies of `scenes`
+    with the given build kernel, measured inside steps (ivp_profile_step:
+    host-driven steps with CUDA events around every kernel), so the build
+    finds the cache state a step leaves it: the slot-ordered positions the
+    preceding reorder pass just wrote.  The two build kernels differ by a few
+    percent of a step, less than the noise of a few timed steps."""
     from .engine import Engine
     opts = dataclasses.replace(base_options, lanes_per_particle=lanes, particles_per_block=ppb,
                                persistent=persistent, row_format=row_format, build_kernel=build_kernel)
     copies = [dataclasses.replace(sc, x=sc.x.copy(), v=sc.v.copy()) for sc in scenes]
     eng = Engine(copies, device=device, options=opts)
     try:
-        for _ in range(max(warmup, 1)):
-            eng.build()
-        stream = torch.cuda.current_stream()
-        flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
-        torch.cuda.synchronize()
-        for a, b in ev:
-            flush.fill_(1)
-            a.record(stream)
-            eng.build()
-            b.record(stream)
-        torch.cuda.synchronize()
-        return sum(a.elapsed_time(b) for a, b in ev) / reps
+        eng.build()
+        eng.step(max(warmup, 1))
+        ms, launches = eng.profile_step(reps)["nbr_build"]
+        return ms / launches
     finally:
         eng.close()
 
@@ -165,8 +157,8 @@ def tune(scenes: Sequence, device: str = "cuda", base_options=None, warmup: int 
     best = min(trials, key=lambda tr: tr.ms_per_step)
     build_ms = None
     if base.build_kernel == 0:
-        # both build kernels with the fastest shape, timed as builds (a caller
-        # that fixed the build kernel keeps it)
+        # both build kernels with the fastest shape, each build launch timed
+        # inside steps (a caller that fixed the build kernel keeps it)
         build_ms = {bk: _time_build(scenes, best.lanes_per_particle, best.particles_per_block, best.persistent,
                                     best.row_format, bk, device, warmup, BUILD_REPS, base)
                     for bk in BUILD_KERNELS}
