@@ -1844,7 +1844,11 @@ __device__ __forceinline__ double visc_setup_tile(const Dev& D, const SceneParam
 template <int G>
 __device__ __forceinline__ double visc_a_tile(const Dev& D, const SceneParams& P, const TileCtx& T, float beta,
                                               int it) {
-    const float4* cc = (it & 1) ? D.cg1 : D.cg0;  // {z | 1/rho, x}
+    // {z | 1/rho, x}.  Only dynamic slots' records are ever written; a
+    // static neighbour's record keeps the zeros of ivp_engine_create's
+    // workspace clear, so its 1/rho = 0 removes it from the sum (the
+    // reference's fluid-only `continue`) with finite arithmetic.
+    const float4* cc = (it & 1) ? D.cg1 : D.cg0;
     const int cnt = T.valid ? D.nbr_cnt[T.row] : 0;
     const bool fluid = T.valid && D.rflu[T.i] != 0.0f;
     float3 xi = make_float3(0.f, 0.f, 0.f), zi = xi;
