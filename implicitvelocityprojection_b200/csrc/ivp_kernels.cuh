@@ -738,7 +738,8 @@ __global__ void __launch_bounds__(256, 4) k_nbr_build(const Dev D) {
 // so it keeps the same first cache_size hits.  Two passes: the filter loop
 // only appends each kept hit to the thread's list in shared memory as 16 bits
 // (which of the 18 slot ranges, and the offset in it; hit k of thread t at
-// [k * blockDim + t], conflict-free), then a dense pass rebuilds each hit's
+// [k * blockDim + t], so two neighbouring threads share a 4-byte bank word:
+// at most 2-way conflicts), then a dense pass rebuilds each hit's
 // slot and computes its row entry, density and Aii terms.  The filter, which
 // runs for every candidate, stays short even though the lanes of a warp hit
 // on different iterations; the small list leaves most of L1 to the candidate
