@@ -302,3 +302,49 @@ def test_overflow_step_vs_oracle(golden_dir):
         ok, eng, st = H.compare_step(H.with_state(base, st.x, st.v))
         compared += ok
     assert compared >= 2, compared
+
+
+def _walls_only():
+    """A one-layer box with no fluid (a scene with no dynamic particle)."""
+    d = 0.02
+    box = (0.3, 0.3, 0.3)
+    margin = 4 * d
+    center = [margin + 0.5 * b for b in box]
+    shell = S.cube_shell(center, box, d, layers=1)
+    return S.assemble([], [shell], particle_radius=0.5 * d, domain_size=[b + 2 * margin for b in box])
+
+
+@pytest.mark.parametrize("persistent", [True, False])
+def test_edge_scenes_in_a_batch(persistent):
+    """Empty and ragged inputs in one batch: a scene with no fluid particle,
+    a single fluid particle, 65 fluid particles (one full tile and one
+    particle), and an ordinary column.  Every scene steps with status OK and
+    equals the scene run alone bit for bit; the fluid-free scene runs no
+    outer iteration and nothing in it moves; the others match the oracle
+    step by step."""
+    scs = [_walls_only(),
+           S.column_in_box((1, 1, 1), 0.02, (0.2, 0.2, 0.2), seed=3),
+           S.column_in_box((5, 13, 1), 0.02, (0.2, 0.4, 0.1), seed=4),
+           S.column_in_box((8, 12, 8), 0.02, (0.3, 0.4, 0.3), seed=1)]
+    assert [sc.n_dynamic for sc in scs] == [0, 1, 65, 768]
+    eng = H.engine(scs, persistent=persistent)
+    eng.build()
+    eng.step(3)
+    for i, sc in enumerate(scs):
+        assert eng.stats(i).status == 0, i
+        alone = H.engine([sc], persistent=persistent)
+        alone.build()
+        alone.step(3)
+        assert np.array_equal(eng.get("x", i), alone.get("x", 0)), i
+        assert np.array_equal(eng.get("v", i), alone.get("v", 0)), i
+    empty = eng.stats(0)
+    assert empty.stats_outer_iters == 0 and list(empty.stats_pcg_iters) == []
+    assert np.array_equal(eng.get("x", 0), scs[0].x) and not np.any(eng.get("v", 0))
+    compared = 0
+    for sc in scs[1:]:
+        state = sc
+        for _ in range(2):
+            ok, e, st = H.compare_step(state, persistent=persistent)
+            compared += ok
+            state = H.with_state(sc, e.get("x"), e.get("v"))
+    assert compared >= 5, compared
