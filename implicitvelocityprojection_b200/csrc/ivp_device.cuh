@@ -225,6 +225,7 @@ struct Dev {
     float4* nbr;
     unsigned short* nbr_g;
     int row_fmt;
+    int row_stream;          // 1: the rows exceed L2 (row loads hint L2 evict-first)
     int* nbr_cnt;
     int stride;
     // reductions
@@ -392,6 +393,16 @@ __device__ __forceinline__ float4 ld_vec(const float4* p) {
 // neighbour records that the particles of a tile share.
 __device__ __forceinline__ void ld_rec_nc(const float4* p, float4& a, float4& b) {
     asm volatile("ld.global.nc.L1::no_allocate.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+                 : "l"(p));
+}
+
+// The same load with an L2 evict-first hint, for rows that exceed L2 and so
+// stream from DRAM in every pass anyway: the hint keeps L2 for the neighbour
+// records the gathers reuse.  (Where the rows fit in L2 they are reused from
+// it by every pass, and the hint would evict them.)
+__device__ __forceinline__ void ld_rec_nc_stream(const float4* p, float4& a, float4& b) {
+    asm volatile("ld.global.nc.L1::no_allocate.L2::evict_first.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
                  : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
                  : "l"(p));
 }

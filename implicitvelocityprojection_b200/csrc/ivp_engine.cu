@@ -1075,6 +1075,17 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
     D.n_keys = e->n_keys;
     D.stride = opt->list_stride;
     D.row_fmt = P.row_fmt;
+    {
+        // rows hold about half their stride in use; beyond the L2 they
+        // stream from DRAM in every pass of the solves
+        int dev = 0, l2 = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev) != cudaSuccess) {
+            cudaGetLastError();
+            l2 = 126 << 20;
+        }
+        const double row_bytes = (double)e->n_dyn_total * opt->list_stride / 2 * 16.0;
+        D.row_stream = (P.row_fmt == ROW_FULL && row_bytes > (double)l2) ? 1 : 0;
+    }
     // few partials: every CTA of the persistent solve sums them itself
     // (2 x 8 B x tiles read per CTA per phase) instead of waiting for the
     // last CTA's decisions to travel back

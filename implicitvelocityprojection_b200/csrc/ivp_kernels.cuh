@@ -1410,7 +1410,10 @@ __device__ __forceinline__ bool load_pairs(const Dev& D, int row, float3 xi, int
         for (int u = 0; u < PU / 2; ++u) {
             const int k = k0 + u * 2 * G;
             float4 e0 = make_float4(0.f, 0.f, 0.f, 0.f), e1 = e0;
-            if (k < cnt) ld_rec_nc(nb + k, e0, e1);
+            if (k < cnt) {
+                if (D.row_stream) ld_rec_nc_stream(nb + k, e0, e1);
+                else ld_rec_nc(nb + k, e0, e1);
+            }
             pair_entry(e0, k < cnt, self, lo, hi, b.j[2 * u], b.J[2 * u], bad, b.live, 2 * u);
             pair_entry(e1, k + 1 < cnt, self, lo, hi, b.j[2 * u + 1], b.J[2 * u + 1], bad, b.live, 2 * u + 1);
         }
