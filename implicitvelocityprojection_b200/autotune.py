@@ -50,12 +50,10 @@ class Trial:
     persistent: bool
     row_format: int
     ms_per_step: float
-    build_kernel: int = 0
 
     def label(self) -> str:
-        b = {0: "", 1: "/thread-per-particle build", 2: "/warp-per-cell build"}[self.build_kernel]
         return (f"{self.lanes_per_particle}x{self.particles_per_block}/"
-                f"{'persistent' if self.persistent else 'per-phase'}/{'full' if self.row_format == 1 else 'compact'}{b}")
+                f"{'persistent' if self.persistent else 'per-phase'}/{'full' if self.row_format == 1 else 'compact'}")
 
 
 def signature(scenes: Sequence) -> str:
@@ -78,14 +76,11 @@ def candidates(per_phase: bool = True, row_formats: Sequence[int] = ROW_FORMATS)
     return out
 
 
-def _time_candidate(scenes, lanes, ppb, persistent, row_format, device, warmup, steps, base_options,
-                    build_kernel=None) -> float:
+def _time_candidate(scenes, lanes, ppb, persistent, row_format, device, warmup, steps, base_options) -> float:
     import torch
     from .engine import Engine
     opts = dataclasses.replace(base_options, lanes_per_particle=lanes, particles_per_block=ppb,
                                persistent=persistent, row_format=row_format)
-    if build_kernel is not None:
-        opts = dataclasses.replace(opts, build_kernel=build_kernel)
     copies = [dataclasses.replace(sc, x=sc.x.copy(), v=sc.v.copy()) for sc in scenes]
     eng = Engine(copies, device=device, options=opts)
     try:
@@ -162,11 +157,10 @@ def tune(scenes: Sequence, device: str = "cuda", base_options=None, warmup: int 
         build_ms = {bk: _time_build(scenes, best.lanes_per_particle, best.particles_per_block, best.persistent,
                                     best.row_format, bk, device, warmup, BUILD_REPS, base)
                     for bk in BUILD_KERNELS}
-        best = dataclasses.replace(best, build_kernel=min(build_ms, key=build_ms.get))
     res = {"signature": key,
            "choice": {"lanes_per_particle": best.lanes_per_particle, "particles_per_block": best.particles_per_block,
                       "persistent": best.persistent, "row_format": best.row_format,
-                      "build_kernel": best.build_kernel or base.build_kernel},
+                      "build_kernel": min(build_ms, key=build_ms.get) if build_ms else base.build_kernel},
            "table": [{"shape": tr.label(), "ms_per_step": round(tr.ms_per_step, 4)} for tr in trials],
            "build_ms": None if build_ms is None else
            {{1: "thread per particle", 2: "warp per cell"}[bk]: round(ms, 4) for bk, ms in build_ms.items()},
