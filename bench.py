@@ -744,38 +744,24 @@ def _e2e_schedule(args):
 
 
 def run_e2e_batch(args, scenes, dev, opts):
-    """Batched form end to end through Engine: every step copies the fluid
-    particles' x and v of all scenes from pinned host memory into the bound
-    arrays, steps, and copies them back (static particles never move, so a
-    caller keeps them on the device); the steps of the device-timed schedule
-    are timed."""
+    """Batched form end to end through Engine: every step uploads all
+    particles' x and v from pinned host memory and writes the new x and v
+    back, the copies overlapped with the step's kernels (Engine.step_io);
+    the steps of the device-timed schedule are timed."""
     import torch
     from implicitvelocityprojection_b200.engine import Engine
     eng = Engine(scenes, device=str(dev), options=opts)
     eng.build()
     x_d, v_d = eng.arrays["x"], eng.arrays["v"]
-    dyn = np.concatenate([np.asarray(sc.is_dynamic) == 1 for sc in scenes])
-    idx = torch.from_numpy(np.nonzero(dyn)[0].astype(np.int64)).to(dev)
-    nf = int(idx.numel())
-    # the fluid state as the caller holds it: contiguous, pinned
-    x_h = torch.empty((nf, 3), dtype=torch.float32).pin_memory()
-    v_h = torch.empty((nf, 3), dtype=torch.float32).pin_memory()
-    x_s = torch.empty((nf, 3), dtype=torch.float32, device=dev)
-    v_s = torch.empty((nf, 3), dtype=torch.float32, device=dev)
-    x_h.copy_(x_d.index_select(0, idx))
-    v_h.copy_(v_d.index_select(0, idx))
+    n = int(x_d.shape[0])
+    x_h = torch.empty((n, 3), dtype=torch.float32).pin_memory()
+    v_h = torch.empty((n, 3), dtype=torch.float32).pin_memory()
+    x_h.copy_(x_d)
+    v_h.copy_(v_d)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
     def one():
-        x_s.copy_(x_h, non_blocking=True)
-        v_s.copy_(v_h, non_blocking=True)
-        x_d.index_copy_(0, idx, x_s)
-        v_d.index_copy_(0, idx, v_s)
-        eng.step(1)
-        torch.index_select(x_d, 0, idx, out=x_s)
-        torch.index_select(v_d, 0, idx, out=v_s)
-        x_h.copy_(x_s, non_blocking=True)
-        v_h.copy_(v_s, non_blocking=True)
+        eng.step_io(x_h, v_h, x_h, v_h)
         torch.cuda.synchronize()
 
     sched = _e2e_schedule(args)
@@ -792,11 +778,11 @@ def run_e2e_batch(args, scenes, dev, opts):
         k += 1
     nd = sum(sc.n_dynamic for sc in scenes)
     del eng
-    return {"value": nd * len(sched) / tot, "unit": UNIT, "h2d_bytes_per_step": 2 * nf * 12,
-            "d2h_bytes_per_step": 2 * nf * 12, "steps": len(sched),
-            "api": "Engine(scenes).step(1) with every scene's fluid x, v copied from/to pinned host memory every "
-                   "step (gathered and scattered on the device by an index list; the device-timed schedule's "
-                   "steps timed)"}
+    return {"value": nd * len(sched) / tot, "unit": UNIT, "h2d_bytes_per_step": 2 * n * 12,
+            "d2h_bytes_per_step": 2 * n * 12, "steps": len(sched),
+            "api": "Engine(scenes).step_io(x, v, x, v): every particle's x, v uploaded from and written back to "
+                   "pinned host memory inside every step, the copies overlapped with its kernels (ivp_step_io; "
+                   "the device-timed schedule's steps timed)"}
 
 
 def run_e2e(args, sc, dev):
@@ -823,11 +809,10 @@ def run_e2e(args, sc, dev):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
     def one():
-        ps.x[:n].copy_(x_h, non_blocking=True)
-        ps.v[:n].copy_(v_h, non_blocking=True)
-        fw.forward()  # raises on a failed solve; reads the stats (one sync)
-        x_h.copy_(ps.x[:n], non_blocking=True)
-        v_h.copy_(ps.v[:n], non_blocking=True)
+        # x, v uploaded into the step and its new x, v written back, the
+        # copies overlapped with the step's kernels; raises on a failed
+        # solve; reads the stats (one sync)
+        fw.forward_host(x_h, v_h)
         torch.cuda.synchronize()
 
     sched = _e2e_schedule(args)
@@ -844,8 +829,9 @@ def run_e2e(args, sc, dev):
         k += 1
     return {"value": sc.n_dynamic * len(sched) / tot, "unit": UNIT, "h2d_bytes_per_step": 2 * n * 12,
             "d2h_bytes_per_step": 2 * n * 12 + 256, "steps": len(sched),
-            "api": "Framework.forward() with the fluid particles' x, v copied from/to pinned host memory every "
-                   "step (the device-timed schedule's steps timed)"}
+            "api": "Framework.forward_host(x, v): the fluid particles' x, v uploaded from and written back to "
+                   "pinned host memory inside every step, the copies overlapped with its kernels (ivp_step_io; "
+                   "the device-timed schedule's steps timed)"}
 
 
 def main():

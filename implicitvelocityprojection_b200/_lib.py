@@ -129,6 +129,7 @@ SIGNATURES = {
     "ivp_apply_gravity": (_I, [_P, _P]),
     "ivp_advect": (_I, [_P, _P]),
     "ivp_step": (_I, [_P, _I, _P]),
+    "ivp_step_io": (_I, [_P, _P, _P, _P, _P, ctypes.c_int64, ctypes.c_int64, _P]),
     "ivp_reset_counters": (_I, [_P, _P]),
     "ivp_profile_step": (_I, [_P, _I, _P, _P, _P]),
     "ivp_read_stats": (_I, [_P, _I, _P, ctypes.POINTER(SolveStats)]),

@@ -79,6 +79,23 @@ struct ivp_engine {
     // graphs
     cudaGraph_t graph_step = nullptr, graph_solve = nullptr, graph_build = nullptr, graph_prj = nullptr;
     cudaGraphExec_t exec_step = nullptr, exec_solve = nullptr, exec_build = nullptr, exec_prj = nullptr;
+    // steps with host input/output (ivp_step_io): the copies of the graph
+    // below are baked in for the host pointers and range of `io_key`
+    cudaGraph_t graph_step_io = nullptr;
+    cudaGraphExec_t exec_step_io = nullptr;
+    struct StepIO {
+        const float* x_in = nullptr;
+        const float* v_in = nullptr;
+        float* x_out = nullptr;
+        float* v_out = nullptr;
+        int64_t first = 0, count = 0;
+        bool operator==(const StepIO& o) const {
+            return x_in == o.x_in && v_in == o.v_in && x_out == o.x_out && v_out == o.v_out && first == o.first &&
+                   count == o.count;
+        }
+    } io, io_key;
+    cudaStream_t io_side = nullptr;                              // stream-ordered steps: the copy stream
+    cudaEvent_t io_ev_start = nullptr, io_ev_x = nullptr, io_ev_adv = nullptr, io_ev_out = nullptr;
     // host mirrors
     SceneCtl* h_ctl = nullptr;   // pinned
     Flags* h_flags = nullptr;    // pinned
@@ -110,6 +127,19 @@ struct Launcher {
     cudaGraphNode_t last = nullptr;
     bool has_last = false;
     Prof* prof = nullptr;
+    // host copies of an ivp_step_io step (null otherwise), and a node the
+    // next chained node must also wait for (graph mode)
+    ivp_engine* io = nullptr;
+    cudaGraphNode_t io_x = nullptr;  // the upload of x (graph mode)
+    cudaGraphNode_t extra = nullptr;
+
+    int deps(cudaGraphNode_t* d) {
+        int n = 0;
+        if (has_last) d[n++] = last;
+        if (extra) d[n++] = extra;
+        extra = nullptr;
+        return n;
+    }
 
     int launch_now(const void* fn, dim3 grid, dim3 block, void** args, size_t smem, bool coop) {
         if (coop) {
@@ -145,8 +175,9 @@ struct Launcher {
         p.sharedMemBytes = (unsigned)smem;
         p.kernelParams = args;
         p.extra = nullptr;
-        cudaGraphNode_t n;
-        CK(cudaGraphAddKernelNode(&n, graph, has_last ? &last : nullptr, has_last ? 1 : 0, &p));
+        cudaGraphNode_t n, d[2];
+        const int nd = deps(d);
+        CK(cudaGraphAddKernelNode(&n, graph, nd ? d : nullptr, nd, &p));
         if (coop) {
             cudaKernelNodeAttrValue v;
             memset(&v, 0, sizeof(v));
@@ -176,10 +207,32 @@ struct Launcher {
         mp.width = bytes;
         mp.height = 1;
         mp.pitch = 0;
-        cudaGraphNode_t n;
-        CK(cudaGraphAddMemsetNode(&n, graph, has_last ? &last : nullptr, has_last ? 1 : 0, &mp));
+        cudaGraphNode_t n, d[2];
+        const int nd = deps(d);
+        CK(cudaGraphAddMemsetNode(&n, graph, nd ? d : nullptr, nd, &mp));
         last = n;
         has_last = true;
+        return IVP_OK;
+    }
+    // A host<->device copy: chained (after the last node, and the next node
+    // waits for it) or, with `branch`, as a node after `after` (none: a root)
+    // that nothing in the chain waits for unless it is handed to `extra`.
+    int copy(void* dst, const void* src, size_t bytes, cudaMemcpyKind kind, bool branch = false,
+             cudaGraphNode_t after = nullptr, cudaGraphNode_t* out = nullptr) {
+        if (bytes == 0) return IVP_OK;
+        cudaGraphNode_t n, d[2];
+        int nd = 0;
+        if (branch) {
+            if (after) d[nd++] = after;
+        } else {
+            nd = deps(d);
+        }
+        CK(cudaGraphAddMemcpyNode1D(&n, graph, nd ? d : nullptr, nd, dst, src, bytes, kind));
+        if (out) *out = n;
+        if (!branch) {
+            last = n;
+            has_last = true;
+        }
         return IVP_OK;
     }
 };
@@ -264,8 +317,29 @@ int emit_build_impl(ivp_engine* e, Launcher& L, bool with_advect) {
     const Dev& D = e->D;
     // cell_count is all zero between builds (k_place clears what it used)
     if (with_advect) {
+        // ivp_step_io: the advection is the step's first reader of x (and the
+        // last writer of x and v), so the upload of x only has to land before
+        // it and the downloads can start right after it
+        const ivp_engine::StepIO* io = L.io ? &L.io->io : nullptr;
+        if (io && io->x_in) {
+            if (L.graph) L.extra = L.io_x;
+            else CK(cudaStreamWaitEvent(L.stream, L.io->io_ev_x, 0));
+        }
         CKS(L.dev(IVP_K_ADVECT, k_advect_keys, blocks_for(std::max(e->n_total, e->n_scenes), ELEM_BLOCK), ELEM_BLOCK,
                   D));
+        if (io && (io->x_out || io->v_out)) {
+            const size_t off = 3 * (size_t)io->first, bytes = 12 * (size_t)io->count;
+            if (L.graph) {
+                if (io->x_out) CKS(L.copy(io->x_out, D.x + off, bytes, cudaMemcpyDeviceToHost, true, L.last));
+                if (io->v_out) CKS(L.copy(io->v_out, D.v + off, bytes, cudaMemcpyDeviceToHost, true, L.last));
+            } else {
+                CK(cudaEventRecord(L.io->io_ev_adv, L.stream));
+                CK(cudaStreamWaitEvent(L.io->io_side, L.io->io_ev_adv, 0));
+                if (io->x_out) CK(cudaMemcpyAsync(io->x_out, D.x + off, bytes, cudaMemcpyDeviceToHost, L.io->io_side));
+                if (io->v_out) CK(cudaMemcpyAsync(io->v_out, D.v + off, bytes, cudaMemcpyDeviceToHost, L.io->io_side));
+                CK(cudaEventRecord(L.io->io_ev_out, L.io->io_side));
+            }
+        }
     } else {
         CKS(L.memset0(D.overflow, sizeof(int) * (size_t)e->n_scenes));
         CKS(L.memset0(D.pairs, sizeof(unsigned long long) * (size_t)e->n_scenes));
@@ -554,7 +628,36 @@ int emit_step(ivp_engine* e, Launcher& L) {
     return IVP_OK;
 }
 
+// A step with host input/output (ivp_step_io): v is uploaded before the
+// step's first force reads it; x, first read by the advection, is uploaded
+// beside the solves; x and v are downloaded beside the next step's build.
+int emit_step_io(ivp_engine* e, Launcher& L) {
+    const ivp_engine::StepIO& io = e->io;
+    const size_t off = 3 * (size_t)io.first, bytes = 12 * (size_t)io.count;
+    L.io = e;
+    if (L.graph) {
+        if (io.v_in) CKS(L.copy(e->D.v + off, io.v_in, bytes, cudaMemcpyHostToDevice));
+        if (io.x_in) CKS(L.copy(e->D.x + off, io.x_in, bytes, cudaMemcpyHostToDevice, true, nullptr, &L.io_x));
+    } else {
+        if (io.v_in) CK(cudaMemcpyAsync(e->D.v + off, io.v_in, bytes, cudaMemcpyHostToDevice, L.stream));
+        if (io.x_in) {
+            CK(cudaEventRecord(e->io_ev_start, L.stream));
+            CK(cudaStreamWaitEvent(e->io_side, e->io_ev_start, 0));
+            CK(cudaMemcpyAsync(e->D.x + off, io.x_in, bytes, cudaMemcpyHostToDevice, e->io_side));
+            CK(cudaEventRecord(e->io_ev_x, e->io_side));
+        }
+    }
+    CKS(emit_step(e, L));
+    // the step ends when its downloads have landed
+    if (!L.graph && (io.x_out || io.v_out)) CK(cudaStreamWaitEvent(L.stream, e->io_ev_out, 0));
+    return IVP_OK;
+}
+
 void destroy_graphs(ivp_engine* e) {
+    if (e->exec_step_io) cudaGraphExecDestroy(e->exec_step_io);
+    if (e->graph_step_io) cudaGraphDestroy(e->graph_step_io);
+    e->exec_step_io = nullptr;
+    e->graph_step_io = nullptr;
     if (e->exec_step) cudaGraphExecDestroy(e->exec_step);
     if (e->exec_solve) cudaGraphExecDestroy(e->exec_solve);
     if (e->exec_prj) cudaGraphExecDestroy(e->exec_prj);
@@ -1160,6 +1263,14 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
 int ivp_engine_destroy(ivp_engine* e) {
     if (!e) return IVP_OK;
     destroy_graphs(e);
+    if (e->io_side) {
+        cudaStreamSynchronize(e->io_side);
+        cudaStreamDestroy(e->io_side);
+        cudaEventDestroy(e->io_ev_start);
+        cudaEventDestroy(e->io_ev_x);
+        cudaEventDestroy(e->io_ev_adv);
+        cudaEventDestroy(e->io_ev_out);
+    }
     if (e->h_ctl) cudaFreeHost(e->h_ctl);
     if (e->h_flags) cudaFreeHost(e->h_flags);
     if (e->h_overflow) cudaFreeHost(e->h_overflow);
@@ -1302,6 +1413,56 @@ int ivp_step(ivp_engine* e, int32_t n_steps, void* stream) {
     if (!e || n_steps < 0) return IVP_ERR_BAD_ARG;
     for (int k = 0; k < n_steps; ++k) CKS(run(e, emit_step, &e->graph_step, &e->exec_step, as_stream(stream)));
     return IVP_OK;
+}
+
+int ivp_step_io(ivp_engine* e, const float* x_in, const float* v_in, float* x_out, float* v_out, int64_t first,
+                int64_t count, void* stream) {
+    if (!e || first < 0 || count < 0 || first + count > e->n_total) return IVP_ERR_BAD_ARG;
+    if (!e->bound) return IVP_ERR_NOT_BOUND;
+    // host buffers must be page-locked: the copies run inside the step
+    const void* host[4] = {x_in, v_in, x_out, v_out};
+    for (const void* h : host) {
+        if (!h) continue;
+        cudaPointerAttributes a;
+        if (cudaPointerGetAttributes(&a, h) != cudaSuccess) {
+            cudaGetLastError();
+            return IVP_ERR_BAD_ARG;
+        }
+        if (a.type != cudaMemoryTypeHost) return IVP_ERR_BAD_ARG;
+    }
+    if (!e->io_side) {
+        CK(cudaStreamCreateWithFlags(&e->io_side, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&e->io_ev_start, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&e->io_ev_x, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&e->io_ev_adv, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&e->io_ev_out, cudaEventDisableTiming));
+    }
+    ivp_engine::StepIO io;
+    io.x_in = x_in;
+    io.v_in = v_in;
+    io.x_out = x_out;
+    io.v_out = v_out;
+    io.first = first;
+    io.count = count;
+    e->io = io;
+    cudaStream_t s = as_stream(stream);
+    if (e->opt.use_graphs) {
+        if (e->exec_step_io && !(io == e->io_key)) {
+            cudaGraphExecDestroy(e->exec_step_io);
+            cudaGraphDestroy(e->graph_step_io);
+            e->exec_step_io = nullptr;
+            e->graph_step_io = nullptr;
+        }
+        if (!e->exec_step_io) {
+            CKS(make_graph(e, emit_step_io, &e->graph_step_io, &e->exec_step_io));
+            e->io_key = io;
+        }
+        CK(cudaGraphLaunch(e->exec_step_io, s));
+        return IVP_OK;
+    }
+    Launcher L;
+    L.stream = s;
+    return emit_step_io(e, L);
 }
 
 int ivp_read_stats(ivp_engine* e, int32_t scene, void* stream, ivp_solve_stats* out) {

@@ -250,6 +250,27 @@ class Engine:
         """n Framework.forward() steps of every scene (asynchronous)."""
         check(self.L.ivp_step(self._handle, int(n), ctypes.c_void_p(_stream_ptr(stream))), "ivp_step")
 
+    def step_io(self, x_in=None, v_in=None, x_out=None, v_out=None, first: int = 0, count=None, stream=None):
+        """One step whose x and v of particles [first, first + count) come
+        from and go back to page-locked host tensors (float32, (count, 3)),
+        the copies overlapped with the step's kernels (ivp_step_io).  Inputs
+        and outputs may be the same tensors.  Asynchronous: the outputs are
+        complete once the stream has passed the step."""
+        import torch
+        n = self.n_total - first if count is None else int(count)
+
+        def ptr(t):
+            if t is None:
+                return None
+            if t.device.type != "cpu" or not t.is_pinned() or t.dtype != torch.float32 or not t.is_contiguous():
+                raise ValueError("step_io needs contiguous, page-locked float32 host tensors")
+            if t.numel() != 3 * n:
+                raise ValueError(f"step_io: expected {n} x 3 values, got {t.numel()}")
+            return ctypes.c_void_p(t.data_ptr())
+
+        check(self.L.ivp_step_io(self._handle, ptr(x_in), ptr(v_in), ptr(x_out), ptr(v_out), int(first), n,
+                                 ctypes.c_void_p(_stream_ptr(stream))), "ivp_step_io")
+
     def set_wait_limit(self, ns: int):
         """Test hook: longest wait on a grid barrier of the persistent kernels
         (ns <= 0 restores the default of 2 s)."""

@@ -102,6 +102,24 @@ class Framework:
         self.pressure.apply_stats(st, self.stats_pressure_ms)
         self.time += self.dt
 
+    def forward_host(self, x, v, first: int = 0):
+        """forward() for a caller that keeps the moving particles' state in
+        host memory: x and v (page-locked float32 (count, 3) tensors holding
+        particles first .. first + count) are uploaded into the step and the
+        step's new x and v written back into them, the copies overlapped with
+        the step's kernels (ivp_step_io).  Statistics as forward()."""
+        if self.use_cfl:
+            self._cfl()
+        if not self.pressure_enabled:
+            raise NotImplementedError("pressureEnabled = false is not supported by the fused step")
+        t0 = time.perf_counter()
+        eng = self.engine()
+        eng.step_io(x, v, x, v, first=first, count=int(x.shape[0]))
+        st = eng.stats(0)
+        self.stats_pressure_ms = (time.perf_counter() - t0) * 1000.0
+        self.pressure.apply_stats(st, self.stats_pressure_ms)
+        self.time += self.dt
+
     def forward_many(self, n: int):
         """n steps queued back to back; statistics and errors of the last step."""
         if self.use_cfl:

@@ -230,6 +230,21 @@ int ivp_advect(ivp_engine* e, void* stream);
  * (ivp_neighbour_build), as Framework.initialize does (framework.py:323-330). */
 int ivp_step(ivp_engine* e, int32_t n_steps, void* stream);
 
+/* One ivp_step whose particle state comes from and goes back to host memory,
+ * as a caller of Framework.forward() that keeps x and v on the host would copy
+ * it around each step (framework.py:423-544 works on device arrays): x_in /
+ * v_in (float[count][3], particles [first, first + count) of the bound
+ * arrays) are uploaded and x_out / v_out downloaded inside the step,
+ * overlapped with its kernels -- v before the first force, x beside the
+ * solves (the advection is its first reader), both downloads beside the next
+ * step's neighbour build (the advection is the last writer of x and v).
+ * Inputs and outputs may alias (the upload of x lands before the advection,
+ * the downloads start after it).  Any pointer may be NULL (that copy is
+ * skipped).  Host buffers must be page-locked (IVP_ERR_BAD_ARG otherwise).
+ * The outputs are complete when the stream has passed the step. */
+int ivp_step_io(ivp_engine* e, const float* x_in, const float* v_in, float* x_out, float* v_out, int64_t first,
+                int64_t count, void* stream);
+
 /* Zeroes the counters reported in ivp_solve_stats (stream-ordered). */
 int ivp_reset_counters(ivp_engine* e, void* stream);
 
