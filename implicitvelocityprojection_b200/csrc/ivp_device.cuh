@@ -123,6 +123,15 @@ struct Flags {
     int timeout, pad0, pad1, pad2;
 };
 
+// Byte layout of the statistics staging block: the scene's control block,
+// overflow count, the flags, pair count, correction count, then its error and
+// CG-count histories (max_hist entries each).
+struct StatStage {
+    size_t ctl, ovf, flags, pairs, fix, err, pcg, total;
+    __host__ __device__ static size_t up8(size_t b) { return (b + 7) & ~size_t(7); }
+    __host__ __device__ explicit StatStage(int hist);
+};
+
 struct Dev {
     // bound arrays (caller order)
     float* x;
@@ -235,6 +244,9 @@ struct Dev {
     Flags* flags;
     double* err_hist;
     int* pcg_hist;
+    // one scene's statistics gathered for a single device-to-host copy
+    // (StatStage layout)
+    unsigned char* stage;
     int hist_len;
     // graph conditionals (0 = not inside a conditional graph)
     unsigned long long h_outer, h_solve, h_cg, h_visc;
@@ -429,6 +441,17 @@ __device__ __forceinline__ double block_sum_d(double v, double* sh) {
     }
     __syncthreads();
     return sh[0];
+}
+
+__host__ __device__ inline StatStage::StatStage(int hist) {
+    ctl = 0;
+    ovf = up8(sizeof(SceneCtl));
+    flags = ovf + 8;
+    pairs = up8(flags + sizeof(Flags));
+    fix = pairs + 8;
+    err = fix + 8;
+    pcg = err + sizeof(double) * (size_t)hist;
+    total = up8(pcg + sizeof(int) * (size_t)hist);
 }
 
 }  // namespace ivp

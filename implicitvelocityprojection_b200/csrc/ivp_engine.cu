@@ -103,6 +103,7 @@ struct ivp_engine {
     unsigned long long* h_pairs = nullptr;  // pinned
     double* h_err = nullptr;     // pinned, max_hist: one scene's density-error history
     int* h_pcg = nullptr;        // pinned, max_hist: one scene's CG counts per outer iteration
+    unsigned char* h_stage = nullptr;  // pinned: one scene's statistics block (StatStage)
 };
 
 // ------------------------------------------------------------ launching
@@ -636,8 +637,11 @@ int emit_step_io(ivp_engine* e, Launcher& L) {
     const size_t off = 3 * (size_t)io.first, bytes = 12 * (size_t)io.count;
     L.io = e;
     if (L.graph) {
-        if (io.v_in) CKS(L.copy(e->D.v + off, io.v_in, bytes, cudaMemcpyHostToDevice));
-        if (io.x_in) CKS(L.copy(e->D.x + off, io.x_in, bytes, cudaMemcpyHostToDevice, true, nullptr, &L.io_x));
+        // x follows v over the bus: v, which the first kernel waits for, gets
+        // the whole host-to-device bandwidth
+        cudaGraphNode_t v_node = nullptr;
+        if (io.v_in) CKS(L.copy(e->D.v + off, io.v_in, bytes, cudaMemcpyHostToDevice, false, nullptr, &v_node));
+        if (io.x_in) CKS(L.copy(e->D.x + off, io.x_in, bytes, cudaMemcpyHostToDevice, true, v_node, &L.io_x));
     } else {
         if (io.v_in) CK(cudaMemcpyAsync(e->D.v + off, io.v_in, bytes, cudaMemcpyHostToDevice, L.stream));
         if (io.x_in) {
@@ -776,7 +780,7 @@ struct Plan {
     bool any_st = false;   // some scene runs the implicit surface tension
     int drop_cap = 0;      // dropped-pair records of the overflow fix-up
     int fix_scan_blocks = 0;
-    size_t off[72];
+    size_t off[73];
     Layout lay;
 };
 
@@ -947,6 +951,7 @@ void plan(const ivp_scene_desc* sc, int n, const ivp_options* o, Plan& P) {
     P.off[i++] = L.add(sizeof(float4) * N);                                    // 65 vpp
     P.off[i++] = L.add(sizeof(float4) * N);                                    // 66 vlp
     P.off[i++] = L.add(P.any_st ? sizeof(float4) * N : 0);                     // 67 stz
+    P.off[i++] = L.add(StatStage(o->max_hist).total);                          // 68 stage
 }
 
 cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
@@ -954,22 +959,28 @@ cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 // Reading a scene's solve statistics: the copies into the engine's pinned
 // mirrors are enqueued on the caller's stream, the caller synchronises once,
 // then the fill functions convert.
-int enqueue_stats(ivp_engine* e, int scene, cudaStream_t s) {
-    CK(cudaMemcpyAsync(e->h_ctl + scene, e->D.ctl + scene, sizeof(SceneCtl), cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(e->h_overflow + scene, e->D.overflow + scene, sizeof(int), cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(e->h_flags, e->D.flags, sizeof(Flags), cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(e->h_pairs + scene, e->D.pairs + scene, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(e->h_fix_scene + scene, e->D.fix_scene + scene, sizeof(int), cudaMemcpyDeviceToHost, s));
+// One scene's statistics and histories (the whole history rows, max_hist
+// entries each) in one device-to-host copy after a gather kernel, instead of
+// one copy per array; unpack_stage places them in the host mirrors.
+int enqueue_stage(ivp_engine* e, int scene, cudaStream_t s) {
+    const int H = e->opt.max_hist;
+    k_stage_stats<<<1, 256, 0, s>>>(e->D, scene, H);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(e->h_stage, e->D.stage, StatStage(H).total, cudaMemcpyDeviceToHost, s));
     return IVP_OK;
 }
 
-// the scene's whole history rows (max_hist entries each)
-int enqueue_history(ivp_engine* e, int scene, cudaStream_t s) {
+void unpack_stage(ivp_engine* e, int scene) {
     const int H = e->opt.max_hist;
-    const size_t base = (size_t)scene * H;
-    CK(cudaMemcpyAsync(e->h_err, e->D.err_hist + base, sizeof(double) * H, cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(e->h_pcg, e->D.pcg_hist + base, sizeof(int) * H, cudaMemcpyDeviceToHost, s));
-    return IVP_OK;
+    const StatStage L(H);
+    const unsigned char* b = e->h_stage;
+    memcpy(e->h_ctl + scene, b + L.ctl, sizeof(SceneCtl));
+    memcpy(e->h_overflow + scene, b + L.ovf, sizeof(int));
+    memcpy(e->h_flags, b + L.flags, sizeof(Flags));
+    memcpy(e->h_pairs + scene, b + L.pairs, sizeof(unsigned long long));
+    memcpy(e->h_fix_scene + scene, b + L.fix, sizeof(int));
+    memcpy(e->h_err, b + L.err, sizeof(double) * (size_t)H);
+    memcpy(e->h_pcg, b + L.pcg, sizeof(int) * (size_t)H);
 }
 
 int fill_stats(ivp_engine* e, int scene, ivp_solve_stats* out) {
@@ -1161,6 +1172,7 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
     D.vpp = reinterpret_cast<float4*>(w + P.off[i++]);
     D.vlp = reinterpret_cast<float4*>(w + P.off[i++]);
     D.stz = reinterpret_cast<float4*>(w + P.off[i++]);
+    D.stage = reinterpret_cast<unsigned char*>(w + P.off[i++]);
     D.drop_cap = P.drop_cap;
     e->fix_scan_blocks = P.fix_scan_blocks;
     D.n_segs = (int)P.segs.size();
@@ -1214,7 +1226,8 @@ int ivp_engine_create(const ivp_scene_desc* scenes, int32_t n_scenes, const ivp_
         cudaHostAlloc((void**)&e->h_err, sizeof(double) * opt->max_hist, cudaHostAllocDefault) != cudaSuccess ||
         cudaHostAlloc((void**)&e->h_pcg, sizeof(int) * opt->max_hist, cudaHostAllocDefault) != cudaSuccess ||
         cudaHostAlloc((void**)&e->h_ovf, sizeof(int), cudaHostAllocDefault) != cudaSuccess ||
-        cudaHostAlloc((void**)&e->h_fix_scene, sizeof(int) * n_scenes, cudaHostAllocDefault) != cudaSuccess)
+        cudaHostAlloc((void**)&e->h_fix_scene, sizeof(int) * n_scenes, cudaHostAllocDefault) != cudaSuccess ||
+        cudaHostAlloc((void**)&e->h_stage, StatStage(opt->max_hist).total, cudaHostAllocDefault) != cudaSuccess)
         return fail(IVP_ERR_CUDA);
     if (cudaMemcpyAsync((void*)D.scenes, P.hp.data(), sizeof(SceneParams) * n_scenes, cudaMemcpyHostToDevice, s) !=
             cudaSuccess ||
@@ -1279,6 +1292,7 @@ int ivp_engine_destroy(ivp_engine* e) {
     if (e->h_pcg) cudaFreeHost(e->h_pcg);
     if (e->h_ovf) cudaFreeHost(e->h_ovf);
     if (e->h_fix_scene) cudaFreeHost(e->h_fix_scene);
+    if (e->h_stage) cudaFreeHost(e->h_stage);
     delete e;
     return IVP_OK;
 }
@@ -1468,8 +1482,9 @@ int ivp_step_io(ivp_engine* e, const float* x_in, const float* v_in, float* x_ou
 int ivp_read_stats(ivp_engine* e, int32_t scene, void* stream, ivp_solve_stats* out) {
     if (!e || !out || scene < 0 || scene >= e->n_scenes) return IVP_ERR_BAD_ARG;
     cudaStream_t s = as_stream(stream);
-    CKS(enqueue_stats(e, scene, s));
+    CKS(enqueue_stage(e, scene, s));
     CK(cudaStreamSynchronize(s));
+    unpack_stage(e, scene);
     return fill_stats(e, scene, out);
 }
 
@@ -1500,9 +1515,9 @@ int ivp_read_history(ivp_engine* e, int32_t scene, void* stream, double* errors,
                      int32_t* n_errors, int32_t* n_pcg) {
     if (!e || scene < 0 || scene >= e->n_scenes || cap < 0) return IVP_ERR_BAD_ARG;
     cudaStream_t s = as_stream(stream);
-    CK(cudaMemcpyAsync(e->h_ctl + scene, e->D.ctl + scene, sizeof(SceneCtl), cudaMemcpyDeviceToHost, s));
-    CKS(enqueue_history(e, scene, s));
+    CKS(enqueue_stage(e, scene, s));
     CK(cudaStreamSynchronize(s));
+    unpack_stage(e, scene);
     fill_history(e, scene, errors, pcg_iters, cap, n_errors, n_pcg);
     return IVP_OK;
 }
@@ -1511,9 +1526,9 @@ int ivp_read_solve(ivp_engine* e, int32_t scene, void* stream, ivp_solve_stats* 
                    int32_t* pcg_iters, int32_t cap, int32_t* n_errors, int32_t* n_pcg) {
     if (!e || !out || scene < 0 || scene >= e->n_scenes || cap < 0) return IVP_ERR_BAD_ARG;
     cudaStream_t s = as_stream(stream);
-    CKS(enqueue_stats(e, scene, s));
-    CKS(enqueue_history(e, scene, s));
+    CKS(enqueue_stage(e, scene, s));
     CK(cudaStreamSynchronize(s));
+    unpack_stage(e, scene);
     fill_history(e, scene, errors, pcg_iters, cap, n_errors, n_pcg);
     return fill_stats(e, scene, out);
 }

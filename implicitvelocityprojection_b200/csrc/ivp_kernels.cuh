@@ -3116,6 +3116,26 @@ __global__ void k_reset_counters(const Dev D) {
 }
 
 // Neighbour lists of one scene in the reference layout, original indices.
+// One scene's statistics and histories gathered into the staging block
+// (StatStage), so the host reads them with one copy.  One CTA, 4-byte words
+// (every part is a multiple of 4 bytes).
+__device__ __forceinline__ void copy_words(unsigned char* dst, const void* src, size_t bytes) {
+    const unsigned* s = static_cast<const unsigned*>(src);
+    unsigned* d = reinterpret_cast<unsigned*>(dst);
+    for (size_t k = threadIdx.x; k < bytes / 4; k += blockDim.x) d[k] = s[k];
+}
+
+__global__ void k_stage_stats(const Dev D, int scene, int hist) {
+    const StatStage L(hist);
+    copy_words(D.stage + L.ctl, D.ctl + scene, sizeof(SceneCtl));
+    copy_words(D.stage + L.ovf, D.overflow + scene, sizeof(int));
+    copy_words(D.stage + L.flags, D.flags, sizeof(Flags));
+    copy_words(D.stage + L.pairs, D.pairs + scene, sizeof(unsigned long long));
+    copy_words(D.stage + L.fix, D.fix_scene + scene, sizeof(int));
+    copy_words(D.stage + L.err, D.err_hist + (size_t)scene * hist, sizeof(double) * (size_t)hist);
+    copy_words(D.stage + L.pcg, D.pcg_hist + (size_t)scene * hist, sizeof(int) * (size_t)hist);
+}
+
 __global__ void k_export(const Dev D, int scene, int* count, int* ids, int cache) {
     const SceneParams& P = D.scenes[scene];
     const int i = P.s_begin + blockIdx.x * blockDim.x + threadIdx.x;
