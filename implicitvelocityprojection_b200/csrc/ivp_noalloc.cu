@@ -4,9 +4,8 @@
 // Who needs this: callers that cannot allocate device memory themselves or let
 // a library do it -- code that runs inside another runtime's memory arena
 // (for example a host whose GPU memory is managed by Warp's or a renderer's
-// fixed-budget allocator), code recorded into a CUDA stream capture in global
-// capture mode, where cudaMalloc is illegal, and real-time loops that cannot
-// afford the implicit device synchronisation of cudaMalloc/cudaFree.  The
+// fixed-budget allocator), and real-time loops that cannot afford the
+// implicit device synchronisation of cudaMalloc/cudaFree.  The
 // regular engine needs a caller-provided workspace sized by
 // ivp_workspace_bytes; this entry point needs none.  Instead it works in one
 // file-scope device array of fixed size (kScratchBytes below, about 6.3 MB),
@@ -24,8 +23,8 @@
 //
 // Set-up: the device address of the array is looked up with
 // cudaGetSymbolAddress the first time the entry point runs on a device (with
-// that device current) and cached.  That first call must come before any
-// stream capture that would record it.
+// that device current) and cached.  Make that first call on a device before
+// any stream capture.
 #include <cuda_runtime.h>
 
 #include <cmath>

@@ -304,9 +304,9 @@ int ivp_set_wait_limit(ivp_engine* e, int64_t ns);
 /* No counterpart in the reference.  SPH density and k = 1/(Aii + 1e-3) of
  * every dynamic particle of one scene (k = 0 for static particles), for
  * callers that cannot allocate device memory: code living inside another
- * runtime's memory arena, code recorded into a stream capture in global mode
- * (where cudaMalloc is illegal), or real-time loops that cannot take the
- * device synchronisation of cudaMalloc/cudaFree.  It allocates nothing and
+ * runtime's memory arena (whose GPU memory another allocator owns), or
+ * real-time loops that cannot take the device synchronisation of
+ * cudaMalloc/cudaFree.  It allocates nothing and
  * needs no workspace: its scratch is one fixed device array inside the
  * library (about 6.3 MB, held on every GPU that loads the library until the
  * process exits).  Results equal those of ivp_neighbour_build for the same

@@ -2,7 +2,7 @@
 C ABI, against the regular neighbour build (ivp_neighbour_build).
 
 It serves callers that cannot allocate device memory (code inside another
-runtime's memory arena, code captured in global stream-capture mode, loops
+runtime's memory arena, whose GPU memory another allocator owns, and loops
 that cannot take cudaMalloc's synchronisation).  Two calls in a row must both
 reproduce the engine's density and k, which also shows that what one call
 leaves in the shared scratch array does not leak into the next.  This file
